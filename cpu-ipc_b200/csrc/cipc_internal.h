@@ -1,0 +1,229 @@
+// Internal state of one GPU simulation context and the launchers each
+// translation unit exports.  Not part of the public C ABI (include/cipc_gpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#define CIPC_CUDA(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t e__ = (call);                                                                \
+        if (e__ != cudaSuccess)                                                                  \
+            throw cipc::CudaError(std::string(#call) + ": " + cudaGetErrorString(e__));          \
+    } while (0)
+
+namespace cipc {
+
+// Number of this library's kernel launches since load (CUB sorts/scans are
+// not counted).  Every launch goes through launch() below.
+extern long long g_kernelLaunches;
+
+template <class... KArgs, class... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args&&... args) {
+    ++g_kernelLaunches;
+    kernel<<<grid, block, smem, stream>>>(static_cast<KArgs>(args)...);
+}
+
+// Optional CUDA-event timing of one kernel family on the context's stream:
+// when enabled, launches of that family are bracketed by events from a
+// pool, read back after the timed region.
+enum ProfileKind { PROF_NONE = 0, PROF_SPMV = 1, PROF_TET = 2, PROF_TRI = 3, PROF_SLOT = 4, PROF_BARRIER = 5, PROF_ACTIVE = 6, PROF_FULLCCD = 7 };
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct InvalidArgument : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
+};
+
+// Grow-only device buffer.
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    void reserve(size_t n) {
+        if (n <= cap) return;
+        if (p) cudaFree(p);
+        size_t c = n < 64 ? 64 : n + n / 4;
+        CIPC_CUDA(cudaMalloc(&p, c * sizeof(T)));
+        cap = c;
+    }
+    void free() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+    operator T*() const { return p; }
+};
+
+// Scalars that kernels read (copied to the device once per change).
+struct SimParams {
+    double dt, drag, Hhat, Fhat, dTol, kappa, bboxDiag2, newtonThr, meanMass, avgEdge;
+    double friction, stretchS, shearS, strainRate, plateRigidity;
+    double groundN[3], groundD;
+    double softW;
+    int useBarrier, applyGravity, quasiStatic;
+};
+
+// Device LBVH over primitive boxes (faces or edges).  Node i < n-1 internal,
+// n-1 <= i < 2n-1 leaves in Morton order.
+struct DevBvh {
+    int n = 0;
+    DBuf<uint64_t> keys, keysAlt;
+    DBuf<int> left, right, parent, leafPrim, flags, escape;
+    DBuf<double> lo, hi;       // 3 per node
+    DBuf<double> primLo, primHi;  // 3 per primitive
+    DBuf<unsigned char> sortTmp;
+    DBuf<double> sceneBox;     // 6
+};
+
+struct Ctx {
+    // sizes
+    int nv = 0, nt = 0, nf = 0, nb = 0, nsf = 0, nsv = 0, nse = 0;
+    int mixed = 0;             // 0 FP64 Hessian/SpMV, 1 FP32
+    int precond = 0;           // 0 block-Jacobi, 1 learned
+    double pcgTol = 1e-6;
+    int pcgMaxIter = 10000;
+    SimParams P;
+    cudaStream_t s = nullptr;
+    std::string lastError;
+    int stepIndex = 0;
+
+    // host mirrors needed by the driver
+    std::vector<int> hBtype, hSoftIdx, hDirIdx;
+    std::vector<double> hRest;
+    int dirMotion = 0, softMotion = 0;
+    double dirRate = 0, softRate = 0;
+
+    // state (3*nv doubles unless noted)
+    DBuf<double> x, x0, xt, vp, vel, rest, dir, grad, mass, softTarget;
+    DBuf<int> btype, softIdx, dirIdx;
+    // topology and rest data
+    DBuf<int> tets, tris, bendV, faces, surfVerts, edges;
+    DBuf<double> DmInv, vol, tetMu, tetLam, DmInv2, area, bendQ;
+
+    // static symmetric BSR pattern (elements), full storage
+    int nnzb = 0;
+    DBuf<int> rowPtr, colIdx, diagSlot;
+    DBuf<int> hcPtr, hcIdx;    // per slot: element-block contributions (bit 31 = transpose)
+    DBuf<int> gcPtr, gcIdx;    // per vertex: element gradient contributions
+    DBuf<double> valD, constD;  // static values (FP64) and the constant bending part
+    DBuf<float> valF;
+    DBuf<double> elemHD;       // element lower blocks, 9 per block
+    DBuf<float> elemHF;
+    DBuf<double> elemG;        // element gradient rows, 3 per entry
+    int nElemBlocks = 0, nElemGrad = 0;
+    DBuf<double> vtxGrad, diagExtra;  // per-vertex accumulators (3 and 9 per vertex)
+
+    // contact sets
+    int nSelf = 0, nPT = 0, nEE = 0, nPPE = 0, nMoll = 0, nCcdPT = 0, nCcdEE = 0, nGround = 0;
+    long long nPPERaw = 0;
+    DBuf<int> selfActive;      // 4 per contact
+    DBuf<int> selfEE, eeIe;    // 4 and 2 per mollified contact
+    DBuf<uint64_t> ccdPT, ccdEE;
+    DBuf<int> ground;
+    DBuf<uint64_t> kPT, kEE, kMoll, kPPE, kTmp;
+    DBuf<uint64_t> uniq;
+    DBuf<int> counts, runs;
+    DBuf<int> counters;        // device counters for candidate emission
+    // friction (lagged at step start)
+    int nFric = 0, nFricG = 0;
+    DBuf<int> fricSet, fricGround;
+    DBuf<double> fricLambda, fricCoord, fricBasis, fricGLambda;
+    // close constraints for the kappa update
+    int nCloseG = 0, nCloseS = 0;
+    DBuf<int> closeG, closeS;
+    DBuf<double> closeGVal, closeSVal;
+
+    // dynamic (contact) contributions
+    int nDynG = 0, nDynH = 0, nDynB = 0;
+    DBuf<int> dynGKey, dynGKeyAlt, dynGIdx, dynGIdxAlt, dynGStart, dynGEnd;
+    DBuf<double> dynGVal;
+    DBuf<uint64_t> dynHKey, dynHKeyAlt;
+    DBuf<int> dynHIdx, dynHIdxAlt;
+    DBuf<double> dynHValD;
+    DBuf<float> dynHValF;
+    DBuf<int> dynRowStart, dynRowEnd, dynCol, dynSrcStart;
+    DBuf<double> dynBD;
+    DBuf<float> dynBF;
+    DBuf<unsigned char> sortTmp;
+
+    // PCG
+    DBuf<double> rhs, sol, r, z, p, Ap, Dinv, red;
+    DBuf<float> rF, zF, pF, ApF, xF, DinvF;
+    int lastPcgIters = 0;
+    double lastPcgRelRes = 0;
+    long long pcgItersTotal = 0;
+
+    // learned preconditioner factor (IC(0) pattern of the lower static+dynamic BSR)
+    DBuf<float> icVal;
+    bool icReady = false;
+
+    // collision structures
+    DevBvh faceTree, edgeTree;
+    DBuf<double> sweptPt;     // 6 per surface vertex
+    DBuf<double> scratch;     // reduction scratch
+    DBuf<int> status;
+    DBuf<double> scal;        // device scalars
+    DBuf<double> energyBuf;
+
+    // kernel-family timing (ProfileKind): event pairs recorded on c.s
+    int profKind = PROF_NONE;
+    std::vector<cudaEvent_t> profEv;
+    int profUsed = 0;
+};
+
+inline void profBegin(Ctx& c, int kind) {
+    if (c.profKind == kind && c.profUsed + 2 <= (int)c.profEv.size()) cudaEventRecord(c.profEv[c.profUsed], c.s);
+}
+inline void profEnd(Ctx& c, int kind) {
+    if (c.profKind == kind && c.profUsed + 2 <= (int)c.profEv.size()) {
+        cudaEventRecord(c.profEv[c.profUsed + 1], c.s);
+        c.profUsed += 2;
+    }
+}
+
+// ---- launchers (elastic.cu) ----
+void buildStaticPattern(Ctx& c, const std::vector<int>& tets, const std::vector<int>& tris, const std::vector<int>& bendV);
+void assembleElastic(Ctx& c);          // vtxGrad, diagExtra, element blocks, static BSR values, element gradient
+double elasticEnergy(Ctx& c);          // (SNH + BW + bending) * dt^2 + inertia + soft, FP64
+void gatherGradient(Ctx& c);           // grad = vtxGrad + element + dynamic contributions
+void initKappaGradE(Ctx& c, double* gE);  // inertia + tet elastic gradient into device buffer gE
+
+// ---- launchers (collision.cu) ----
+void buildBvh(Ctx& c, DevBvh& t, int n);
+void computeFaceBoxes(Ctx& c, const double* x, const double* d, double step, bool swept);
+void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, bool swept);
+void buildCollisionSets(Ctx& c, bool rehash);
+void groundActiveSet(Ctx& c);
+bool isIntersected(Ctx& c);
+double groundStepBound(Ctx& c);
+double partialCCD(Ctx& c, double alpha);
+double cflBound(Ctx& c);
+double fullCCD(Ctx& c, double alpha);
+void dirichletBound(Ctx& c, double& alpha);
+
+// ---- launchers (contact.cu) ----
+int contactAssemble(Ctx& c);           // barrier + mollified + friction gradient/Hessian -> dynamic lists; returns collisions
+double contactEnergy(Ctx& c, double kappa);
+void frictionInitialize(Ctx& c);
+void contactGradientKappa(Ctx& c, double* gc);  // ground + self barrier gradient with coefficient 1
+void closeConstraintCheck(Ctx& c, bool& update);
+void closeConstraintRecord(Ctx& c);
+void constraintMinMax(Ctx& c, double& mn, double& mx, bool& any);
+void finalizeDynamic(Ctx& c);          // sort + segment dynamic gradient and Hessian entries
+
+// ---- launchers (pcg.cu) ----
+int pcgSolve(Ctx& c);                  // solves A sol = rhs; returns iterations
+void spmv(Ctx& c, const double* x, double* y);
+void buildRhs(Ctx& c);
+
+// ---- reductions (util.cu) ----
+double deviceSum(Ctx& c, const double* v, int n);
+double deviceMax(Ctx& c, const double* v, int n);
+double deviceMin(Ctx& c, const double* v, int n, double init);
+double deviceDot(Ctx& c, const double* a, const double* b, int n);
+double deviceInfNorm(Ctx& c, const double* v, int n);
+void checkStatus(Ctx& c, const char* stage);
+
+}  // namespace cipc

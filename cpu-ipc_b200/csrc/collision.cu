@@ -1,0 +1,682 @@
+// Broad phase and step bounds on the GPU.
+//
+// * LBVH build: primitive boxes -> scene box -> 30-bit Morton keys with the
+//   primitive id in the low word -> radix sort -> Karras internal nodes ->
+//   bottom-up boxes (first-arrival flags).  Topology follows
+//   CPULinearBVH::build, CPU IPC/LBVH.cpp:163-250.
+// * Active sets: one thread per query traverses the tree with the inclusive
+//   overlaps(gap) test (LBVH.cpp:157-161), applies the collider / incidence
+//   filters of SpatialHash::calculateActivateSet
+//   (CPU IPC/CollisionBroadPhase.cpp:765-1059), classifies and emits 64-bit
+//   pair keys.  Keys are radix-sorted, so every list comes out in the
+//   reference's order (query ascending, then primitive ascending); PP/PE
+//   duplicates are merged by sort + run-length encoding, the job of the
+//   reference's std::map.
+// * Partial CCD, full (swept) CCD, ground bound, CFL bound and the
+//   edge-triangle intersection test (IPCSolver.cpp:476-542, 943-990;
+//   ContactMechanics.cpp:3704-3867; FeasibleStep.cpp:8-40).
+#include "cipc_internal.h"
+#include "geometry.cuh"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+namespace cipc {
+
+namespace {
+
+constexpr int TB = 128;
+inline int blocksFor(int n, int tb = TB) { return std::max(1, std::min((n + tb - 1) / tb, 148 * 32)); }
+
+__device__ __forceinline__ void boxInit(double lo[3], double hi[3]) {
+    for (int k = 0; k < 3; ++k) { lo[k] = 1.7976931348623157e308; hi[k] = -1.7976931348623157e308; }
+}
+__device__ __forceinline__ void boxAdd(double lo[3], double hi[3], d3 p) {
+    lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
+    hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
+}
+// (query lo, hi).overlaps(node lo, hi, gap), inclusive.
+__device__ __forceinline__ bool overlaps(const double* qlo, const double* qhi, const double* nlo, const double* nhi, double gap) {
+    return !((nlo[0] - qhi[0] > gap) || (nlo[1] - qhi[1] > gap) || (nlo[2] - qhi[2] > gap) || (qlo[0] - nhi[0] > gap) ||
+             (qlo[1] - nhi[1] > gap) || (qlo[2] - nhi[2] > gap));
+}
+
+// Swept point box: combine(p) then combine(p - step * d).
+__device__ __forceinline__ void sweptAdd(double lo[3], double hi[3], d3 p, d3 d, double step) {
+    boxAdd(lo, hi, p);
+    boxAdd(lo, hi, p - step * d);
+}
+
+__global__ void faceBoxKernel(int n, const int* faces, const double* x, const double* d, double step, int swept, double* lo, double* hi) {
+    CIPC_KERNEL_LOOP(f, n) {
+        double l[3], h[3];
+        boxInit(l, h);
+        for (int k = 0; k < 3; ++k) {
+            int v = faces[3 * f + k];
+            if (swept) sweptAdd(l, h, ld3(x, v), ld3(d, v), step);
+            else boxAdd(l, h, ld3(x, v));
+        }
+        for (int k = 0; k < 3; ++k) { lo[3 * f + k] = l[k]; hi[3 * f + k] = h[k]; }
+    }
+}
+__global__ void edgeBoxKernel(int n, const int* edges, const double* x, const double* d, double step, int swept, double* lo, double* hi) {
+    CIPC_KERNEL_LOOP(e, n) {
+        double l[3], h[3];
+        boxInit(l, h);
+        for (int k = 0; k < 2; ++k) {
+            int v = edges[2 * e + k];
+            if (swept) sweptAdd(l, h, ld3(x, v), ld3(d, v), step);
+            else boxAdd(l, h, ld3(x, v));
+        }
+        for (int k = 0; k < 3; ++k) { lo[3 * e + k] = l[k]; hi[3 * e + k] = h[k]; }
+    }
+}
+
+__global__ void sceneBoxKernel(int n, const double* lo, const double* hi, double* out) {
+    double l[3], h[3];
+    boxInit(l, h);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int k = 0; k < 3; ++k) { l[k] = fmin(l[k], lo[3 * i + k]); h[k] = fmax(h[k], hi[3 * i + k]); }
+    for (int k = 0; k < 3; ++k) {
+        l[k] = blockReduce(l[k], MinOp(), 1.7976931348623157e308);
+        __syncthreads();
+        h[k] = blockReduce(h[k], MaxOp(), -1.7976931348623157e308);
+        __syncthreads();
+        if (threadIdx.x == 0) { out[k] = l[k]; out[3 + k] = h[k]; }
+    }
+}
+
+__device__ __forceinline__ uint32_t expandBits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t quantize(double v) {
+    v = fmax(0.0, fmin(v * 1024.0, 1023.0));
+    return (uint32_t)v;
+}
+
+__global__ void mortonKernel(int n, const double* lo, const double* hi, const double* scene, uint64_t* keys) {
+    CIPC_KERNEL_LOOP(i, n) {
+        double c[3], q[3];
+        for (int k = 0; k < 3; ++k) {
+            c[k] = 0.5 * (lo[3 * i + k] + hi[3 * i + k]);
+            double ext = scene[3 + k] - scene[k];
+            double off = c[k] - scene[k];
+            q[k] = ext > 0.0 ? off / ext : 0.0;
+        }
+        uint32_t code = (expandBits(quantize(q[0])) << 2) | (expandBits(quantize(q[1])) << 1) | expandBits(quantize(q[2]));
+        keys[i] = ((uint64_t)code << 32) | (uint32_t)i;
+    }
+}
+
+__device__ __forceinline__ int prefixLen(const uint64_t* k, int n, int a, int b) {
+    if (b < 0 || b >= n) return -1;
+    uint64_t x = k[a] ^ k[b];
+    return x == 0 ? 64 : __clzll(x);
+}
+
+__global__ void karrasKernel(int n, const uint64_t* keys, int* left, int* right, int* parent) {
+    CIPC_KERNEL_LOOP(in, n - 1) {
+        int first, last;
+        if (in == 0) { first = 0; last = n - 1; }
+        else {
+            int lp = prefixLen(keys, n, in, in - 1), rp = prefixLen(keys, n, in, in + 1);
+            int dir = rp > lp ? 1 : -1;
+            int minp = min(lp, rp);
+            int maxLen = 2;
+            while (prefixLen(keys, n, in, in + dir * maxLen) > minp) maxLen <<= 1;
+            int len = 0;
+            for (int step = maxLen >> 1; step > 0; step >>= 1)
+                if (prefixLen(keys, n, in, in + dir * (len + step)) > minp) len += step;
+            int other = in + dir * len;
+            first = min(in, other); last = max(in, other);
+        }
+        int split;
+        uint64_t fc = keys[first], lc = keys[last];
+        if (fc == lc) split = (first + last) >> 1;
+        else {
+            int common = __clzll(fc ^ lc);
+            split = first;
+            unsigned step = (unsigned)(last - first);
+            do {
+                step = (step + 1) >> 1;
+                int cand = split + (int)step;
+                if (cand < last && __clzll(fc ^ keys[cand]) > common) split = cand;
+            } while (step > 1);
+        }
+        int l = split, r = split + 1;
+        if (split == first) l += n - 1;
+        if (split + 1 == last) r += n - 1;
+        left[in] = l; right[in] = r;
+        parent[l] = in; parent[r] = in;
+    }
+}
+
+__global__ void leafKernel(int n, const uint64_t* keys, const double* plo, const double* phi, int* leafPrim, double* lo, double* hi,
+                           int* flags, int* parent) {
+    CIPC_KERNEL_LOOP(s, n) {
+        int prim = (int)(keys[s] & 0xffffffffu);
+        leafPrim[s] = prim;
+        int node = s + n - 1;
+        for (int k = 0; k < 3; ++k) { lo[3 * node + k] = plo[3 * prim + k]; hi[3 * node + k] = phi[3 * prim + k]; }
+        if (s < n - 1) flags[s] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) parent[0] = -1;
+}
+
+// Bottom-up box merge: the second child to arrive at a node combines both
+// child boxes (left first, then right, as the reference's post-order merge).
+__global__ void refitKernel(int n, const int* left, const int* right, const int* parent, double* lo, double* hi, int* flags) {
+    CIPC_KERNEL_LOOP(s, n) {
+        int node = s + n - 1;
+        int p = parent[node];
+        for (int guard = 0; guard < 64 && p >= 0; ++guard) {
+            __threadfence();
+            if (atomicAdd(&flags[p], 1) == 0) break;
+            __threadfence();
+            int l = left[p], r = right[p];
+            for (int k = 0; k < 3; ++k) {
+                // L2 loads (__ldcg): a child box written by another SM must
+                // not be served from a stale L1 line.
+                double a = fmin(1.7976931348623157e308, __ldcg(&lo[3 * l + k]));
+                a = fmin(a, __ldcg(&lo[3 * r + k]));
+                double b = fmax(-1.7976931348623157e308, __ldcg(&hi[3 * l + k]));
+                b = fmax(b, __ldcg(&hi[3 * r + k]));
+                lo[3 * p + k] = a; hi[3 * p + k] = b;
+            }
+            node = p;
+            p = parent[node];
+        }
+    }
+}
+
+struct BvhView {
+    int n;
+    const int *left, *right, *leafPrim;
+    const double *lo, *hi;
+};
+BvhView view(const DevBvh& t) { return BvhView{t.n, t.left, t.right, t.leafPrim, t.lo, t.hi}; }
+
+// Depth-first traversal (right pushed before left, as the reference); calls
+// f(prim) for every leaf whose box overlaps the query box with the gap.
+template <class F>
+__device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, const double* qhi, double gap, int* status, F f) {
+    if (t.n <= 0) return;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        int node = stack[--sp];
+        if (!overlaps(qlo, qhi, t.lo + 3 * node, t.hi + 3 * node, gap)) continue;
+        if (node >= t.n - 1) { f(t.leafPrim[node - (t.n - 1)]); continue; }
+        if (sp + 2 > 64) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
+        stack[sp++] = t.right[node];
+        stack[sp++] = t.left[node];
+    }
+}
+
+__device__ __forceinline__ bool isCollider(int t) { return t >= 2; }
+
+// Packed PP/PE key: lexicographic order of (c0 = -v-1, c1, c2) with c3 = -1.
+constexpr uint64_t M21 = (1ull << 21) - 1;
+__device__ __forceinline__ uint64_t ppeKey(int c0, int c1, int c2) {
+    uint64_t v = (uint64_t)(-c0 - 1);
+    return ((M21 - v) << 42) | ((uint64_t)c1 << 21) | (uint64_t)(c2 + 1);
+}
+
+struct Emit {
+    uint64_t* buf;
+    int cap;
+    int* counter;
+    __device__ void operator()(uint64_t k, int* status) const {
+        int i = atomicAdd(counter, 1);
+        if (i < cap) buf[i] = k;
+        else raiseStatus(status, CIPC_ST_CAPACITY);
+    }
+};
+
+__global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, BvhView tree, double sq,
+                               double Hhat, Emit ccd, Emit ptk, Emit ppe, int* status) {
+    CIPC_KERNEL_LOOP(svI, nsv) {
+        int vI = surfVerts[svI];
+        d3 p = ld3(x, vI);
+        double lo[3] = {p.x, p.y, p.z};
+        traverse(tree, lo, lo, sq, status, [&](int sfI) {
+            int f0 = faces[3 * sfI], f1 = faces[3 * sfI + 1], f2 = faces[3 * sfI + 2];
+            if (isCollider(btype[vI]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
+            if (vI == f0 || vI == f1 || vI == f2) return;
+            ccd(((uint64_t)svI << 32) | (uint32_t)sfI, status);
+            d3 a = ld3(x, f0), b = ld3(x, f1), c = ld3(x, f2);
+            int t = dTypePT(p, a, b, c);
+            double d;
+            switch (t) {
+            case 0: d = dPP(p, a); if (d < Hhat) ppe(ppeKey(-vI - 1, f0, -1), status); break;
+            case 1: d = dPP(p, b); if (d < Hhat) ppe(ppeKey(-vI - 1, f1, -1), status); break;
+            case 2: d = dPP(p, c); if (d < Hhat) ppe(ppeKey(-vI - 1, f2, -1), status); break;
+            case 3: d = dPE(p, a, b); if (d < Hhat) ppe(ppeKey(-vI - 1, f0, f1), status); break;
+            case 4: d = dPE(p, b, c); if (d < Hhat) ppe(ppeKey(-vI - 1, f1, f2), status); break;
+            case 5: d = dPE(p, c, a); if (d < Hhat) ppe(ppeKey(-vI - 1, f2, f0), status); break;
+            default: d = dPT(p, a, b, c); if (d < Hhat) ptk(((uint64_t)svI << 32) | (uint32_t)sfI, status); break;
+            }
+        });
+    }
+}
+
+__global__ void activeEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* rest, BvhView tree, double sq,
+                               double Hhat, Emit ccd, Emit eek, Emit moll, Emit ppe, int* status) {
+    CIPC_KERNEL_LOOP(eI, ne) {
+        int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
+        d3 p0 = ld3(x, e0), p1 = ld3(x, e1);
+        double lo[3], hi[3];
+        boxInit(lo, hi);
+        boxAdd(lo, hi, p0); boxAdd(lo, hi, p1);
+        traverse(tree, lo, hi, sq, status, [&](int eJ) {
+            if (eJ <= eI) return;
+            int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
+            if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[g0]) && isCollider(btype[g1])) return;
+            if (e0 == g0 || e0 == g1 || e1 == g0 || e1 == g1) return;
+            ccd(((uint64_t)eI << 32) | (uint32_t)eJ, status);
+            d3 q0 = ld3(x, g0), q1 = ld3(x, g1);
+            int t = dTypeEE(p0, p1, q0, q1);
+            double cs = crossSqNormEE(p0, p1, q0, q1);
+            double ex = 1e-3 * sqn(ld3(rest, e0) - ld3(rest, e1)) * sqn(ld3(rest, g0) - ld3(rest, g1));
+            bool mol = cs < ex;
+            double d;
+            int c0 = 0, c1 = 0, c2 = -1;
+            switch (t) {
+            case 0: d = dPP(p0, q0); c0 = -e0 - 1; c1 = g0; break;
+            case 1: d = dPP(p0, q1); c0 = -e0 - 1; c1 = g1; break;
+            case 2: d = dPE(p0, q0, q1); c0 = -e0 - 1; c1 = g0; c2 = g1; break;
+            case 3: d = dPP(p1, q0); c0 = -e1 - 1; c1 = g0; break;
+            case 4: d = dPP(p1, q1); c0 = -e1 - 1; c1 = g1; break;
+            case 5: d = dPE(p1, q0, q1); c0 = -e1 - 1; c1 = g0; c2 = g1; break;
+            case 6: d = dPE(q0, p0, p1); c0 = -g0 - 1; c1 = e0; c2 = e1; break;
+            case 7: d = dPE(q1, p0, p1); c0 = -g1 - 1; c1 = e0; c2 = e1; break;
+            default: d = dEE(p0, p1, q0, q1); break;
+            }
+            if (!(d < Hhat)) return;
+            if (mol) moll(((uint64_t)eI << 34) | ((uint64_t)eJ << 4) | (uint64_t)t, status);
+            else if (t == 8) eek(((uint64_t)eI << 32) | (uint32_t)eJ, status);
+            else ppe(ppeKey(c0, c1, c2), status);
+        });
+    }
+}
+
+__global__ void decodeSelfKernel(int nPT, int nEE, int nPPE, const uint64_t* kPT, const uint64_t* kEE, const uint64_t* uniq, const int* counts,
+                                 const int* surfVerts, const int* faces, const int* edges, int* out) {
+    int n = nPT + nEE + nPPE;
+    CIPC_KERNEL_LOOP(i, n) {
+        int c[4];
+        if (i < nPT) {
+            int svI = (int)(kPT[i] >> 32), sfI = (int)(kPT[i] & 0xffffffffu);
+            c[0] = -surfVerts[svI] - 1; c[1] = faces[3 * sfI]; c[2] = faces[3 * sfI + 1]; c[3] = faces[3 * sfI + 2];
+        } else if (i < nPT + nEE) {
+            uint64_t k = kEE[i - nPT];
+            int eI = (int)(k >> 32), eJ = (int)(k & 0xffffffffu);
+            c[0] = edges[2 * eI]; c[1] = edges[2 * eI + 1]; c[2] = edges[2 * eJ]; c[3] = edges[2 * eJ + 1];
+        } else {
+            int j = i - nPT - nEE;
+            uint64_t k = uniq[j];
+            int v = (int)(M21 - (k >> 42));
+            c[0] = -v - 1; c[1] = (int)((k >> 21) & M21); c[2] = (int)(k & M21) - 1; c[3] = -counts[j];
+        }
+        for (int q = 0; q < 4; ++q) out[4 * i + q] = c[q];
+    }
+}
+
+__global__ void decodeMollKernel(int n, const uint64_t* k, const int* edges, int* selfEE, int* eeIe) {
+    CIPC_KERNEL_LOOP(i, n) {
+        uint64_t key = k[i];
+        int eI = (int)(key >> 34), eJ = (int)((key >> 4) & ((1u << 30) - 1)), t = (int)(key & 15);
+        int e0 = edges[2 * eI], e1 = edges[2 * eI + 1], g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
+        int c[4] = {0, 0, -1, -1};
+        switch (t) {
+        case 0: c[0] = -e0 - 1; c[1] = g0; break;
+        case 1: c[0] = -e0 - 1; c[1] = g1; break;
+        case 2: c[0] = -e0 - 1; c[1] = g0; c[2] = g1; break;
+        case 3: c[0] = -e1 - 1; c[1] = g0; break;
+        case 4: c[0] = -e1 - 1; c[1] = g1; break;
+        case 5: c[0] = -e1 - 1; c[1] = g0; c[2] = g1; break;
+        case 6: c[0] = -g0 - 1; c[1] = e0; c[2] = e1; break;
+        case 7: c[0] = -g1 - 1; c[1] = e0; c[2] = e1; break;
+        default: c[0] = e0; c[1] = e1; c[2] = g0; c[3] = g1; break;
+        }
+        for (int q = 0; q < 4; ++q) selfEE[4 * i + q] = c[q];
+        eeIe[2 * i] = t == 8 ? -1 : eI;
+        eeIe[2 * i + 1] = t == 8 ? -1 : eJ;
+    }
+}
+
+__global__ void groundFlagKernel(int nsv, const int* surfVerts, const double* x, double nx, double ny, double nz, double D, double Hhat, int* flags) {
+    CIPC_KERNEL_LOOP(i, nsv) {
+        d3 p = ld3(x, surfVerts[i]);
+        double dist = nx * p.x + ny * p.y + nz * p.z - D;
+        flags[i] = dist * dist < Hhat ? 1 : 0;
+    }
+}
+
+// ---- step bounds ----
+__global__ void groundBoundKernel(int nsv, const int* surfVerts, const double* x, const double* dir, double nx, double ny, double nz, double D,
+                                  double slack, double* out) {
+    CIPC_KERNEL_LOOP(i, nsv) {
+        int v = surfVerts[i];
+        d3 p = ld3(x, v), d = ld3(dir, v);
+        double r = 1.0;
+        double nm = nx * -d.x + ny * -d.y + nz * -d.z;
+        if (nm < 0.0) {
+            double dist = nx * p.x + ny * p.y + nz * p.z - D;
+            double cand = -dist / nm * slack;
+            if (cand >= 0.0) r = cand;
+        }
+        out[i] = r;
+    }
+}
+
+__global__ void surfMoveKernel(int nsv, const int* surfVerts, const double* dir, double* out) {
+    CIPC_KERNEL_LOOP(i, nsv) out[i] = sqrt(sqn(ld3(dir, surfVerts[i])));
+}
+
+__global__ void partialCCDKernel(int nPT, int nEE, const uint64_t* ccdPT, const uint64_t* ccdEE, const int* surfVerts, const int* faces,
+                                 const int* edges, const double* x, const double* dir, double eta, double* out, int* status) {
+    CIPC_KERNEL_LOOP(i, nPT + nEE) {
+        double a;
+        if (i < nPT) {
+            int svI = (int)(ccdPT[i] >> 32), sfI = (int)(ccdPT[i] & 0xffffffffu);
+            int p = surfVerts[svI], f0 = faces[3 * sfI], f1 = faces[3 * sfI + 1], f2 = faces[3 * sfI + 2];
+            a = pointTriangleCCD(ld3(x, p), ld3(x, f0), ld3(x, f1), ld3(x, f2), -ld3(dir, p), -ld3(dir, f0), -ld3(dir, f1), -ld3(dir, f2), eta, status);
+        } else {
+            uint64_t k = ccdEE[i - nPT];
+            int eI = (int)(k >> 32), eJ = (int)(k & 0xffffffffu);
+            int a0 = edges[2 * eI], a1 = edges[2 * eI + 1], b0 = edges[2 * eJ], b1 = edges[2 * eJ + 1];
+            a = edgeEdgeCCD(ld3(x, a0), ld3(x, a1), ld3(x, b0), ld3(x, b1), -ld3(dir, a0), -ld3(dir, a1), -ld3(dir, b0), -ld3(dir, b1), eta, status);
+        }
+        out[i] = a;
+    }
+}
+
+__global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, const double* dir, double step,
+                             BvhView tree, double eta, double* out, int* status) {
+    CIPC_KERNEL_LOOP(svI, nsv) {
+        int vI = surfVerts[svI];
+        d3 p = ld3(x, vI), dp = ld3(dir, vI);
+        double lo[3], hi[3];
+        boxInit(lo, hi);
+        sweptAdd(lo, hi, p, dp, step);
+        double best = 1.0;
+        traverse(tree, lo, hi, 0.0, status, [&](int sfI) {
+            int f0 = faces[3 * sfI], f1 = faces[3 * sfI + 1], f2 = faces[3 * sfI + 2];
+            if (isCollider(btype[vI]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
+            if (vI == f0 || vI == f1 || vI == f2) return;
+            double a = pointTriangleCCD(p, ld3(x, f0), ld3(x, f1), ld3(x, f2), -dp, -ld3(dir, f0), -ld3(dir, f1), -ld3(dir, f2), eta, status);
+            best = fmin(a, best);
+        });
+        out[svI] = best;
+    }
+}
+
+__global__ void fullEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* dir, const double* treeBoxLo,
+                             const double* treeBoxHi, double eeStep, BvhView tree, double eta, double* out, int* status) {
+    CIPC_KERNEL_LOOP(eJ, ne) {
+        int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
+        d3 q0 = ld3(x, g0), q1 = ld3(x, g1), dq0 = ld3(dir, g0), dq1 = ld3(dir, g1);
+        double qlo[3], qhi[3];
+        for (int k = 0; k < 3; ++k) { qlo[k] = treeBoxLo[3 * eJ + k]; qhi[k] = treeBoxHi[3 * eJ + k]; }
+        double blo[3], bhi[3];
+        boxInit(blo, bhi);
+        sweptAdd(blo, bhi, q0, dq0, eeStep);
+        sweptAdd(blo, bhi, q1, dq1, eeStep);
+        double best = 1.0;
+        traverse(tree, qlo, qhi, 0.0, status, [&](int eI) {
+            if (eI <= eJ) return;
+            int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
+            if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[g0]) && isCollider(btype[g1])) return;
+            if (e0 == g0 || e0 == g1 || e1 == g0 || e1 == g1) return;
+            d3 p0 = ld3(x, e0), p1 = ld3(x, e1), dp0 = ld3(dir, e0), dp1 = ld3(dir, e1);
+            double clo[3], chi[3];
+            boxInit(clo, chi);
+            sweptAdd(clo, chi, p0, dp0, eeStep);
+            sweptAdd(clo, chi, p1, dp1, eeStep);
+            if (!overlaps(blo, bhi, clo, chi, 0.0)) return;
+            double a = edgeEdgeCCD(p0, p1, q0, q1, -dp0, -dp1, -dq0, -dq1, eta, status);
+            best = fmin(a, best);
+        });
+        out[eJ] = best;
+    }
+}
+
+__global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, BvhView tree, int* flag, int* status) {
+    CIPC_KERNEL_LOOP(f, nsf) {
+        int f0 = faces[3 * f], f1 = faces[3 * f + 1], f2 = faces[3 * f + 2];
+        d3 a = ld3(x, f0), b = ld3(x, f1), c = ld3(x, f2);
+        double lo[3], hi[3];
+        boxInit(lo, hi);
+        boxAdd(lo, hi, a); boxAdd(lo, hi, b); boxAdd(lo, hi, c);
+        bool hit = false;
+        traverse(tree, lo, hi, 0.0, status, [&](int e) {
+            if (hit) return;
+            int e0 = edges[2 * e], e1 = edges[2 * e + 1];
+            if (e0 == f0 || e0 == f1 || e0 == f2 || e1 == f0 || e1 == f1 || e1 == f2) return;
+            if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
+            if (segTriIntersect(ld3(x, e0), ld3(x, e1), a, b, c)) hit = true;
+        });
+        if (hit) atomicOr(flag, 1);
+    }
+}
+
+__global__ void groundIntersectKernel(int n, const int* ground, const double* x, double nx, double ny, double nz, double D, int* flag) {
+    CIPC_KERNEL_LOOP(i, n) {
+        d3 p = ld3(x, ground[i]);
+        double dist = nx * p.x + ny * p.y + nz * p.z - D;
+        if (dist * dist <= 0.0) atomicOr(flag, 1);
+    }
+}
+
+void sortKeys(Ctx& c, uint64_t* in, uint64_t* tmp, int n, int endBit) {
+    if (n <= 1) return;
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, in, tmp, n, 0, endBit, c.s);
+    c.sortTmp.reserve(bytes + 16);
+    CIPC_CUDA(cub::DeviceRadixSort::SortKeys(c.sortTmp.p, bytes, in, tmp, n, 0, endBit, c.s));
+    CIPC_CUDA(cudaMemcpyAsync(in, tmp, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, c.s));
+}
+
+}  // namespace
+
+void computeFaceBoxes(Ctx& c, const double* x, const double* d, double step, bool swept) {
+    c.faceTree.primLo.reserve(3 * std::max(1, c.nsf));
+    c.faceTree.primHi.reserve(3 * std::max(1, c.nsf));
+    if (c.nsf) launch(faceBoxKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, x, d, step, swept, c.faceTree.primLo, c.faceTree.primHi);
+}
+void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, bool swept) {
+    c.edgeTree.primLo.reserve(3 * std::max(1, c.nse));
+    c.edgeTree.primHi.reserve(3 * std::max(1, c.nse));
+    if (c.nse) launch(edgeBoxKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, x, d, step, swept, c.edgeTree.primLo, c.edgeTree.primHi);
+}
+
+void buildBvh(Ctx& c, DevBvh& t, int n) {
+    t.n = n;
+    if (n <= 0) return;
+    int nn = 2 * n - 1;
+    t.keys.reserve(n); t.keysAlt.reserve(n);
+    t.left.reserve(nn); t.right.reserve(nn); t.parent.reserve(nn); t.leafPrim.reserve(n); t.flags.reserve(n);
+    t.lo.reserve(3 * nn); t.hi.reserve(3 * nn); t.sceneBox.reserve(6);
+    launch(sceneBoxKernel, 1, 1024, 0, c.s, n, t.primLo, t.primHi, t.sceneBox);
+    launch(mortonKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, t.sceneBox, t.keys);
+    sortKeys(c, t.keys, t.keysAlt, n, 64);
+    if (n > 1) launch(karrasKernel, blocksFor(n - 1), TB, 0, c.s, n, t.keys, t.left, t.right, t.parent);
+    launch(leafKernel, blocksFor(n), TB, 0, c.s, n, t.keys, t.primLo, t.primHi, t.leafPrim, t.lo, t.hi, t.flags, t.parent);
+    if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, t.left, t.right, t.parent, t.lo, t.hi, t.flags);
+    CIPC_CUDA(cudaGetLastError());
+}
+
+static void buildStaticTrees(Ctx& c) {
+    computeFaceBoxes(c, c.x, c.x, 0.0, false);
+    buildBvh(c, c.faceTree, c.nsf);
+    computeEdgeBoxes(c, c.x, c.x, 0.0, false);
+    buildBvh(c, c.edgeTree, c.nse);
+}
+
+void groundActiveSet(Ctx& c) {
+    c.ground.reserve(std::max(1, c.nsv));
+    c.counts.reserve(std::max(1, c.nsv) + 1);
+    if (c.nsv == 0) { c.nGround = 0; return; }
+    launch(groundFlagKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.x, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2], c.P.groundD,
+                                                       c.P.Hhat, c.counts);
+    size_t bytes = 0;
+    c.counters.reserve(16);
+    cub::DeviceSelect::Flagged(nullptr, bytes, c.surfVerts.p, c.counts.p, c.ground.p, c.counters.p + 15, c.nsv, c.s);
+    c.sortTmp.reserve(bytes + 16);
+    CIPC_CUDA(cub::DeviceSelect::Flagged(c.sortTmp.p, bytes, c.surfVerts.p, c.counts.p, c.ground.p, c.counters.p + 15, c.nsv, c.s));
+    int n = 0;
+    CIPC_CUDA(cudaMemcpyAsync(&n, c.counters.p + 15, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    c.nGround = n;
+}
+
+// SpatialHash::calculateActivateSet with the LBVH backend, then
+// Ground::calculateActivateSet (IPCSolver.cpp:544-556).
+void buildCollisionSets(Ctx& c, bool rehash) {
+    if (c.P.useBarrier) {
+        if (rehash) buildStaticTrees(c);
+        double sq = sqrt(c.P.Hhat);
+        int caps[6] = {(int)std::max<size_t>(c.ccdPT.cap, 1024), (int)std::max<size_t>(c.kPT.cap, 1024), (int)std::max<size_t>(c.kPPE.cap, 1024),
+                       (int)std::max<size_t>(c.ccdEE.cap, 1024), (int)std::max<size_t>(c.kEE.cap, 1024), (int)std::max<size_t>(c.kMoll.cap, 1024)};
+        int cnt[6];
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            c.ccdPT.reserve(caps[0]); c.kPT.reserve(caps[1]); c.kPPE.reserve(caps[2]);
+            c.ccdEE.reserve(caps[3]); c.kEE.reserve(caps[4]); c.kMoll.reserve(caps[5]);
+            c.counters.reserve(16);
+            CIPC_CUDA(cudaMemsetAsync(c.counters.p, 0, 8 * sizeof(int), c.s));
+            Emit eCcdPT{c.ccdPT, caps[0], c.counters.p + 0}, ePT{c.kPT, caps[1], c.counters.p + 1}, ePPE{c.kPPE, caps[2], c.counters.p + 2};
+            Emit eCcdEE{c.ccdEE, caps[3], c.counters.p + 3}, eEE{c.kEE, caps[4], c.counters.p + 4}, eMoll{c.kMoll, caps[5], c.counters.p + 5};
+            profBegin(c, PROF_ACTIVE);
+            if (c.nsv)
+                launch(activePTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, view(c.faceTree), sq, c.P.Hhat,
+                                                                  eCcdPT, ePT, ePPE, c.status);
+            if (c.nse)
+                launch(activeEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.rest, view(c.edgeTree), sq, c.P.Hhat, eCcdEE,
+                                                                  eEE, eMoll, ePPE, c.status);
+            profEnd(c, PROF_ACTIVE);
+            CIPC_CUDA(cudaGetLastError());
+            CIPC_CUDA(cudaMemcpyAsync(cnt, c.counters.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
+            CIPC_CUDA(cudaStreamSynchronize(c.s));
+            bool ok = true;
+            for (int k = 0; k < 6; ++k)
+                if (cnt[k] > caps[k]) { caps[k] = cnt[k] + cnt[k] / 2 + 1024; ok = false; }
+            if (ok) break;
+            int st = 0;  // clear the capacity bit before retrying
+            CIPC_CUDA(cudaMemcpyAsync(c.status.p, &st, sizeof(int), cudaMemcpyHostToDevice, c.s));
+        }
+        checkStatus(c, "active set");
+        c.nCcdPT = cnt[0]; c.nPT = cnt[1]; c.nPPERaw = cnt[2]; c.nCcdEE = cnt[3]; c.nEE = cnt[4]; c.nMoll = cnt[5];
+        int mx = std::max(std::max(std::max(cnt[0], cnt[1]), std::max(cnt[2], cnt[3])), std::max(cnt[4], cnt[5]));
+        c.kTmp.reserve(std::max(mx, 1));
+        sortKeys(c, c.ccdPT, c.kTmp, cnt[0], 64);
+        sortKeys(c, c.kPT, c.kTmp, cnt[1], 64);
+        sortKeys(c, c.kPPE, c.kTmp, cnt[2], 63);
+        sortKeys(c, c.ccdEE, c.kTmp, cnt[3], 64);
+        sortKeys(c, c.kEE, c.kTmp, cnt[4], 64);
+        sortKeys(c, c.kMoll, c.kTmp, cnt[5], 64);
+        // merge PP/PE duplicates (multiplicity)
+        int nu = 0;
+        c.uniq.reserve(std::max(cnt[2], 1));
+        c.runs.reserve(std::max(cnt[2], 1));
+        if (cnt[2] > 0) {
+            size_t bytes = 0;
+            cub::DeviceRunLengthEncode::Encode(nullptr, bytes, c.kPPE.p, c.uniq.p, c.runs.p, c.counters.p + 6, cnt[2], c.s);
+            c.sortTmp.reserve(bytes + 16);
+            CIPC_CUDA(cub::DeviceRunLengthEncode::Encode(c.sortTmp.p, bytes, c.kPPE.p, c.uniq.p, c.runs.p, c.counters.p + 6, cnt[2], c.s));
+            CIPC_CUDA(cudaMemcpyAsync(&nu, c.counters.p + 6, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+            CIPC_CUDA(cudaStreamSynchronize(c.s));
+        }
+        c.nPPE = nu;
+        c.nSelf = c.nPT + c.nEE + c.nPPE;
+        c.selfActive.reserve(4 * std::max(c.nSelf, 1));
+        if (c.nSelf)
+            launch(decodeSelfKernel, blocksFor(c.nSelf), TB, 0, c.s, c.nPT, c.nEE, c.nPPE, c.kPT, c.kEE, c.uniq, c.runs, c.surfVerts, c.faces, c.edges,
+                                                                 c.selfActive);
+        c.selfEE.reserve(4 * std::max(c.nMoll, 1));
+        c.eeIe.reserve(2 * std::max(c.nMoll, 1));
+        if (c.nMoll) launch(decodeMollKernel, blocksFor(c.nMoll), TB, 0, c.s, c.nMoll, c.kMoll, c.edges, c.selfEE, c.eeIe);
+        CIPC_CUDA(cudaGetLastError());
+    }
+    groundActiveSet(c);
+}
+
+bool isIntersected(Ctx& c) {
+    c.counters.reserve(16);
+    CIPC_CUDA(cudaMemsetAsync(c.counters.p + 7, 0, sizeof(int), c.s));
+    if (c.nGround)
+        launch(groundIntersectKernel, blocksFor(c.nGround), TB, 0, c.s, c.nGround, c.ground, c.x, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2],
+                                                                   c.P.groundD, c.counters.p + 7);
+    if (c.nsf) launch(intersectKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, view(c.edgeTree), c.counters.p + 7, c.status);
+    int f = 0;
+    CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    checkStatus(c, "intersection test");
+    return f != 0;
+}
+
+// Rebuild the static trees at the current positions (sh.build in the line search).
+void rebuildTrees(Ctx& c) { buildStaticTrees(c); }
+
+double groundStepBound(Ctx& c) {
+    if (c.nsv == 0) return 1.0;
+    c.energyBuf.reserve(std::max(c.nsv, 1));
+    launch(groundBoundKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.x, c.dir, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2], c.P.groundD,
+                                                        0.8, c.energyBuf);
+    return deviceMin(c, c.energyBuf, c.nsv, 1e308);
+}
+
+double partialCCD(Ctx& c, double alpha) {
+    int n = c.nCcdPT + c.nCcdEE;
+    if (n == 0) return alpha;
+    c.energyBuf.reserve(n);
+    launch(partialCCDKernel, blocksFor(n), TB, 0, c.s, c.nCcdPT, c.nCcdEE, c.ccdPT, c.ccdEE, c.surfVerts, c.faces, c.edges, c.x, c.dir, 1.0 - 0.8,
+                                                  c.energyBuf, c.status);
+    double mn = deviceMin(c, c.energyBuf, n, 1e308);
+    checkStatus(c, "partial CCD");
+    return std::min(alpha, mn);
+}
+
+double cflBound(Ctx& c) {
+    if (c.nsv == 0) return 1.0;
+    c.energyBuf.reserve(c.nsv);
+    launch(surfMoveKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.dir, c.energyBuf);
+    double mx = std::max(0.0, deviceMax(c, c.energyBuf, c.nsv));
+    return mx > 0.0 ? sqrt(c.P.Hhat) / (mx * 2.0) : 1.0;
+}
+
+// Swept build with the entry step, then Self_largestFeasibleStepSize_CCD.
+double fullCCDDir(Ctx& c, const double* d, double alpha) {
+    double step = alpha;
+    computeFaceBoxes(c, c.x, d, step, true);
+    buildBvh(c, c.faceTree, c.nsf);
+    computeEdgeBoxes(c, c.x, d, step, true);
+    buildBvh(c, c.edgeTree, c.nse);
+    c.energyBuf.reserve(std::max(std::max(c.nsv, c.nse), 1));
+    if (c.nsv) {
+        profBegin(c, PROF_FULLCCD);
+        launch(fullPTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, step, view(c.faceTree), 1.0 - 0.8, c.energyBuf,
+                                                       c.status);
+        profEnd(c, PROF_FULLCCD);
+        step = std::min(step, deviceMin(c, c.energyBuf, c.nsv, 1e308));
+    }
+    if (c.nse) {
+        profBegin(c, PROF_FULLCCD);
+        launch(fullEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi, step, view(c.edgeTree),
+                                                       1.0 - 0.8, c.energyBuf, c.status);
+        profEnd(c, PROF_FULLCCD);
+        step = std::min(step, deviceMin(c, c.energyBuf, c.nse, 1e308));
+    }
+    checkStatus(c, "full CCD");
+    return step;
+}
+
+double fullCCD(Ctx& c, double alpha) { return fullCCDDir(c, c.dir, alpha); }
+
+}  // namespace cipc

@@ -1,0 +1,529 @@
+// Elastic assembly on the GPU: inertia/drag/soft per vertex, Stable
+// Neo-Hookean tetrahedra, Baraff-Witkin cloth triangles and quadratic bending
+// hinges.  Every element writes its gradient rows and lower-triangular 3x3
+// Hessian blocks to private slots; per-vertex and per-BSR-slot gathers then
+// sum them in a fixed order (no atomics, deterministic).
+//
+// Reference: computeGradientAndHessian, CPU IPC/IPCSolver.cpp:108-237;
+// Elasticity.cpp:1144-1205 (PK1), 1337-1544 (Hessians), 695-771 (energies).
+#include "cipc_device.cuh"
+#include "cipc_internal.h"
+
+#include <algorithm>
+#include <numeric>
+
+namespace cipc {
+
+namespace {
+
+constexpr int TB = 128;
+inline int blocksFor(int n, int tb = TB) { return std::max(1, std::min((n + tb - 1) / tb, 148 * 16)); }
+
+// Lower-block index of local pair (a, b), a >= b.
+__host__ __device__ __forceinline__ int lowerIdx(int a, int b) { return a * (a + 1) / 2 + b; }
+
+__global__ void vertexInitKernel(int nv, const double* x, const double* xt, const double* vp, const double* mass, double drag,
+                                 double* vtxGrad, double* diagExtra) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        double m = mass[v];
+        for (int k = 0; k < 3; ++k) {
+            double g = m * (x[3 * v + k] - xt[3 * v + k]);
+            g += drag * m * (x[3 * v + k] - vp[3 * v + k]);
+            vtxGrad[3 * v + k] = g;
+        }
+        double d = m * (1.0 + drag);
+        for (int k = 0; k < 9; ++k) diagExtra[9 * v + k] = (k % 4 == 0) ? d : 0.0;
+    }
+}
+
+__global__ void softKernel(int ns, const int* idx, const double* target, double w, const double* x, double* vtxGrad, double* diagExtra) {
+    CIPC_KERNEL_LOOP(k, ns) {
+        int v = idx[k];
+        for (int d = 0; d < 3; ++d) vtxGrad[3 * v + d] += w * (x[3 * v + d] - target[3 * k + d]);
+        diagExtra[9 * v + 0] += w; diagExtra[9 * v + 4] += w; diagExtra[9 * v + 8] += w;
+    }
+}
+
+// G rows: dF/dx_a = G[a][c] (column c of F), a = 0..3.
+__device__ __forceinline__ void tetG(const double* Di, double G[4][3]) {
+    for (int c = 0; c < 3; ++c) {
+        G[1][c] = Di[0 * 3 + c];
+        G[2][c] = Di[1 * 3 + c];
+        G[3][c] = Di[2 * 3 + c];
+        G[0][c] = -(G[1][c] + G[2][c] + G[3][c]);
+    }
+}
+
+// Stable Neo-Hookean Hessian, projected to PSD through its analytic
+// eigensystem: 3 scaling modes (3x3 eigenproblem in the singular-value
+// basis), 3 twist and 3 flip modes with closed-form eigenvalues
+// mu*Ic/(Ic+1) +/- lambda*(J-alpha)*sigma_k.  Equals makePD of the closed-form
+// 9x9 matrix of project_StabbleNHK_2_H_3D.
+template <class T>
+__device__ void snhProjectedBlocks(const double Fd[3][3], double mu, double lam, const double G[4][3], double scale, T* out) {
+    T F[3][3], U[3][3], V[3][3], s[3];
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) F[i][j] = T(Fd[i][j]);
+    svd3<T>(F, U, s, V);
+    T Ic = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+    T J = s[0] * s[1] * s[2];
+    T Ut = T(mu) * Ic / (Ic + T(1));
+    T lJ = T(lam) * (J - T(1) - T(3) * T(mu) / (T(4) * T(lam)));
+    T gC = T(mu) / (T(2) * (Ic + T(1)) * (Ic + T(1)));
+    T cf[3] = {s[1] * s[2], s[0] * s[2], s[0] * s[1]};
+    T A[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            A[i][j] = gC * T(4) * s[i] * s[j] + T(lam) * cf[i] * cf[j];
+            if (i == j) A[i][j] += Ut;
+            else A[i][j] += lJ * s[3 - i - j];
+        }
+    T W[3][3];
+    jacobiSym3<T>(A, W);
+    T acc[10][9];
+    for (int b = 0; b < 10; ++b) for (int e = 0; e < 9; ++e) acc[b][e] = T(0);
+    const T isq2 = T(0.70710678118654752440);
+    for (int m = 0; m < 9; ++m) {
+        T ev;
+        T Q[3][3];
+        if (m < 3) {
+            ev = A[m][m];
+            if (!(ev > T(0))) continue;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c)
+                    Q[r][c] = U[r][0] * W[0][m] * V[c][0] + U[r][1] * W[1][m] * V[c][1] + U[r][2] * W[2][m] * V[c][2];
+        } else {
+            int t = (m - 3) % 3;
+            int i = t == 2 ? 1 : 0, j = t == 0 ? 1 : 2, k = 3 - i - j;
+            bool twist = m < 6;
+            ev = twist ? Ut + lJ * s[k] : Ut - lJ * s[k];
+            if (!(ev > T(0))) continue;
+            T sg = twist ? T(-1) : T(1);
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) Q[r][c] = isq2 * (U[r][i] * V[c][j] + sg * U[r][j] * V[c][i]);
+        }
+        T w[4][3];
+        for (int a = 0; a < 4; ++a)
+            for (int r = 0; r < 3; ++r) w[a][r] = Q[r][0] * T(G[a][0]) + Q[r][1] * T(G[a][1]) + Q[r][2] * T(G[a][2]);
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b <= a; ++b) {
+                T* blk = acc[lowerIdx(a, b)];
+                for (int r = 0; r < 3; ++r) {
+                    T er = ev * w[a][r];
+                    for (int q = 0; q < 3; ++q) blk[3 * r + q] += er * w[b][q];
+                }
+            }
+    }
+    for (int b = 0; b < 10; ++b) for (int e = 0; e < 9; ++e) out[9 * b + e] = T(scale) * acc[b][e];
+}
+
+template <class T>
+__global__ void tetKernel(int nt, const int* tets, const double* x, const double* DmInv, const double* vol, const double* tmu,
+                          const double* tlam, const int* btype, double dt2, double* elemG, T* elemH) {
+    CIPC_KERNEL_LOOP(i, nt) {
+        int v[4];
+        for (int a = 0; a < 4; ++a) v[a] = tets[4 * i + a];
+        const double* Di = DmInv + 9 * i;
+        d3 x0 = ld3(x, v[0]);
+        d3 e1 = ld3(x, v[1]) - x0, e2 = ld3(x, v[2]) - x0, e3 = ld3(x, v[3]) - x0;
+        double Ds[3][3] = {{e1.x, e2.x, e3.x}, {e1.y, e2.y, e3.y}, {e1.z, e2.z, e3.z}};
+        double F[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) F[r][c] = Ds[r][0] * Di[c] + Ds[r][1] * Di[3 + c] + Ds[r][2] * Di[6 + c];
+        double u = tmu[i], lr = tlam[i];
+        double I2 = 0;
+        for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) I2 += F[r][c] * F[r][c];
+        double cof[3][3];
+        cof[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+        cof[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+        cof[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+        cof[1][0] = F[2][1] * F[0][2] - F[2][2] * F[0][1];
+        cof[1][1] = F[2][2] * F[0][0] - F[2][0] * F[0][2];
+        cof[1][2] = F[2][0] * F[0][1] - F[2][1] * F[0][0];
+        cof[2][0] = F[0][1] * F[1][2] - F[1][1] * F[0][2];
+        cof[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+        cof[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+        double J = F[0][0] * cof[0][0] + F[0][1] * cof[0][1] + F[0][2] * cof[0][2];
+        double ca = u * (1 - 1 / (I2 + 1)), cb = lr * (J - 1 - u * 3 / (lr * 4));
+        double G[4][3];
+        tetG(Di, G);
+        double sc = vol[i] * dt2;
+        for (int a = 0; a < 4; ++a)
+            for (int r = 0; r < 3; ++r) {
+                double f = 0;
+                for (int c = 0; c < 3; ++c) f += (ca * F[r][c] + cb * cof[r][c]) * G[a][c];
+                elemG[3 * (4 * i + a) + r] = sc * f;
+            }
+        T* out = elemH + (size_t)90 * i;
+        snhProjectedBlocks<T>(F, u, lr, G, sc, out);
+        bool fr[4];
+        for (int a = 0; a < 4; ++a) fr[a] = btype[v[a]] == 0;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b <= a; ++b)
+                if (!(fr[a] && fr[b])) for (int e = 0; e < 9; ++e) out[9 * lowerIdx(a, b) + e] = T(0);
+    }
+}
+
+// Baraff-Witkin membrane, project_baraffwitkint_H_3D + computePEPF_baraffwitkin_double.
+template <class T>
+__global__ void triKernel(int nf, const int* tris, const double* x, const double* DmInv2, const double* area, const int* btype,
+                          double stretchS, double shearS, double sr, double dt2, double* elemG, T* elemH, int blockBase,
+                          int gradBase) {
+    CIPC_KERNEL_LOOP(i, nf) {
+        int v[3] = {tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]};
+        const double* D = DmInv2 + 4 * i;
+        d3 x0 = ld3(x, v[0]);
+        d3 a1 = ld3(x, v[1]) - x0, a2 = ld3(x, v[2]) - x0;
+        d3 f0 = D[0] * a1 + D[2] * a2;  // column 0: D(0,0), D(1,0)
+        d3 f1 = D[1] * a1 + D[3] * a2;  // column 1: D(0,1), D(1,1)
+        double Gt[3][2] = {{-(D[0] + D[2]), -(D[1] + D[3])}, {D[0], D[1]}, {D[2], D[3]}};
+        double I6 = dot(f0, f1), I5u = dot(f0, f0), I5v = dot(f1, f1);
+        double uc = 1.0 - 1 / sqrt(I5u), vc = 1.0 - 1 / sqrt(I5v);
+        if (I5u > 1) uc += 1.5 * sr * (sqrt(I5u) + 1 / sqrt(I5u) - 2);
+        if (I5v > 1) vc += 1.5 * sr * (sqrt(I5v) + 1 / sqrt(I5v) - 2);
+        double P[3][2];
+        for (int k = 0; k < 3; ++k) {
+            P[k][0] = stretchS * (uc * 2. * comp(f0, k)) + shearS * (2 * I6 * comp(f1, k));
+            P[k][1] = stretchS * (vc * 2. * comp(f1, k)) + shearS * (2 * I6 * comp(f0, k));
+        }
+        double sc = dt2 * area[i];
+        for (int a = 0; a < 3; ++a)
+            for (int r = 0; r < 3; ++r) elemG[3 * (gradBase + 3 * i + a) + r] = sc * (P[r][0] * Gt[a][0] + P[r][1] * Gt[a][1]);
+        // 6x6 Hessian in T
+        T H[6][6];
+        for (int p = 0; p < 6; ++p) for (int q = 0; q < 6; ++q) H[p][q] = T(0);
+        {
+            T su = sqrt(T(I5u)), sv = sqrt(T(I5v));
+            T s = T(sr);
+            if (su > T(1)) { T d = T(2) * (((su - T(1)) * (T(3) * su * s - T(3) * s + T(2))) / (T(2) * su)); H[0][0] = H[1][1] = H[2][2] = d; }
+            if (sv > T(1)) { T d = T(2) * (((sv - T(1)) * (T(3) * sv * s - T(3) * s + T(2))) / (T(2) * sv)); H[3][3] = H[4][4] = H[5][5] = d; }
+            T nu = sqrt(T(I5u)), nvv = sqrt(T(I5v));
+            T fu[3] = {T(f0.x) / nu, T(f0.y) / nu, T(f0.z) / nu}, fv[3] = {T(f1.x) / nvv, T(f1.y) / nvv, T(f1.z) / nvv};
+            T uC = (su > T(1)) ? (T(3) * T(I5u) * s - T(3) * s + T(2)) / sqrt(T(I5u)) : T(2);
+            T vC = (sv > T(1)) ? (T(3) * T(I5v) * s - T(3) * s + T(2)) / sqrt(T(I5v)) : T(2);
+            for (int p = 0; p < 3; ++p)
+                for (int q = 0; q < 3; ++q) { H[p][q] += uC * (fu[p] * fu[q]); H[3 + p][3 + q] += vC * (fv[p] * fv[q]); }
+            for (int p = 0; p < 6; ++p) for (int q = 0; q < 6; ++q) H[p][q] *= T(stretchS);
+        }
+        {
+            T sign = I6 >= 0 ? T(1) : T(-1);
+            T g[6] = {T(f1.x), T(f1.y), T(f1.z), T(f0.x), T(f0.y), T(f0.z)};
+            T Hg[6] = {g[3], g[4], g[5], g[0], g[1], g[2]};
+            T I2 = T(I5u + I5v);
+            T i6 = T(I6);
+            T l0 = T(0.5) * (I2 + sqrt(I2 * I2 + T(12) * i6 * i6));
+            T q0[6];
+            T qn = T(0);
+            for (int k = 0; k < 6; ++k) { q0[k] = i6 * Hg[k] + l0 * g[k]; qn += q0[k] * q0[k]; }
+            qn = sqrt(qn);
+            if (qn > T(0)) for (int k = 0; k < 6; ++k) q0[k] /= qn;
+            // T = 0.5 (I + sign * Hs), Hs swaps the two 3-blocks
+            T Tq[6];
+            for (int k = 0; k < 6; ++k) Tq[k] = T(0.5) * (q0[k] + sign * q0[(k + 3) % 6]);
+            T nTq = T(0);
+            for (int k = 0; k < 6; ++k) nTq += Tq[k] * Tq[k];
+            T ai6 = fabs(i6);
+            for (int p = 0; p < 6; ++p)
+                for (int q = 0; q < 6; ++q) {
+                    T Tpq = T(0.5) * ((p == q ? T(1) : T(0)) + ((q == (p + 3) % 6) ? sign : T(0)));
+                    H[p][q] += T(shearS) * T(2) * (ai6 * (Tpq - (Tq[p] * Tq[q]) / nTq) + l0 * (q0[p] * q0[q]));
+                }
+        }
+        T* out = elemH + (size_t)9 * (blockBase + 6 * i);
+        T scT = T(sc);
+        bool fr[3] = {btype[v[0]] == 0, btype[v[1]] == 0, btype[v[2]] == 0};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b <= a; ++b) {
+                T* blk = out + 9 * lowerIdx(a, b);
+                for (int r = 0; r < 3; ++r)
+                    for (int q = 0; q < 3; ++q) {
+                        T s = T(0);
+                        for (int c = 0; c < 2; ++c)
+                            for (int d = 0; d < 2; ++d) s += T(Gt[a][c]) * H[3 * c + r][3 * d + q] * T(Gt[b][d]);
+                        blk[3 * r + q] = (fr[a] && fr[b]) ? scT * s : T(0);
+                    }
+            }
+    }
+}
+
+template <class T>
+__global__ void bendKernel(int nb, const int* bv, const double* Q, const double* x, const int* btype, double bs, double* elemG,
+                           T* elemH, int blockBase, int gradBase) {
+    CIPC_KERNEL_LOOP(i, nb) {
+        int v[4];
+        for (int a = 0; a < 4; ++a) v[a] = bv[4 * i + a];
+        const double* q = Q + 16 * i;
+        d3 p[4];
+        for (int a = 0; a < 4; ++a) p[a] = ld3(x, v[a]);
+        for (int a = 0; a < 4; ++a) {
+            d3 s = mk(0, 0, 0);
+            for (int b = 0; b < 4; ++b) s = s + q[4 * a + b] * p[b];
+            st3(elemG, gradBase + 4 * i + a, bs * s);
+        }
+        T* out = elemH + (size_t)9 * (blockBase + 10 * i);
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b <= a; ++b) {
+                T* blk = out + 9 * lowerIdx(a, b);
+                bool ok = btype[v[a]] == 0 && btype[v[b]] == 0;
+                T d = ok ? T(bs * q[4 * a + b]) : T(0);
+                for (int e = 0; e < 9; ++e) blk[e] = (e % 4 == 0) ? d : T(0);
+            }
+    }
+}
+
+template <class T>
+__global__ void slotReduceKernel(int nnzb, const int* hcPtr, const int* hcIdx, const T* elemH, T* val) {
+    CIPC_KERNEL_LOOP(sl, nnzb) {
+        T acc[9];
+        for (int e = 0; e < 9; ++e) acc[e] = T(0);
+        for (int k = hcPtr[sl]; k < hcPtr[sl + 1]; ++k) {
+            int code = hcIdx[k];
+            bool tr = code < 0;
+            int b = tr ? ~code : code;
+            const T* blk = elemH + (size_t)9 * b;
+            if (tr) {
+                for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) acc[3 * r + q] += blk[3 * q + r];
+            } else {
+                for (int e = 0; e < 9; ++e) acc[e] += blk[e];
+            }
+        }
+        for (int e = 0; e < 9; ++e) val[(size_t)9 * sl + e] = acc[e];
+    }
+}
+
+__global__ void gatherGradKernel(int nv, const double* vtxGrad, const int* gcPtr, const int* gcIdx, const double* elemG,
+                                 const int* dynStart, const int* dynEnd, const int* dynIdx, const double* dynVal, double* grad) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        double g[3] = {vtxGrad[3 * v], vtxGrad[3 * v + 1], vtxGrad[3 * v + 2]};
+        for (int k = gcPtr[v]; k < gcPtr[v + 1]; ++k) {
+            int e = gcIdx[k];
+            g[0] += elemG[3 * e]; g[1] += elemG[3 * e + 1]; g[2] += elemG[3 * e + 2];
+        }
+        if (dynStart) {
+            for (int k = dynStart[v]; k < dynEnd[v]; ++k) {
+                int e = dynIdx[k];
+                g[0] += dynVal[3 * e]; g[1] += dynVal[3 * e + 1]; g[2] += dynVal[3 * e + 2];
+            }
+        }
+        grad[3 * v] = g[0]; grad[3 * v + 1] = g[1]; grad[3 * v + 2] = g[2];
+    }
+}
+
+// ---- energies ----
+__global__ void tetEnergyKernel(int nt, const int* tets, const double* x, const double* DmInv, const double* vol, const double* tmu,
+                                const double* tlam, double* out) {
+    CIPC_KERNEL_LOOP(i, nt) {
+        const double* Di = DmInv + 9 * i;
+        d3 x0 = ld3(x, tets[4 * i]);
+        d3 e1 = ld3(x, tets[4 * i + 1]) - x0, e2 = ld3(x, tets[4 * i + 2]) - x0, e3 = ld3(x, tets[4 * i + 3]) - x0;
+        double F[3][3];
+        double Ds[3][3] = {{e1.x, e2.x, e3.x}, {e1.y, e2.y, e3.y}, {e1.z, e2.z, e3.z}};
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) F[r][c] = Ds[r][0] * Di[c] + Ds[r][1] * Di[3 + c] + Ds[r][2] * Di[6 + c];
+        double I2 = 0;
+        for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) I2 += F[r][c] * F[r][c];
+        double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) - F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                   F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+        double u = tmu[i], r = tlam[i];
+        double t = J - 1 - 3 * u / 4 / r;
+        out[i] = (0.5 * u * (I2 - 3) + 0.5 * r * t * t - 0.5 * u * log(I2 + 1)) * vol[i];
+    }
+}
+
+__global__ void triEnergyKernel(int nf, const int* tris, const double* x, const double* DmInv2, const double* area, double stretchS,
+                                double shearS, double sr, double* out) {
+    CIPC_KERNEL_LOOP(i, nf) {
+        const double* D = DmInv2 + 4 * i;
+        d3 x0 = ld3(x, tris[3 * i]);
+        d3 a1 = ld3(x, tris[3 * i + 1]) - x0, a2 = ld3(x, tris[3 * i + 2]) - x0;
+        d3 f0 = D[0] * a1 + D[2] * a2, f1 = D[1] * a1 + D[3] * a2;
+        double I6 = dot(f0, f1);
+        double u = sqrt(dot(f0, f0)), v = sqrt(dot(f1, f1));
+        double uc = u <= 1 ? 0 : 1, vc = v <= 1 ? 0 : 1;
+        double st = (u - 1) * (u - 1) + uc * sr * (u - 1) * (u - 1) * (u - 1) + (v - 1) * (v - 1) + vc * sr * (v - 1) * (v - 1) * (v - 1);
+        out[i] = (stretchS * st + shearS * I6 * I6) * area[i];
+    }
+}
+
+__global__ void bendEnergyKernel(int nb, const int* bv, const double* Q, const double* x, double* out) {
+    CIPC_KERNEL_LOOP(i, nb) {
+        const double* q = Q + 16 * i;
+        d3 p[4];
+        for (int a = 0; a < 4; ++a) p[a] = ld3(x, bv[4 * i + a]);
+        double s = 0;
+        for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) s += q[4 * a + b] * dot(p[a], p[b]);
+        out[i] = s;
+    }
+}
+
+__global__ void inertiaEnergyKernel(int nv, const double* x, const double* xt, const double* vp, const double* mass, double drag, double* out) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        d3 a = ld3(x, v) - ld3(xt, v), b = ld3(x, v) - ld3(vp, v);
+        out[v] = sqn(a) * mass[v] / 2.0 + sqn(b) * drag * mass[v] / 2.0;
+    }
+}
+
+__global__ void softEnergyKernel(int ns, const int* idx, const double* target, double w, const double* x, double* out) {
+    CIPC_KERNEL_LOOP(k, ns) {
+        int v = idx[k];
+        d3 d = ld3(x, v) - ld3(target, k);
+        out[k] = 0.5 * w * sqn(d);
+    }
+}
+
+}  // namespace
+
+void buildStaticPattern(Ctx& c, const std::vector<int>& tets, const std::vector<int>& tris, const std::vector<int>& bendV) {
+    int nv = c.nv;
+    struct Contrib { long long key; int code; };
+    std::vector<Contrib> hc;
+    std::vector<std::pair<int, int>> gc;  // (vertex, element gradient index)
+    hc.reserve((size_t)16 * c.nt + 9 * (size_t)c.nf + 16 * (size_t)c.nb);
+    int blockBase = 0, gradBase = 0;
+    auto addElem = [&](const int* vs, int k, int bBase, int gBase) {
+        for (int a = 0; a < k; ++a) {
+            gc.push_back({vs[a], gBase + a});
+            for (int b = 0; b < k; ++b) {
+                long long key = (long long)vs[a] * nv + vs[b];
+                int code = a >= b ? (bBase + lowerIdx(a, b)) : ~(bBase + lowerIdx(b, a));
+                hc.push_back({key, code});
+            }
+        }
+    };
+    for (int i = 0; i < c.nt; ++i) addElem(&tets[4 * i], 4, blockBase + 10 * i, gradBase + 4 * i);
+    blockBase += 10 * c.nt; gradBase += 4 * c.nt;
+    for (int i = 0; i < c.nf; ++i) addElem(&tris[3 * i], 3, blockBase + 6 * i, gradBase + 3 * i);
+    blockBase += 6 * c.nf; gradBase += 3 * c.nf;
+    for (int i = 0; i < c.nb; ++i) addElem(&bendV[4 * i], 4, blockBase + 10 * i, gradBase + 4 * i);
+    blockBase += 10 * c.nb; gradBase += 4 * c.nb;
+    // every vertex owns a diagonal slot even without elements
+    for (int v = 0; v < nv; ++v) hc.push_back({(long long)v * nv + v, INT32_MIN});
+    c.nElemBlocks = blockBase;
+    c.nElemGrad = gradBase;
+    std::stable_sort(hc.begin(), hc.end(), [](const Contrib& a, const Contrib& b) { return a.key < b.key; });
+    std::vector<int> rowPtr(nv + 1, 0), col, hcPtr, hcIdx, diag(nv, -1);
+    hcPtr.push_back(0);
+    for (size_t k = 0; k < hc.size();) {
+        size_t e = k;
+        while (e < hc.size() && hc[e].key == hc[k].key) {
+            if (hc[e].code != INT32_MIN) hcIdx.push_back(hc[e].code);
+            ++e;
+        }
+        int r = (int)(hc[k].key / nv), cl = (int)(hc[k].key % nv);
+        if (r == cl) diag[r] = (int)col.size();
+        col.push_back(cl);
+        rowPtr[r + 1]++;
+        hcPtr.push_back((int)hcIdx.size());
+        k = e;
+    }
+    for (int r = 0; r < nv; ++r) rowPtr[r + 1] += rowPtr[r];
+    c.nnzb = (int)col.size();
+    std::stable_sort(gc.begin(), gc.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<int> gcPtr(nv + 1, 0), gcIdx(gc.size());
+    for (size_t k = 0; k < gc.size(); ++k) { gcPtr[gc[k].first + 1]++; gcIdx[k] = gc[k].second; }
+    for (int v = 0; v < nv; ++v) gcPtr[v + 1] += gcPtr[v];
+    auto up = [&](DBuf<int>& d, const std::vector<int>& h) {
+        d.reserve(std::max<size_t>(h.size(), 1));
+        if (!h.empty()) CIPC_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+    };
+    up(c.rowPtr, rowPtr); up(c.colIdx, col); up(c.diagSlot, diag); up(c.hcPtr, hcPtr); up(c.hcIdx, hcIdx);
+    up(c.gcPtr, gcPtr); up(c.gcIdx, gcIdx);
+    c.valD.reserve((size_t)9 * c.nnzb);
+    c.valF.reserve((size_t)9 * c.nnzb);
+    c.elemG.reserve((size_t)3 * std::max(1, c.nElemGrad));
+    c.elemHD.reserve((size_t)9 * std::max(1, c.nElemBlocks));
+    c.elemHF.reserve((size_t)9 * std::max(1, c.nElemBlocks));
+    c.vtxGrad.reserve((size_t)3 * nv);
+    c.diagExtra.reserve((size_t)9 * nv);
+}
+
+template <class T>
+static void assembleElasticT(Ctx& c, T* elemH, T* val) {
+    const SimParams& P = c.P;
+    double dt2 = P.dt * P.dt;
+    if (c.nt) {
+        profBegin(c, PROF_TET);
+        launch(tetKernel<T>, blocksFor(c.nt), TB, 0, c.s, c.nt, c.tets, c.x, c.DmInv, c.vol, c.tetMu, c.tetLam, c.btype, dt2, c.elemG, elemH);
+        profEnd(c, PROF_TET);
+    }
+    profBegin(c, PROF_TRI);
+    int bBase = 10 * c.nt, gBase = 4 * c.nt;
+    if (c.nf)
+        launch(triKernel<T>, blocksFor(c.nf), TB, 0, c.s, c.nf, c.tris, c.x, c.DmInv2, c.area, c.btype, P.stretchS, P.shearS, P.strainRate, dt2,
+                                                       c.elemG, elemH, bBase, gBase);
+    profEnd(c, PROF_TRI);
+    bBase += 6 * c.nf; gBase += 3 * c.nf;
+    if (c.nb)
+        launch(bendKernel<T>, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.btype, P.plateRigidity * dt2, c.elemG, elemH, bBase, gBase);
+    profBegin(c, PROF_SLOT);
+    launch(slotReduceKernel<T>, blocksFor(c.nnzb), TB, 0, c.s, c.nnzb, c.hcPtr, c.hcIdx, elemH, val);
+    profEnd(c, PROF_SLOT);
+}
+
+void assembleElastic(Ctx& c) {
+    launch(vertexInitKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.vp, c.mass, c.P.drag, c.vtxGrad, c.diagExtra);
+    int ns = (int)c.hSoftIdx.size();
+    if (ns) launch(softKernel, blocksFor(ns), TB, 0, c.s, ns, c.softIdx, c.softTarget, c.P.softW, c.x, c.vtxGrad, c.diagExtra);
+    if (c.mixed) assembleElasticT<float>(c, c.elemHF, c.valF);
+    else assembleElasticT<double>(c, c.elemHD, c.valD);
+    CIPC_CUDA(cudaGetLastError());
+}
+
+void gatherGradient(Ctx& c) {
+    bool dyn = c.nDynG > 0;
+    launch(gatherGradKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.vtxGrad, c.gcPtr, c.gcIdx, c.elemG, dyn ? c.dynGStart.p : nullptr,
+                                                      dyn ? c.dynGEnd.p : nullptr, dyn ? c.dynGIdx.p : nullptr, c.dynGVal, c.grad);
+    CIPC_CUDA(cudaGetLastError());
+}
+
+double elasticEnergy(Ctx& c) {
+    const SimParams& P = c.P;
+    int n = std::max(std::max(c.nt, c.nf), std::max(c.nb, c.nv));
+    c.energyBuf.reserve(std::max(n, 1));
+    double E = 0;
+    if (c.nt) {
+        launch(tetEnergyKernel, blocksFor(c.nt), TB, 0, c.s, c.nt, c.tets, c.x, c.DmInv, c.vol, c.tetMu, c.tetLam, c.energyBuf);
+        E += deviceSum(c, c.energyBuf, c.nt);
+    }
+    if (c.nf) {
+        launch(triEnergyKernel, blocksFor(c.nf), TB, 0, c.s, c.nf, c.tris, c.x, c.DmInv2, c.area, P.stretchS, P.shearS, P.strainRate, c.energyBuf);
+        E += deviceSum(c, c.energyBuf, c.nf);
+    }
+    if (c.nb) {
+        launch(bendEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.energyBuf);
+        E += 0.5 * P.plateRigidity * deviceSum(c, c.energyBuf, c.nb);
+    }
+    E *= P.dt * P.dt;
+    launch(inertiaEnergyKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.vp, c.mass, P.drag, c.energyBuf);
+    E += deviceSum(c, c.energyBuf, c.nv);
+    int ns = (int)c.hSoftIdx.size();
+    if (ns) {
+        launch(softEnergyKernel, blocksFor(ns), TB, 0, c.s, ns, c.softIdx, c.softTarget, P.softW, c.x, c.energyBuf);
+        E += deviceSum(c, c.energyBuf, ns);
+    }
+    return E;
+}
+
+namespace {
+__global__ void gradEKernel(int nv, const double* x, const double* xt, const double* mass, const int* gcPtr, const int* gcIdx,
+                            const double* elemG, int ntGrad, double* gE) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        double g[3];
+        for (int k = 0; k < 3; ++k) g[k] = mass[v] * (x[3 * v + k] - xt[3 * v + k]);
+        for (int k = gcPtr[v]; k < gcPtr[v + 1]; ++k) {
+            int e = gcIdx[k];
+            if (e >= ntGrad) continue;  // tetrahedra only
+            g[0] += elemG[3 * e]; g[1] += elemG[3 * e + 1]; g[2] += elemG[3 * e + 2];
+        }
+        gE[3 * v] = g[0]; gE[3 * v + 1] = g[1]; gE[3 * v + 2] = g[2];
+    }
+}
+}  // namespace
+
+// computeEGradient (IPCSolver.cpp:72-106): inertia (no drag) plus the
+// tetrahedral elastic gradient.  Requires elemG from assembleElastic at x.
+void initKappaGradE(Ctx& c, double* gE) {
+    launch(gradEKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.mass, c.gcPtr, c.gcIdx, c.elemG, 4 * c.nt, gE);
+    CIPC_CUDA(cudaGetLastError());
+}
+
+}  // namespace cipc

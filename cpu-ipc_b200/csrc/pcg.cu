@@ -1,0 +1,285 @@
+// Newton linear solve on the GPU: block-Jacobi preconditioned conjugate
+// gradients on A = (static element BSR) + (contact BSR) + (per-vertex
+// diagonal: mass, ground, soft), replacing NewtonLinearSystem::solve's
+// backends (CPU IPC/NewtonLinearSystem.cpp:21-56, 176-207).  The stopping rule
+// is Eigen's: ||r||^2 < tol^2 ||b||^2 with x0 = 0.
+//
+// SpMV: a group of 8 lanes owns one block row; lanes stride over the row's
+// 3x3 blocks (contiguous 72-byte FP64 or 36-byte FP32 blocks, so a group reads
+// one coalesced run) and combine with shuffles.  Dot products reduce per block
+// into partials; the next kernel sums the partials in a fixed order, so no
+// host round trip is needed inside an iteration and results are reproducible.
+#include "cipc_device.cuh"
+#include "cipc_internal.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace cipc {
+
+namespace {
+
+constexpr int VB = 256;          // threads per block for vector kernels
+constexpr int GROUP = 8;         // lanes per block row in SpMV
+constexpr int MAXPART = 512;
+
+inline int vecBlocks(int n) { return std::max(1, std::min((n + VB - 1) / VB, MAXPART)); }
+
+template <class MT, class VT>
+__device__ __forceinline__ void blockMulAdd(const MT* B, const VT* xv, VT acc[3]) {
+    acc[0] += (VT)B[0] * xv[0] + (VT)B[1] * xv[1] + (VT)B[2] * xv[2];
+    acc[1] += (VT)B[3] * xv[0] + (VT)B[4] * xv[1] + (VT)B[5] * xv[2];
+    acc[2] += (VT)B[6] * xv[0] + (VT)B[7] * xv[1] + (VT)B[8] * xv[2];
+}
+
+// y = A x ; partial[block] = sum over the block's rows of x . y (for p.Ap)
+template <class MT, class VT>
+__global__ void spmvKernel(int nv, const int* rowPtr, const int* col, const MT* val, const int* dRowS, const int* dRowE, const int* dCol,
+                           const MT* dVal, const double* diagExtra, const VT* x, VT* y, double* partial, const int* flag) {
+    if (flag && *flag) return;
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    int lane = threadIdx.x & (GROUP - 1);
+    int grp = (threadIdx.x & 31) / GROUP;
+    const int RPW = 32 / GROUP;  // rows per warp per pass
+    int nWarps = gridDim.x * blockDim.x / 32;
+    double dotAcc = 0;
+    // the loop bound is uniform across a warp, so every lane reaches the shuffles
+    for (int base = (gid / 32) * RPW; base < nv; base += nWarps * RPW) {
+        int row = base + grp;
+        bool active = row < nv;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        if (active) {
+            for (int k = rowPtr[row] + lane; k < rowPtr[row + 1]; k += GROUP) {
+                int c = col[k];
+                VT xv[3] = {x[3 * c], x[3 * c + 1], x[3 * c + 2]};
+                blockMulAdd(val + (size_t)9 * k, xv, acc);
+            }
+            if (dRowS) {
+                for (int k = dRowS[row] + lane; k < dRowE[row]; k += GROUP) {
+                    int c = dCol[k];
+                    VT xv[3] = {x[3 * c], x[3 * c + 1], x[3 * c + 2]};
+                    blockMulAdd(dVal + (size_t)9 * k, xv, acc);
+                }
+            }
+        }
+        for (int o = GROUP / 2; o > 0; o >>= 1)
+            for (int q = 0; q < 3; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o, GROUP);
+        if (active && lane == 0) {
+            VT xv[3] = {x[3 * row], x[3 * row + 1], x[3 * row + 2]};
+            const double* D = diagExtra + 9 * row;
+            for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)xv[0] + D[3 * q + 1] * (double)xv[1] + D[3 * q + 2] * (double)xv[2]);
+            for (int q = 0; q < 3; ++q) {
+                y[3 * row + q] = acc[q];
+                dotAcc += (double)xv[q] * (double)acc[q];
+            }
+        }
+    }
+    if (partial) {
+        double s = blockReduce(dotAcc, AddOp(), 0.0);
+        if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    }
+}
+
+__device__ __forceinline__ double sumPartials(const double* p, int n) {
+    // every block sums the partials in the same order (deterministic)
+    __shared__ double sh;
+    double v = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
+    v = blockReduce(v, AddOp(), 0.0);
+    if (threadIdx.x == 0) sh = v;
+    __syncthreads();
+    return sh;
+}
+
+// block-Jacobi inverse of the assembled diagonal blocks
+template <class MT>
+__global__ void dinvKernel(int nv, const int* diagSlot, const MT* val, const int* dRowS, const int* dRowE, const int* dCol, const MT* dVal,
+                           const double* diagExtra, double* Dinv) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        double D[9];
+        for (int k = 0; k < 9; ++k) D[k] = diagExtra[9 * v + k];
+        int s = diagSlot[v];
+        if (s >= 0) for (int k = 0; k < 9; ++k) D[k] += (double)val[(size_t)9 * s + k];
+        if (dRowS)
+            for (int k = dRowS[v]; k < dRowE[v]; ++k)
+                if (dCol[k] == v) for (int q = 0; q < 9; ++q) D[q] += (double)dVal[(size_t)9 * k + q];
+        double c00 = D[4] * D[8] - D[5] * D[7], c10 = D[5] * D[6] - D[3] * D[8], c20 = D[3] * D[7] - D[4] * D[6];
+        double det = D[0] * c00 + D[1] * c10 + D[2] * c20;
+        double* o = Dinv + 9 * v;
+        if (det == 0.0 || !isfinite(det)) { for (int k = 0; k < 9; ++k) o[k] = 0.0; continue; }
+        o[0] = c00 / det; o[3] = c10 / det; o[6] = c20 / det;
+        o[1] = (D[2] * D[7] - D[1] * D[8]) / det;
+        o[4] = (D[0] * D[8] - D[2] * D[6]) / det;
+        o[7] = (D[1] * D[6] - D[0] * D[7]) / det;
+        o[2] = (D[1] * D[5] - D[2] * D[4]) / det;
+        o[5] = (D[2] * D[3] - D[0] * D[5]) / det;
+        o[8] = (D[0] * D[4] - D[1] * D[3]) / det;
+    }
+}
+
+template <class VT>
+__device__ __forceinline__ void applyDinv(const double* Dinv, const VT* r, VT* z, int v) {
+    const double* D = Dinv + 9 * v;
+    double r0 = r[3 * v], r1 = r[3 * v + 1], r2 = r[3 * v + 2];
+    z[3 * v] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
+    z[3 * v + 1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
+    z[3 * v + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
+}
+
+// scal layout: 0 rz, 1 (unused), 2 thr, 3 rr, 4 iterations, 5 converged flag (int view), 6 rhs2
+__global__ void pcgInitKernel(int nv, const double* b, const double* Dinv, double* x, double* r, double* z, double* p, double* part0, double* part1) {
+    double rr = 0, rz = 0;
+    CIPC_KERNEL_LOOP(v, nv) {
+        for (int q = 0; q < 3; ++q) { x[3 * v + q] = 0.0; r[3 * v + q] = b[3 * v + q]; }
+        applyDinv(Dinv, r, z, v);
+        for (int q = 0; q < 3; ++q) {
+            p[3 * v + q] = z[3 * v + q];
+            rr += r[3 * v + q] * r[3 * v + q];
+            rz += r[3 * v + q] * z[3 * v + q];
+        }
+    }
+    double a = blockReduce(rr, AddOp(), 0.0);
+    __syncthreads();
+    double c = blockReduce(rz, AddOp(), 0.0);
+    if (threadIdx.x == 0) { part0[blockIdx.x] = a; part1[blockIdx.x] = c; }
+}
+
+__global__ void pcgInitScalars(const double* part0, const double* part1, int np, double tol, double* scal, int* flag) {
+    double rr = sumPartials(part0, np);
+    double rz = sumPartials(part1, np);
+    if (threadIdx.x == 0) {
+        scal[6] = rr;
+        double thr = fmax(tol * tol * rr, 2.2250738585072014e-308);
+        scal[2] = thr;
+        scal[3] = rr;
+        scal[0] = rz;
+        scal[4] = 0;
+        *flag = (rr == 0.0 || rr < thr) ? 1 : 0;
+    }
+}
+
+// x += a p ; r -= a Ap ; z = M r ; partials of r.r and r.z
+__global__ void pcgUpdateKernel(int nv, const double* pAp, int np, const double* scal, const double* Dinv, const double* p, const double* Ap, double* x,
+                                double* r, double* z, double* partRR, double* partRZ, const int* flag) {
+    if (*flag) return;
+    double alpha = scal[0] / sumPartials(pAp, np);
+    double rr = 0, rz = 0;
+    CIPC_KERNEL_LOOP(v, nv) {
+        for (int q = 0; q < 3; ++q) {
+            x[3 * v + q] += alpha * p[3 * v + q];
+            r[3 * v + q] -= alpha * Ap[3 * v + q];
+        }
+        applyDinv(Dinv, r, z, v);
+        for (int q = 0; q < 3; ++q) { rr += r[3 * v + q] * r[3 * v + q]; rz += r[3 * v + q] * z[3 * v + q]; }
+    }
+    double a = blockReduce(rr, AddOp(), 0.0);
+    __syncthreads();
+    double c = blockReduce(rz, AddOp(), 0.0);
+    if (threadIdx.x == 0) { partRR[blockIdx.x] = a; partRZ[blockIdx.x] = c; }
+}
+
+// scalar step: convergence test, beta; one block.
+__global__ void pcgScalarKernel(const double* partRR, const double* partRZ, int np, double* scal, int* flag, int maxIter) {
+    if (*flag) return;
+    double rr = sumPartials(partRR, np);
+    double rz = sumPartials(partRZ, np);
+    if (threadIdx.x == 0) {
+        scal[3] = rr;
+        if (rr < scal[2]) { *flag = 1; scal[4] += 1; return; }
+        scal[1] = rz / scal[0];  // beta
+        scal[0] = rz;
+        scal[4] += 1;
+        if (scal[4] >= maxIter) *flag = 2;
+    }
+}
+
+__global__ void pcgDirKernel(int nv, const double* scal, const double* z, double* p, const int* flag) {
+    if (*flag == 1) return;
+    double beta = scal[1];
+    CIPC_KERNEL_LOOP(i, 3 * nv) p[i] = z[i] + beta * p[i];
+}
+
+__global__ void rhsKernel(int nv, const double* g, const int* btype, double* b) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        bool fr = btype[v] == 0;
+        for (int q = 0; q < 3; ++q) b[3 * v + q] = fr ? g[3 * v + q] : 0.0;
+    }
+}
+
+}  // namespace
+
+void buildRhs(Ctx& c) {
+    c.rhs.reserve(3 * c.nv);
+    launch(rhsKernel, vecBlocks(c.nv), VB, 0, c.s, c.nv, c.grad, c.btype, c.rhs);
+    CIPC_CUDA(cudaGetLastError());
+}
+
+template <class MT>
+static void spmvT(Ctx& c, const MT* val, const MT* dval, const double* x, double* y, double* partial, const int* flag, int nblk) {
+    bool dyn = c.nDynB > 0;
+    launch(spmvKernel<MT, double>, nblk, VB, 0, c.s, c.nv, c.rowPtr, c.colIdx, val, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
+                                                 dyn ? c.dynCol.p : nullptr, dval, c.diagExtra, x, y, partial, flag);
+}
+
+static int spmvBlocks(Ctx& c) { return std::max(1, std::min((c.nv * GROUP + VB - 1) / VB, MAXPART)); }
+
+void spmv(Ctx& c, const double* x, double* y) {
+    if (c.mixed) spmvT<float>(c, c.valF, c.dynBF, x, y, nullptr, nullptr, spmvBlocks(c));
+    else spmvT<double>(c, c.valD, c.dynBD, x, y, nullptr, nullptr, spmvBlocks(c));
+    CIPC_CUDA(cudaGetLastError());
+}
+
+// FP64 PCG (mixed mode: FP32 matrix blocks promoted in the FP64 SpMV).
+int pcgSolve(Ctx& c) {
+    int nv = c.nv;
+    size_t n3 = 3 * (size_t)nv;
+    c.sol.reserve(n3); c.r.reserve(n3); c.z.reserve(n3); c.p.reserve(n3); c.Ap.reserve(n3); c.Dinv.reserve(9 * (size_t)nv);
+    c.red.reserve(4 * MAXPART + 16);
+    c.scal.reserve(16);
+    c.counters.reserve(16);
+    bool dyn = c.nDynB > 0;
+    if (c.mixed)
+        launch(dinvKernel<float>, vecBlocks(nv), VB, 0, c.s, nv, c.diagSlot, c.valF, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
+                                                         dyn ? c.dynCol.p : nullptr, c.dynBF, c.diagExtra, c.Dinv);
+    else
+        launch(dinvKernel<double>, vecBlocks(nv), VB, 0, c.s, nv, c.diagSlot, c.valD, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
+                                                          dyn ? c.dynCol.p : nullptr, c.dynBD, c.diagExtra, c.Dinv);
+    int vb = vecBlocks(nv), sb = spmvBlocks(c);
+    double* partA = c.red.p;
+    double* partB = c.red.p + MAXPART;
+    double* partC = c.red.p + 2 * MAXPART;
+    int* flag = c.counters.p + 10;
+    launch(pcgInitKernel, vb, VB, 0, c.s, nv, c.rhs, c.Dinv, c.sol, c.r, c.z, c.p, partA, partB);
+    launch(pcgInitScalars, 1, VB, 0, c.s, partA, partB, vb, c.pcgTol, c.scal, flag);
+    CIPC_CUDA(cudaGetLastError());
+    const int chunk = 16;
+    int it = 0;
+    int hflag = 0;
+    double hs[8];
+    while (true) {
+        for (int k = 0; k < chunk; ++k) {
+            profBegin(c, PROF_SPMV);
+            if (c.mixed) spmvT<float>(c, c.valF, c.dynBF, c.p, c.Ap, partC, flag, sb);
+            else spmvT<double>(c, c.valD, c.dynBD, c.p, c.Ap, partC, flag, sb);
+            profEnd(c, PROF_SPMV);
+            launch(pcgUpdateKernel, vb, VB, 0, c.s, nv, partC, sb, c.scal, c.Dinv, c.p, c.Ap, c.sol, c.r, c.z, partA, partB, flag);
+            launch(pcgScalarKernel, 1, VB, 0, c.s, partA, partB, vb, c.scal, flag, c.pcgMaxIter);
+            launch(pcgDirKernel, vb, VB, 0, c.s, nv, c.scal, c.z, c.p, flag);
+        }
+        CIPC_CUDA(cudaGetLastError());
+        CIPC_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        CIPC_CUDA(cudaMemcpyAsync(hs, c.scal.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        it = (int)hs[4];
+        if (hflag) break;
+    }
+    double rhs2 = 0;
+    CIPC_CUDA(cudaMemcpy(&rhs2, c.scal.p + 6, sizeof(double), cudaMemcpyDeviceToHost));
+    c.lastPcgIters = it;
+    c.lastPcgRelRes = rhs2 > 0 ? std::sqrt(hs[3] / rhs2) : 0.0;
+    c.pcgItersTotal += it;
+    if (hflag == 2) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
+    return it;
+}
+
+}  // namespace cipc

@@ -1,0 +1,842 @@
+// Host driver of the GPU IPC time step and the C ABI (include/cipc_gpu.h).
+//
+// The control flow mirrors the reference's solver so that iteration counts,
+// backtracking decisions and kappa updates follow the same rules:
+//   solveIPCStep           CPU IPC/IPCSolver.cpp:1079-1336
+//   solveBarrierSubproblem CPU IPC/IPCSolver.cpp:890-1064
+//   lineSearch             CPU IPC/IPCSolver.cpp:560-749
+//   kappa rules            CPU IPC/IPCSolver.cpp:751-869
+// Every numeric stage runs on the GPU (elastic.cu, contact.cu, collision.cu,
+// pcg.cu); the host only sequences stages and reads back scalars.
+#include "../../include/cipc_gpu.h"
+#include "cipc_device.cuh"
+#include "cipc_internal.h"
+#include "scene_setup.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+
+namespace cipc {
+
+long long g_kernelLaunches = 0;
+
+double fullCCDDir(Ctx& c, const double* d, double alpha);
+void rebuildTrees(Ctx& c);
+
+namespace {
+
+constexpr int TB = 256;
+inline int blocksFor(int n) { return std::max(1, std::min((n + TB - 1) / TB, 148 * 16)); }
+
+__global__ void stepForwardKernel(int nv, const double* x0, const double* dir, const int* btype, double alpha, int all, double* x) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        if (all || btype[v] == 0)
+            for (int q = 0; q < 3; ++q) x[3 * v + q] = x0[3 * v + q] - alpha * dir[3 * v + q];
+    }
+}
+__global__ void velocityKernel(int nv, const double* x, double* vp, double* vel, double* xt, double dt, int quasi, double g) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        for (int q = 0; q < 3; ++q) {
+            double xv = x[3 * v + q];
+            double ve = quasi ? 0.0 : (xv - vp[3 * v + q]) / dt;
+            vel[3 * v + q] = ve;
+            vp[3 * v + q] = xv;
+        }
+        double gd[3] = {0.0, g * dt * dt, 0.0};
+        for (int q = 0; q < 3; ++q) xt[3 * v + q] = vp[3 * v + q] + vel[3 * v + q] * dt + gd[q];
+    }
+}
+__global__ void inertialTargetKernel(int nv, const double* vp, const double* vel, double* xt, double dt, double g) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        double gd[3] = {0.0, g * dt * dt, 0.0};
+        for (int q = 0; q < 3; ++q) xt[3 * v + q] = vp[3 * v + q] + vel[3 * v + q] * dt + gd[q];
+    }
+}
+
+using Clock = std::chrono::steady_clock;
+double ms(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); }
+
+void sync(Ctx& c) { CIPC_CUDA(cudaStreamSynchronize(c.s)); }
+
+void stepForward(Ctx& c, const double* x0, const double* d, double alpha, bool all = false) {
+    launch(stepForwardKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, x0, d, c.btype, alpha, all ? 1 : 0, c.x);
+}
+
+double totalEnergy(Ctx& c, double kappa) { return elasticEnergy(c) + contactEnergy(c, kappa); }
+
+void suggestKappa(double& kappa, double Hhat, double bbox2, double meanMass) {
+    double d = 1.0e-16 * bbox2, t = d - Hhat;
+    double hb = (std::log(d / Hhat) * -2.0 - t * 4.0 / d) + 1.0 / (d * d) * (t * t);
+    kappa = 1e13 * meanMass / (4.0e-16 * bbox2 * hb);
+}
+void upperBoundKappa(double& kappa, double Hhat, double bbox2, double meanMass) {
+    double d = 1.0e-16 * bbox2, t = d - Hhat;
+    double hb = (std::log(d / Hhat) * -2.0 - t * 4.0 / d) + 1.0 / (d * d) * (t * t);
+    double kmax = 100 * 1e13 * meanMass / (4.0e-16 * bbox2 * hb);
+    if (kappa > kmax) kappa = kmax;
+}
+
+// initKappa (IPCSolver.cpp:770-809); `kappa` may alias c.P.kappa.
+void initKappa(Ctx& c, double& kappa) {
+    if (c.nGround + c.nSelf == 0) return;
+    assembleElastic(c);  // elemG holds the tetrahedral gradient at x
+    c.scratch.reserve(8 + 1024);
+    DBuf<double>& gE = c.z;
+    DBuf<double>& gc = c.Ap;
+    gE.reserve(3 * c.nv); gc.reserve(3 * c.nv);
+    initKappaGradE(c, gE);
+    contactGradientKappa(c, gc);
+    double gsum = deviceDot(c, gc, gE, 3 * c.nv);
+    double gsnorm = deviceDot(c, gc, gc, 3 * c.nv);
+    double minKappa = -gsum / gsnorm;
+    if (minKappa > 0.0) kappa = minKappa;
+    suggestKappa(minKappa, c.P.Hhat, c.P.bboxDiag2, c.P.meanMass);
+    if (kappa < minKappa) kappa = minKappa;
+    upperBoundKappa(c.P.kappa, c.P.Hhat, c.P.bboxDiag2, c.P.meanMass);
+}
+
+// postLineSearch (IPCSolver.cpp:811-869); kappa is the sub-problem's copy.
+void postLineSearch(Ctx& c, double& kappa) {
+    if (kappa == 0.0) { initKappa(c, kappa); return; }
+    bool update = false;
+    closeConstraintCheck(c, update);
+    if (update) {
+        kappa *= 2.0;
+        upperBoundKappa(c.P.kappa, c.P.Hhat, c.P.bboxDiag2, c.P.meanMass);
+    }
+    closeConstraintRecord(c);
+}
+
+struct Stats {
+    cipc_step_stats s;
+};
+
+bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st) {
+    double E0 = totalEnergy(c, kappa);
+    double gTp = deviceDot(c, c.grad, c.dir, 3 * c.nv);
+    if (!std::isfinite(E0) || !std::isfinite(gTp)) throw std::runtime_error("line search received a non-finite energy or direction");
+    CIPC_CUDA(cudaMemcpyAsync(c.x0.p, c.x.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToDevice, c.s));
+    stepForward(c, c.x0, c.dir, alpha);
+    int nInter = 0;
+    if (c.P.useBarrier) {
+        rebuildTrees(c);
+        while (isIntersected(c)) {
+            if (nInter >= 64 || alpha <= std::numeric_limits<double>::epsilon())
+                throw std::runtime_error("line search could not find a non-intersecting step");
+            nInter++;
+            alpha /= 2.0;
+            stepForward(c, c.x0, c.dir, alpha);
+            rebuildTrees(c);
+        }
+    }
+    buildCollisionSets(c, false);
+    double E = totalEnergy(c, kappa);
+    int nLS = 0;
+    const double LF = alpha;
+    auto ok = [&](double e) { return std::isfinite(e) && e < E0; };
+    while (!ok(E)) {
+        if (nLS >= 64 || alpha <= std::numeric_limits<double>::epsilon() * std::max(1.0, LF)) {
+            double thr = c.P.newtonThr * std::sqrt(c.P.bboxDiag2) * c.P.dt;
+            if (deviceInfNorm(c, c.dir, 3 * c.nv) < thr) {
+                CIPC_CUDA(cudaMemcpyAsync(c.x.p, c.x0.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToDevice, c.s));
+                buildCollisionSets(c, true);
+                st.energyBacktracks += nLS;
+                st.intersectionBacktracks += nInter;
+                st.lineSearchBacktracks += nInter + nLS;
+                st.maximumEnergyBacktracksPerNewton = std::max(st.maximumEnergyBacktracksPerNewton, nLS);
+                if (nLS > 2) ++st.newtonStepsWithMoreThanTwoBacktracks;
+                return false;
+            }
+            throw std::runtime_error("line search failed to find a strict energy decrease");
+        }
+        alpha *= 0.5;
+        ++nLS;
+        stepForward(c, c.x0, c.dir, alpha);
+        buildCollisionSets(c, true);
+        E = totalEnergy(c, kappa);
+    }
+    if (alpha < LF) {
+        bool recompute = false;
+        if (c.P.useBarrier) {
+            int it = 0;
+            while (isIntersected(c)) {
+                if (it++ >= 64 || alpha <= std::numeric_limits<double>::epsilon()) throw std::runtime_error("backtracked step remains intersecting");
+                alpha /= 2.0;
+                nInter++;
+                stepForward(c, c.x0, c.dir, alpha);
+                rebuildTrees(c);
+                recompute = true;
+            }
+        }
+        if (recompute) buildCollisionSets(c, false);
+    }
+    st.energyBacktracks += nLS;
+    st.intersectionBacktracks += nInter;
+    st.lineSearchBacktracks += nInter + nLS;
+    st.maximumEnergyBacktracksPerNewton = std::max(st.maximumEnergyBacktracksPerNewton, nLS);
+    if (nLS > 2) ++st.newtonStepsWithMoreThanTwoBacktracks;
+    st.acceptedStepSum += alpha;
+    st.minimumAcceptedStep = std::min(st.minimumAcceptedStep, alpha);
+    st.maximumAcceptedStep = std::max(st.maximumAcceptedStep, alpha);
+    return true;
+}
+
+// Assembly stage: gradient into c.grad, Hessian into the static + contact BSR.
+int assembleAll(Ctx& c) {
+    assembleElastic(c);
+    int coll = contactAssemble(c);
+    gatherGradient(c);
+    checkStatus(c, "assembly");
+    return coll;
+}
+
+void linearSolve(Ctx& c) {
+    buildRhs(c);
+    pcgSolve(c);
+    CIPC_CUDA(cudaMemcpyAsync(c.dir.p, c.sol.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToDevice, c.s));
+}
+
+int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
+    int k = 0;
+    double beta = 1;
+    const int kmin = 6;
+    for (; k < 10000; ++k) {
+        auto t0 = Clock::now();
+        st.collisions += assembleAll(c);
+        sync(c);
+        auto t1 = Clock::now();
+        linearSolve(c);
+        st.pcgIterations += c.lastPcgIters;
+        st.pcgRelativeResidual = std::max(st.pcgRelativeResidual, c.lastPcgRelRes);
+        st.matrixBlocks = std::max<long long>(st.matrixBlocks, (long long)c.nnzb + c.nDynB);
+        double thr = c.P.newtonThr * std::sqrt(c.P.bboxDiag2) * c.P.dt;
+        double dn = deviceInfNorm(c, c.dir, 3 * c.nv);
+        auto t2 = Clock::now();
+        if (dn < thr) {
+            st.assemblyMilliseconds += ms(t0, t1);
+            st.linearSolveMilliseconds += ms(t1, t2);
+            break;
+        }
+        double alpha = groundStepBound(c);
+        alpha = std::min(1.0, alpha);
+        if (alpha <= 0) alpha = 1;
+        if (c.P.useBarrier) {
+            double partial = partialCCD(c, alpha);
+            double aCFL = cflBound(c);
+            double full = fullCCD(c, alpha);
+            alpha = std::min(alpha, aCFL);
+            if (partial > 2.0 * aCFL) {
+                alpha = std::min(partial, full);
+                alpha = std::max(alpha, aCFL);
+            }
+        }
+        sync(c);
+        auto t3 = Clock::now();
+        bool accepted = lineSearch(c, alpha, kappa, st);
+        sync(c);
+        auto t4 = Clock::now();
+        if (!accepted) {
+            st.assemblyMilliseconds += ms(t0, t1);
+            st.linearSolveMilliseconds += ms(t1, t2);
+            st.ccdMilliseconds += ms(t2, t3);
+            st.lineSearchMilliseconds += ms(t3, t4);
+            break;
+        }
+        postLineSearch(c, kappa);
+        sync(c);
+        auto t5 = Clock::now();
+        st.assemblyMilliseconds += ms(t0, t1);
+        st.linearSolveMilliseconds += ms(t1, t2);
+        st.ccdMilliseconds += ms(t2, t3);
+        st.lineSearchMilliseconds += ms(t3, t4);
+        st.postLineSearchMilliseconds += ms(t4, t5);
+        if (k + 1 >= kmin) beta = (1 - alpha) * beta;
+        if (beta <= thr) break;
+    }
+    st.newtonIterations += k;
+    return k;
+}
+
+// twistingBoundaryDirection (Simulator.cpp:24-46) with a rate parameter.
+void motionDir(int motion, double rate, const double* x, const double* rest, double frac, double dt, double* out) {
+    out[0] = out[1] = out[2] = 0.0;
+    if (motion != CIPC_MOTION_TWIST_X) return;
+    double ang = rate * dt * frac, cs = std::cos(ang), sn = std::sin(ang);
+    if (rest[0] < 0.0) { out[0] = 0; out[1] = cs * x[1] + sn * x[2] - x[1]; out[2] = -sn * x[1] + cs * x[2] - x[2]; }
+    else if (rest[0] > 0.0) { out[0] = 0; out[1] = cs * x[1] - sn * x[2] - x[1]; out[2] = sn * x[1] + cs * x[2] - x[2]; }
+}
+
+void solveIPCStep(Ctx& c, cipc_step_stats& st) {
+    std::memset(&st, 0, sizeof(st));
+    st.frame = c.stepIndex;
+    st.minimumAcceptedStep = 1.0;
+    st.minConstraintDistance2 = -1.0;
+    auto tBegin = Clock::now();
+    SimParams& P = c.P;
+    upperBoundKappa(P.kappa, P.Hhat, P.bboxDiag2, P.meanMass);
+    if (P.kappa < 1e-16) suggestKappa(P.kappa, P.Hhat, P.bboxDiag2, P.meanMass);
+    initKappa(c, P.kappa);
+    frictionInitialize(c);
+    int nv = c.nv;
+    bool needHost = (!c.hSoftIdx.empty() && c.softMotion != CIPC_MOTION_NONE) || (!c.hDirIdx.empty() && c.dirMotion != CIPC_MOTION_NONE);
+    std::vector<double> hx;
+    if (needHost) {
+        hx.resize(3 * (size_t)nv);
+        CIPC_CUDA(cudaMemcpy(hx.data(), c.x.p, sizeof(double) * 3 * nv, cudaMemcpyDeviceToHost));
+    }
+    if (!c.hSoftIdx.empty() && c.softMotion != CIPC_MOTION_NONE) {
+        std::vector<double> tg(3 * c.hSoftIdx.size());
+        for (size_t k = 0; k < c.hSoftIdx.size(); ++k) {
+            int v = c.hSoftIdx[k];
+            double d[3];
+            motionDir(c.softMotion, c.softRate, &hx[3 * v], &c.hRest[3 * v], 1.0, P.dt, d);
+            for (int q = 0; q < 3; ++q) tg[3 * k + q] = hx[3 * v + q] - d[q];
+        }
+        CIPC_CUDA(cudaMemcpy(c.softTarget.p, tg.data(), tg.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (!c.hDirIdx.empty() && c.dirMotion != CIPC_MOTION_NONE) {
+        std::vector<double> d(3 * (size_t)nv, 0.0);
+        auto dirs = [&](double frac, const std::vector<double>& xs) {
+            std::fill(d.begin(), d.end(), 0.0);
+            for (int v : c.hDirIdx) motionDir(c.dirMotion, c.dirRate, &xs[3 * v], &c.hRest[3 * v], frac, P.dt, &d[3 * v]);
+            CIPC_CUDA(cudaMemcpy(c.Ap.p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+        };
+        c.Ap.reserve(3 * (size_t)nv);
+        double na = 1;
+        dirs(na, hx);
+        na = fullCCDDir(c, c.Ap, na);
+        dirs(na, hx);
+        CIPC_CUDA(cudaMemcpyAsync(c.x0.p, c.x.p, sizeof(double) * 3 * nv, cudaMemcpyDeviceToDevice, c.s));
+        stepForward(c, c.x0, c.Ap, 1.0, true);
+        rebuildTrees(c);
+        int ni = 0;
+        while (isIntersected(c)) {
+            if (ni++ >= 64 || na <= std::numeric_limits<double>::epsilon()) throw std::runtime_error("animated boundary update remains intersecting");
+            na /= 2.0;
+            dirs(na, hx);
+            stepForward(c, c.x0, c.Ap, 1.0, true);
+            rebuildTrees(c);
+        }
+        buildCollisionSets(c, false);
+    }
+    for (; st.kappaIterations < 64; ++st.kappaIterations) {
+        c.nCloseG = c.nCloseS = 0;
+        solveBarrierSubproblem(c, P.kappa, st);
+        double mn, mx;
+        bool any;
+        constraintMinMax(c, mn, mx, any);
+        if (any) {
+            st.minConstraintDistance2 = mn;
+            if (mn < P.dTol) break;
+            else if (mx < P.Hhat) break;
+        } else break;
+    }
+    if (st.kappaIterations == 64) throw std::runtime_error("IPC kappa loop exceeded its iteration limit");
+    ++st.kappaIterations;
+    launch(velocityKernel, blocksFor(nv), TB, 0, c.s, nv, c.x, c.vp, c.vel, c.xt, P.dt, P.quasiStatic, P.applyGravity ? -9.8 : 0.0);
+    CIPC_CUDA(cudaGetLastError());
+    sync(c);
+    st.stepMilliseconds = ms(tBegin, Clock::now());
+    st.kappa = P.kappa;
+    st.groundContacts = c.nGround;
+    st.selfContacts = c.nSelf;
+    st.mollifiedContacts = c.nMoll;
+    c.stepIndex++;
+}
+
+template <class T>
+void upload(DBuf<T>& d, const std::vector<T>& h) {
+    d.reserve(std::max<size_t>(h.size(), 1));
+    if (!h.empty()) CIPC_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
+    if (!s || s->nv <= 0 || !s->x || !s->btype) throw InvalidArgument("scene needs vertices and boundary types");
+    if (s->nt < 0 || s->nf < 0 || (s->nt > 0 && !s->tets) || (s->nf > 0 && !s->tris)) throw InvalidArgument("invalid element arrays");
+    if (s->nv >= (1 << 21) - 2) throw InvalidArgument("vertex count exceeds the 2^21 limit of the packed contact keys");
+    if (!(s->dt > 0) || !(s->relDhat > 0)) throw InvalidArgument("time step and dHat must be positive");
+    if (o && o->backend != CIPC_LINEAR_GPU_PCG) throw InvalidArgument("only the GPU PCG backend is implemented by this library");
+    for (int i = 0; i < 4 * s->nt; ++i)
+        if (s->tets[i] < 0 || s->tets[i] >= s->nv) throw InvalidArgument("tetrahedron references an out-of-range vertex");
+    for (int i = 0; i < 3 * s->nf; ++i)
+        if (s->tris[i] < 0 || s->tris[i] >= s->nv) throw InvalidArgument("triangle references an out-of-range vertex");
+    // BoundaryConditionOps::initialize validation (BoundaryConditions.cpp:55-109)
+    for (int k = 0; k < s->nsoft; ++k) {
+        int v = s->softIdx[k];
+        if (v < 0 || v >= s->nv || s->btype[v] != 0) throw InvalidArgument("soft boundary vertices must remain free Newton unknowns");
+    }
+    if (s->nsoft > 0 && !(s->softW > 0)) throw InvalidArgument("soft boundary weight must be finite and positive");
+    for (int k = 0; k < s->ndir; ++k) {
+        int v = s->dirIdx[k];
+        if (v < 0 || v >= s->nv || s->btype[v] == 0) throw InvalidArgument("animated Dirichlet vertices must be marked constrained");
+    }
+    int dev = 0;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device is available");
+    CIPC_CUDA(cudaGetDevice(&dev));
+    auto c = new Ctx();
+    try {
+        c->nv = s->nv; c->nt = s->nt; c->nf = s->nf;
+        if (o) {
+            c->mixed = o->precision == CIPC_PRECISION_MIXED;
+            c->precond = o->preconditioner;
+            c->pcgTol = o->relativeTolerance > 0 ? o->relativeTolerance : 1e-6;
+            c->pcgMaxIter = o->maximumIterations > 0 ? o->maximumIterations : 10000;
+        }
+        SceneInput in;
+        in.nv = s->nv; in.nt = s->nt; in.nf = s->nf;
+        in.x.assign(s->x, s->x + 3 * (size_t)s->nv);
+        in.tets.assign(s->tets, s->tets + 4 * (size_t)s->nt);
+        in.tris.assign(s->tris, s->tris + 3 * (size_t)s->nf);
+        if (s->tetE) in.tetE.assign(s->tetE, s->tetE + s->nt);
+        in.density = s->density; in.cloth_density = s->cloth_density; in.thickness = s->thickness; in.E = s->E; in.nu = s->nu;
+        in.clothE = s->clothE; in.shearE = s->shearE; in.bendE = s->bendE; in.strainRate = s->strainRate; in.relDhat = s->relDhat;
+        in.quadBending = s->quad_bending != 0;
+        for (int k = 0; k < 3; ++k) { in.bboxMin[k] = s->bboxMin[k]; in.bboxMax[k] = s->bboxMax[k]; }
+        if (s->surfFaces && s->surfVerts && s->surfEdges) {
+            in.hasSurface = true;
+            in.faces.assign(s->surfFaces, s->surfFaces + 3 * (size_t)s->nsf);
+            in.surfVerts.assign(s->surfVerts, s->surfVerts + s->nsv);
+            in.edges.assign(s->surfEdges, s->surfEdges + 2 * (size_t)s->nse);
+        }
+        SceneRest r;
+        setupScene(in, r);
+        c->nb = (int)r.bendV.size() / 4;
+        c->nsf = (int)r.faces.size() / 3;
+        c->nsv = (int)r.surfVerts.size();
+        c->nse = (int)r.edges.size() / 2;
+        SimParams& P = c->P;
+        std::memset(&P, 0, sizeof(P));
+        P.dt = s->dt; P.drag = s->drag; P.Hhat = r.Hhat; P.Fhat = r.Fhat; P.dTol = r.dTol; P.kappa = 0; P.bboxDiag2 = r.bboxDiag2;
+        P.newtonThr = s->newtonThr; P.meanMass = r.meanMass; P.avgEdge = r.avgEdge; P.friction = s->friction;
+        P.stretchS = r.stretchS; P.shearS = r.shearS; P.strainRate = s->strainRate; P.plateRigidity = r.plateRigidity;
+        P.groundN[0] = 0; P.groundN[1] = 1; P.groundN[2] = 0; P.groundD = -1;
+        P.softW = s->softW;
+        P.useBarrier = s->use_barrier; P.applyGravity = s->apply_gravity; P.quasiStatic = s->quasi_static;
+        c->hBtype.assign(s->btype, s->btype + s->nv);
+        c->hRest = in.x;
+        if (s->nsoft > 0) c->hSoftIdx.assign(s->softIdx, s->softIdx + s->nsoft);
+        if (s->ndir > 0) c->hDirIdx.assign(s->dirIdx, s->dirIdx + s->ndir);
+        c->softMotion = s->softMotion; c->softRate = s->softRate; c->dirMotion = s->dirMotion; c->dirRate = s->dirRate;
+        for (int v : c->hSoftIdx) if (v < 0 || v >= s->nv || c->hBtype[v] != 0) throw InvalidArgument("soft boundary vertices must be free");
+        for (int v : c->hDirIdx) if (v < 0 || v >= s->nv || c->hBtype[v] == 0) throw InvalidArgument("animated Dirichlet vertices must be marked constrained");
+        CIPC_CUDA(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+        size_t n3 = 3 * (size_t)s->nv;
+        upload(c->x, in.x); upload(c->rest, in.x); upload(c->vp, in.x);
+        c->x0.reserve(n3); c->xt.reserve(n3); c->dir.reserve(n3); c->grad.reserve(n3);
+        std::vector<double> vel(n3, 0.0);
+        if (s->vel) vel.assign(s->vel, s->vel + n3);
+        upload(c->vel, vel);
+        upload(c->mass, r.mass);
+        upload(c->btype, c->hBtype);
+        upload(c->tets, in.tets); upload(c->tris, in.tris);
+        upload(c->DmInv, r.DmInv); upload(c->vol, r.vol); upload(c->tetMu, r.tetMu); upload(c->tetLam, r.tetLam);
+        upload(c->DmInv2, r.DmInv2); upload(c->area, r.area);
+        upload(c->bendV, r.bendV); upload(c->bendQ, r.bendQ);
+        upload(c->faces, r.faces); upload(c->surfVerts, r.surfVerts); upload(c->edges, r.edges);
+        upload(c->softIdx, c->hSoftIdx);
+        std::vector<double> tgt;
+        for (int v : c->hSoftIdx) for (int q = 0; q < 3; ++q) tgt.push_back(in.x[3 * v + q]);
+        upload(c->softTarget, tgt);
+        upload(c->dirIdx, c->hDirIdx);
+        c->status.reserve(4);
+        CIPC_CUDA(cudaMemset(c->status.p, 0, sizeof(int)));
+        c->counters.reserve(16);
+        c->scratch.reserve(2048);
+        buildStaticPattern(*c, in.tets, in.tris, r.bendV);
+        launch(inertialTargetKernel, blocksFor(c->nv), TB, 0, c->s, c->nv, c->vp, c->vel, c->xt, P.dt, P.applyGravity ? -9.8 : 0.0);
+        CIPC_CUDA(cudaGetLastError());
+        // rebuildCollisionSets (Simulator.cpp:532-540)
+        buildCollisionSets(*c, true);
+        sync(*c);
+        return c;
+    } catch (...) {
+        delete c;
+        throw;
+    }
+}
+
+}  // namespace
+}  // namespace cipc
+
+using namespace cipc;
+
+struct cipc_gpu_context {
+    Ctx* c;
+};
+
+static thread_local std::string g_createError;
+
+template <class F>
+static int guarded(cipc_gpu_context* h, F f) {
+    if (!h || !h->c) return CIPC_ERR_INVALID_ARGUMENT;
+    try {
+        f(*h->c);
+        return CIPC_OK;
+    } catch (const InvalidArgument& e) {
+        h->c->lastError = e.what();
+        return CIPC_ERR_INVALID_ARGUMENT;
+    } catch (const CudaError& e) {
+        h->c->lastError = e.what();
+        return CIPC_ERR_CUDA;
+    } catch (const std::exception& e) {
+        h->c->lastError = e.what();
+        std::string m = e.what();
+        if (m.find("device status") != std::string::npos) return CIPC_ERR_DEVICE_STATUS;
+        if (m.find("did not converge") != std::string::npos) return CIPC_ERR_NOT_CONVERGED;
+        return CIPC_ERR_RUNTIME;
+    }
+}
+
+extern "C" {
+
+const char* cipc_gpu_create_error(void) { return g_createError.c_str(); }
+
+int cipc_gpu_create(const cipc_scene_desc* scene, const cipc_linear_options* options, cipc_gpu_context** out) {
+    if (!out) return CIPC_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        Ctx* c = createContext(scene, options);
+        *out = new cipc_gpu_context{c};
+        g_createError.clear();
+        return CIPC_OK;
+    } catch (const InvalidArgument& e) {
+        g_createError = e.what();
+        return CIPC_ERR_INVALID_ARGUMENT;
+    } catch (const CudaError& e) {
+        g_createError = e.what();
+        return CIPC_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_createError = e.what();
+        return CIPC_ERR_RUNTIME;
+    }
+}
+
+void cipc_gpu_destroy(cipc_gpu_context* h) {
+    if (!h) return;
+    if (h->c) {
+        if (h->c->s) cudaStreamSynchronize(h->c->s);
+        Ctx& c = *h->c;
+        DBuf<double>* ds[] = {&c.x, &c.x0, &c.xt, &c.vp, &c.vel, &c.rest, &c.dir, &c.grad, &c.mass, &c.softTarget, &c.DmInv, &c.vol, &c.tetMu,
+                              &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
+                              &c.fricLambda, &c.fricCoord, &c.fricBasis, &c.fricGLambda, &c.closeGVal, &c.closeSVal, &c.dynGVal, &c.dynHValD,
+                              &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.sweptPt, &c.scratch, &c.scal, &c.energyBuf,
+                              &c.faceTree.lo, &c.faceTree.hi, &c.faceTree.primLo, &c.faceTree.primHi, &c.faceTree.sceneBox, &c.edgeTree.lo,
+                              &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox};
+        for (auto* d : ds) d->free();
+        DBuf<float>* fs[] = {&c.valF, &c.elemHF, &c.dynHValF, &c.dynBF, &c.rF, &c.zF, &c.pF, &c.ApF, &c.xF, &c.DinvF, &c.icVal};
+        for (auto* d : fs) d->free();
+        DBuf<int>* is[] = {&c.btype, &c.softIdx, &c.dirIdx, &c.tets, &c.tris, &c.bendV, &c.faces, &c.surfVerts, &c.edges, &c.rowPtr, &c.colIdx,
+                           &c.diagSlot, &c.hcPtr, &c.hcIdx, &c.gcPtr, &c.gcIdx, &c.selfActive, &c.selfEE, &c.eeIe, &c.ground, &c.counts, &c.runs,
+                           &c.counters, &c.fricSet, &c.fricGround, &c.closeG, &c.closeS, &c.dynGKey, &c.dynGKeyAlt, &c.dynGIdx, &c.dynGIdxAlt,
+                           &c.dynGStart, &c.dynGEnd, &c.dynHIdx, &c.dynHIdxAlt, &c.dynRowStart, &c.dynRowEnd, &c.dynCol, &c.dynSrcStart, &c.status,
+                           &c.faceTree.left, &c.faceTree.right, &c.faceTree.parent, &c.faceTree.leafPrim, &c.faceTree.flags, &c.faceTree.escape,
+                           &c.edgeTree.left, &c.edgeTree.right, &c.edgeTree.parent, &c.edgeTree.leafPrim, &c.edgeTree.flags, &c.edgeTree.escape};
+        for (auto* d : is) d->free();
+        DBuf<uint64_t>* us[] = {&c.ccdPT, &c.ccdEE, &c.kPT, &c.kEE, &c.kMoll, &c.kPPE, &c.kTmp, &c.uniq, &c.dynHKey, &c.dynHKeyAlt,
+                                &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
+        for (auto* d : us) d->free();
+        c.sortTmp.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
+        if (c.s) cudaStreamDestroy(c.s);
+        delete h->c;
+    }
+    delete h;
+}
+
+const char* cipc_gpu_last_error(const cipc_gpu_context* h) { return (h && h->c) ? h->c->lastError.c_str() : "invalid context"; }
+
+int cipc_gpu_step(cipc_gpu_context* h, cipc_step_stats* stats) {
+    return guarded(h, [&](Ctx& c) {
+        cipc_step_stats st;
+        solveIPCStep(c, st);
+        if (stats) *stats = st;
+    });
+}
+
+static DBuf<double>* stateBuf(Ctx& c, int which) {
+    switch (which) {
+    case 0: return &c.x; case 1: return &c.vel; case 2: return &c.vp; case 3: return &c.xt; case 4: return &c.rest;
+    default: throw InvalidArgument("unknown state field");
+    }
+}
+
+int cipc_gpu_get_state(cipc_gpu_context* h, int which, double* out) {
+    return guarded(h, [&](Ctx& c) {
+        if (!out) throw InvalidArgument("null output");
+        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        CIPC_CUDA(cudaMemcpy(out, stateBuf(c, which)->p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cipc_gpu_set_state(cipc_gpu_context* h, int which, const double* in) {
+    return guarded(h, [&](Ctx& c) {
+        if (!in) throw InvalidArgument("null input");
+        if (which == 4) throw InvalidArgument("rest positions are fixed at creation");
+        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        CIPC_CUDA(cudaMemcpy(stateBuf(c, which)->p, in, sizeof(double) * 3 * c.nv, cudaMemcpyHostToDevice));
+    });
+}
+
+int cipc_gpu_get_scalars(cipc_gpu_context* h, double* o) {
+    return guarded(h, [&](Ctx& c) {
+        const SimParams& P = c.P;
+        double v[14] = {P.kappa, P.Hhat, P.Fhat, P.dTol, P.bboxDiag2, P.meanMass, P.avgEdge, 0, 0, P.stretchS, P.shearS, P.plateRigidity, P.dt, P.newtonThr};
+        if (c.nt > 0) {
+            CIPC_CUDA(cudaMemcpy(&v[7], c.tetMu.p, sizeof(double), cudaMemcpyDeviceToHost));
+            CIPC_CUDA(cudaMemcpy(&v[8], c.tetLam.p, sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        std::memcpy(o, v, sizeof(v));
+    });
+}
+
+int cipc_gpu_set_kappa(cipc_gpu_context* h, double kappa) {
+    return guarded(h, [&](Ctx& c) { c.P.kappa = kappa; });
+}
+
+int cipc_gpu_get_counts(cipc_gpu_context* h, long long* o) {
+    return guarded(h, [&](Ctx& c) {
+        o[0] = c.nv; o[1] = c.nsf; o[2] = c.nsv; o[3] = c.nse; o[4] = c.nb; o[5] = c.nt; o[6] = c.nf; o[7] = c.nnzb; o[8] = c.nDynB;
+    });
+}
+
+int cipc_gpu_get_surface(cipc_gpu_context* h, int* faces, int* verts, int* edges) {
+    return guarded(h, [&](Ctx& c) {
+        CIPC_CUDA(cudaMemcpy(faces, c.faces.p, sizeof(int) * 3 * c.nsf, cudaMemcpyDeviceToHost));
+        CIPC_CUDA(cudaMemcpy(verts, c.surfVerts.p, sizeof(int) * c.nsv, cudaMemcpyDeviceToHost));
+        CIPC_CUDA(cudaMemcpy(edges, c.edges.p, sizeof(int) * 2 * c.nse, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cipc_gpu_build_collision_sets(cipc_gpu_context* h, long long* o) {
+    return guarded(h, [&](Ctx& c) {
+        buildCollisionSets(c, true);
+        sync(c);
+        if (o) { o[0] = c.nSelf; o[1] = c.nMoll; o[2] = (long long)c.nCcdPT + c.nCcdEE; o[3] = c.nGround; }
+    });
+}
+
+int cipc_gpu_get_active_sets(cipc_gpu_context* h, int* sa, int* see, int* eeie, int* ccd, int* gr) {
+    return guarded(h, [&](Ctx& c) {
+        sync(c);
+        if (sa && c.nSelf) CIPC_CUDA(cudaMemcpy(sa, c.selfActive.p, sizeof(int) * 4 * c.nSelf, cudaMemcpyDeviceToHost));
+        if (see && c.nMoll) CIPC_CUDA(cudaMemcpy(see, c.selfEE.p, sizeof(int) * 4 * c.nMoll, cudaMemcpyDeviceToHost));
+        if (eeie && c.nMoll) CIPC_CUDA(cudaMemcpy(eeie, c.eeIe.p, sizeof(int) * 2 * c.nMoll, cudaMemcpyDeviceToHost));
+        if (ccd) {
+            std::vector<uint64_t> a(c.nCcdPT), b(c.nCcdEE);
+            if (c.nCcdPT) CIPC_CUDA(cudaMemcpy(a.data(), c.ccdPT.p, sizeof(uint64_t) * c.nCcdPT, cudaMemcpyDeviceToHost));
+            if (c.nCcdEE) CIPC_CUDA(cudaMemcpy(b.data(), c.ccdEE.p, sizeof(uint64_t) * c.nCcdEE, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < c.nCcdPT; ++i) { ccd[2 * i] = -(int)(a[i] >> 32) - 1; ccd[2 * i + 1] = (int)(a[i] & 0xffffffffu); }
+            for (int i = 0; i < c.nCcdEE; ++i) {
+                ccd[2 * (c.nCcdPT + i)] = (int)(b[i] >> 32);
+                ccd[2 * (c.nCcdPT + i) + 1] = (int)(b[i] & 0xffffffffu);
+            }
+        }
+        if (gr && c.nGround) CIPC_CUDA(cudaMemcpy(gr, c.ground.p, sizeof(int) * c.nGround, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cipc_gpu_friction_init(cipc_gpu_context* h) {
+    return guarded(h, [&](Ctx& c) { frictionInitialize(c); sync(c); });
+}
+
+int cipc_gpu_assemble(cipc_gpu_context* h, double* grad, int* collisions) {
+    return guarded(h, [&](Ctx& c) {
+        int coll = assembleAll(c);
+        sync(c);
+        if (collisions) *collisions = coll;
+        if (grad) CIPC_CUDA(cudaMemcpy(grad, c.grad.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cipc_gpu_export_matrix(cipc_gpu_context* h, long long* count, int* rows, int* cols, double* vals) {
+    return guarded(h, [&](Ctx& c) {
+        sync(c);
+        long long n = 9LL * (c.nnzb + c.nDynB + c.nv);
+        if (count) *count = n;
+        if (!rows) return;
+        std::vector<int> rp(c.nv + 1), col(c.nnzb), drs(c.nv), dre(c.nv), dcol(std::max(c.nDynB, 1));
+        std::vector<double> val(9 * (size_t)c.nnzb), dval(9 * (size_t)std::max(c.nDynB, 1)), diag(9 * (size_t)c.nv);
+        CIPC_CUDA(cudaMemcpy(rp.data(), c.rowPtr.p, sizeof(int) * (c.nv + 1), cudaMemcpyDeviceToHost));
+        CIPC_CUDA(cudaMemcpy(col.data(), c.colIdx.p, sizeof(int) * c.nnzb, cudaMemcpyDeviceToHost));
+        if (c.mixed) {
+            std::vector<float> f(9 * (size_t)c.nnzb);
+            CIPC_CUDA(cudaMemcpy(f.data(), c.valF.p, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < f.size(); ++i) val[i] = f[i];
+        } else {
+            CIPC_CUDA(cudaMemcpy(val.data(), c.valD.p, sizeof(double) * val.size(), cudaMemcpyDeviceToHost));
+        }
+        if (c.nDynB) {
+            CIPC_CUDA(cudaMemcpy(drs.data(), c.dynRowStart.p, sizeof(int) * c.nv, cudaMemcpyDeviceToHost));
+            CIPC_CUDA(cudaMemcpy(dre.data(), c.dynRowEnd.p, sizeof(int) * c.nv, cudaMemcpyDeviceToHost));
+            CIPC_CUDA(cudaMemcpy(dcol.data(), c.dynCol.p, sizeof(int) * c.nDynB, cudaMemcpyDeviceToHost));
+            if (c.mixed) {
+                std::vector<float> f(9 * (size_t)c.nDynB);
+                CIPC_CUDA(cudaMemcpy(f.data(), c.dynBF.p, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < f.size(); ++i) dval[i] = f[i];
+            } else {
+                CIPC_CUDA(cudaMemcpy(dval.data(), c.dynBD.p, sizeof(double) * 9 * c.nDynB, cudaMemcpyDeviceToHost));
+            }
+        }
+        CIPC_CUDA(cudaMemcpy(diag.data(), c.diagExtra.p, sizeof(double) * diag.size(), cudaMemcpyDeviceToHost));
+        long long k = 0;
+        auto put = [&](int r, int cl, const double* B) {
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) { rows[k] = 3 * r + a; cols[k] = 3 * cl + b; vals[k] = B[3 * a + b]; ++k; }
+        };
+        for (int r = 0; r < c.nv; ++r) {
+            for (int q = rp[r]; q < rp[r + 1]; ++q) put(r, col[q], &val[9 * (size_t)q]);
+            if (c.nDynB) for (int q = drs[r]; q < dre[r]; ++q) put(r, dcol[q], &dval[9 * (size_t)q]);
+            put(r, r, &diag[9 * (size_t)r]);
+        }
+        if (count) *count = k;
+    });
+}
+
+int cipc_gpu_solve(cipc_gpu_context* h, double* direction, int* iterations, double* relRes) {
+    return guarded(h, [&](Ctx& c) {
+        linearSolve(c);
+        sync(c);
+        if (direction) CIPC_CUDA(cudaMemcpy(direction, c.dir.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToHost));
+        if (iterations) *iterations = c.lastPcgIters;
+        if (relRes) *relRes = c.lastPcgRelRes;
+    });
+}
+
+int cipc_gpu_energy(cipc_gpu_context* h, double kappa, double* e) {
+    return guarded(h, [&](Ctx& c) { *e = totalEnergy(c, kappa); });
+}
+
+int cipc_gpu_step_bounds(cipc_gpu_context* h, const double* dir, double alphaIn, double* out) {
+    return guarded(h, [&](Ctx& c) {
+        CIPC_CUDA(cudaMemcpy(c.dir.p, dir, sizeof(double) * 3 * c.nv, cudaMemcpyHostToDevice));
+        out[0] = std::min(1.0, groundStepBound(c));
+        out[1] = partialCCD(c, alphaIn);
+        out[2] = cflBound(c);
+        out[3] = fullCCD(c, alphaIn);
+        rebuildTrees(c);
+        sync(c);
+    });
+}
+
+int cipc_gpu_timed_steps(cipc_gpu_context* h, int nsteps, cipc_step_stats* last, double* deviceMs) {
+    return guarded(h, [&](Ctx& c) {
+        if (nsteps <= 0) throw InvalidArgument("nsteps must be positive");
+        cudaEvent_t a, b;
+        CIPC_CUDA(cudaEventCreate(&a));
+        CIPC_CUDA(cudaEventCreate(&b));
+        CIPC_CUDA(cudaEventRecord(a, c.s));
+        cipc_step_stats st;
+        try {
+            for (int k = 0; k < nsteps; ++k) solveIPCStep(c, st);
+        } catch (...) {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            throw;
+        }
+        CIPC_CUDA(cudaEventRecord(b, c.s));
+        CIPC_CUDA(cudaEventSynchronize(b));
+        float msf = 0;
+        CIPC_CUDA(cudaEventElapsedTime(&msf, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (last) *last = st;
+        if (deviceMs) *deviceMs = msf;
+    });
+}
+
+int cipc_gpu_profile(cipc_gpu_context* h, int kind, int capacity) {
+    return guarded(h, [&](Ctx& c) {
+        sync(c);
+        for (cudaEvent_t e : c.profEv) cudaEventDestroy(e);
+        c.profEv.clear();
+        c.profUsed = 0;
+        c.profKind = kind;
+        if (kind == PROF_NONE) return;
+        if (capacity <= 0) throw InvalidArgument("capacity must be positive");
+        c.profEv.resize(2 * (size_t)capacity);
+        for (auto& e : c.profEv) CIPC_CUDA(cudaEventCreate(&e));
+    });
+}
+
+int cipc_gpu_profile_read(cipc_gpu_context* h, long long* launches, double* totalMs) {
+    return guarded(h, [&](Ctx& c) {
+        sync(c);
+        double tot = 0;
+        for (int i = 0; i + 1 < c.profUsed; i += 2) {
+            float m = 0;
+            CIPC_CUDA(cudaEventElapsedTime(&m, c.profEv[i], c.profEv[i + 1]));
+            tot += m;
+        }
+        if (launches) *launches = c.profUsed / 2;
+        if (totalMs) *totalMs = tot;
+    });
+}
+
+long long cipc_gpu_kernel_launches(void) { return g_kernelLaunches; }
+
+int cipc_gpu_intersected(cipc_gpu_context* h, int* result) {
+    return guarded(h, [&](Ctx& c) {
+        rebuildTrees(c);
+        *result = isIntersected(c) ? 1 : 0;
+    });
+}
+
+}  // extern "C"
+
+extern "C" int cipc_gpu_pcg_bsr(int nv, const int* rowPtr, const int* colIdx, const double* vals, const double* rhs, double* sol,
+                                const cipc_linear_options* options, int* iterations, double* relResidual, char* err, int errlen) {
+    auto fail = [&](const char* m, int code) {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", m);
+        return code;
+    };
+    if (nv <= 0 || !rowPtr || !colIdx || !vals || !rhs || !sol) return fail("invalid arguments", CIPC_ERR_INVALID_ARGUMENT);
+    Ctx c;
+    try {
+        c.nv = nv;
+        if (options) {
+            c.pcgTol = options->relativeTolerance > 0 ? options->relativeTolerance : 1e-6;
+            c.pcgMaxIter = options->maximumIterations > 0 ? options->maximumIterations : 10000;
+            c.mixed = options->precision == CIPC_PRECISION_MIXED;
+        }
+        int nnzb = rowPtr[nv];
+        c.nnzb = nnzb;
+        std::vector<int> rp(rowPtr, rowPtr + nv + 1), ci(colIdx, colIdx + nnzb), diag(nv, -1);
+        for (int r = 0; r < nv; ++r)
+            for (int k = rp[r]; k < rp[r + 1]; ++k) {
+                if (ci[k] < 0 || ci[k] >= nv) return fail("column index out of range", CIPC_ERR_INVALID_ARGUMENT);
+                if (ci[k] == r) diag[r] = k;
+            }
+        CIPC_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        upload(c.rowPtr, rp); upload(c.colIdx, ci); upload(c.diagSlot, diag);
+        std::vector<double> v(vals, vals + 9 * (size_t)nnzb);
+        if (c.mixed) {
+            std::vector<float> f(v.begin(), v.end());
+            upload(c.valF, f);
+        } else {
+            upload(c.valD, v);
+        }
+        upload(c.diagExtra, std::vector<double>(9 * (size_t)nv, 0.0));
+        upload(c.rhs, std::vector<double>(rhs, rhs + 3 * (size_t)nv));
+        c.counters.reserve(16);
+        c.status.reserve(4);
+        int it = pcgSolve(c);
+        CIPC_CUDA(cudaMemcpy(sol, c.sol.p, sizeof(double) * 3 * nv, cudaMemcpyDeviceToHost));
+        if (iterations) *iterations = it;
+        if (relResidual) *relResidual = c.lastPcgRelRes;
+    } catch (const std::exception& e) {
+        int code = std::string(e.what()).find("did not converge") != std::string::npos ? CIPC_ERR_NOT_CONVERGED : CIPC_ERR_CUDA;
+        c.rowPtr.free(); c.colIdx.free(); c.diagSlot.free(); c.valD.free(); c.valF.free(); c.diagExtra.free(); c.rhs.free();
+        c.sol.free(); c.r.free(); c.z.free(); c.p.free(); c.Ap.free(); c.Dinv.free(); c.red.free(); c.scal.free(); c.counters.free(); c.status.free();
+        if (c.s) cudaStreamDestroy(c.s);
+        return fail(e.what(), code);
+    }
+    c.rowPtr.free(); c.colIdx.free(); c.diagSlot.free(); c.valD.free(); c.valF.free(); c.diagExtra.free(); c.rhs.free();
+    c.sol.free(); c.r.free(); c.z.free(); c.p.free(); c.Ap.free(); c.Dinv.free(); c.red.free(); c.scal.free(); c.counters.free(); c.status.free();
+    if (c.s) cudaStreamDestroy(c.s);
+    return CIPC_OK;
+}

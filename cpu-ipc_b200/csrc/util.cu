@@ -1,0 +1,96 @@
+// Deterministic device reductions (the partition depends only on n, so the
+// summation order is reproducible) and the status-word check.
+#include "cipc_device.cuh"
+#include "cipc_internal.h"
+
+#include <algorithm>
+#include <cstdio>
+
+namespace cipc {
+
+namespace {
+constexpr int RB = 256;
+
+template <int OP>
+__device__ __forceinline__ double combine(double a, double b) {
+    if (OP == 0) return a + b;
+    if (OP == 1) return a > b ? a : b;
+    if (OP == 2) return a < b ? a : b;
+    return a + b;
+}
+template <int OP>
+__device__ __forceinline__ double ident() { return OP == 2 ? 1e308 : (OP == 1 ? -1e308 : 0.0); }
+
+// OP: 0 sum, 1 max, 2 min, 3 dot(a,b), 4 max |a|
+template <int OP>
+__global__ void partialKernel(const double* a, const double* b, int n, int chunk, double* part) {
+    const int OPC = (OP == 3 ? 0 : (OP == 4 ? 1 : OP));
+    double acc = ident<OPC>();
+    int beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        double v = OP == 3 ? a[i] * b[i] : (OP == 4 ? fabs(a[i]) : a[i]);
+        acc = combine<OPC>(acc, v);
+    }
+    __shared__ double sh[RB];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = RB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = combine<OPC>(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+template <int OPC>
+__global__ void finalKernel(const double* part, int np, double* out) {
+    __shared__ double sh[RB];
+    double acc = ident<OPC>();
+    for (int i = threadIdx.x; i < np; i += RB) acc = combine<OPC>(acc, part[i]);
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = RB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = combine<OPC>(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+template <int OP>
+double reduce(Ctx& c, const double* a, const double* b, int n) {
+    const int OPC = (OP == 3 ? 0 : (OP == 4 ? 1 : OP));
+    if (n <= 0) return OPC == 2 ? 1e308 : (OPC == 1 ? -1e308 : 0.0);
+    int nb = std::min(1024, (n + 4 * RB - 1) / (4 * RB));
+    int chunk = (n + nb - 1) / nb;
+    c.scratch.reserve(nb + 8);
+    launch(partialKernel<OP>, nb, RB, 0, c.s, a, b, n, chunk, c.scratch.p + 8);
+    launch(finalKernel<OPC>, 1, RB, 0, c.s, c.scratch.p + 8, nb, c.scratch.p);
+    double h;
+    CIPC_CUDA(cudaMemcpyAsync(&h, c.scratch.p, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    return h;
+}
+}  // namespace
+
+double deviceSum(Ctx& c, const double* v, int n) { return reduce<0>(c, v, nullptr, n); }
+double deviceMax(Ctx& c, const double* v, int n) { return reduce<1>(c, v, nullptr, n); }
+double deviceMin(Ctx& c, const double* v, int n, double init) { return std::min(init, reduce<2>(c, v, nullptr, n)); }
+double deviceDot(Ctx& c, const double* a, const double* b, int n) { return reduce<3>(c, a, b, n); }
+double deviceInfNorm(Ctx& c, const double* v, int n) { return std::max(0.0, reduce<4>(c, v, nullptr, n)); }
+
+void checkStatus(Ctx& c, const char* stage) {
+    int st = 0;
+    CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    if (st) {
+        CIPC_CUDA(cudaMemsetAsync(c.status.p, 0, sizeof(int), c.s));
+        std::string msg = std::string("device status in ") + stage + ":";
+        if (st & CIPC_ST_NONFINITE) msg += " non-finite value;";
+        if (st & CIPC_ST_STACK_OVERFLOW) msg += " BVH traversal stack overflow;";
+        if (st & CIPC_ST_CAPACITY) msg += " candidate buffer capacity exceeded;";
+        if (st & CIPC_ST_CCD_CAP) msg += " CCD iteration cap;";
+        if (st & CIPC_ST_JACOBI_CAP) msg += " eigen-solver sweep cap;";
+        throw std::runtime_error(msg);
+    }
+}
+
+}  // namespace cipc

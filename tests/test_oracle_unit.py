@@ -1,0 +1,109 @@
+"""Unit checks of the oracle's building blocks (no GPU): exact distance
+derivatives against finite differences, the PSD projection of the Stable
+Neo-Hookean Hessian, additive CCD conservativeness, and the active set built
+through the LBVH against a brute-force pair enumeration."""
+import numpy as np
+import pytest
+
+import cipc
+
+
+def _fd(kind, pts, h=1e-6):
+    import oracle
+    d0, g0, H0 = oracle.distance(kind, pts)
+    n = len(g0)
+    p = np.asarray(pts, float).reshape(-1)
+    gfd = np.zeros(n)
+    Hfd = np.zeros((n, n))
+    for i in range(n):
+        e = np.zeros(n); e[i] = h
+        dp, gp, _ = oracle.distance(kind, p + e)
+        dm, gm, _ = oracle.distance(kind, p - e)
+        gfd[i] = (dp - dm) / (2 * h)
+        Hfd[:, i] = (gp - gm) / (2 * h)
+    return g0, H0, gfd, Hfd
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
+def test_distance_derivatives_match_finite_differences(oracle_mod, kind):
+    rng = np.random.default_rng(kind)
+    npt = {0: 2, 1: 3}.get(kind, 4)
+    for _ in range(5):
+        pts = rng.standard_normal((npt, 3))
+        g, H, gfd, Hfd = _fd(kind, pts)
+        assert np.allclose(g, gfd, rtol=1e-6, atol=1e-7 * max(1, np.abs(g).max()))
+        assert np.allclose(H, Hfd, rtol=1e-5, atol=1e-6 * max(1, np.abs(H).max()))
+        assert np.allclose(H, H.T, atol=1e-12 * max(1, np.abs(H).max()))
+
+
+def test_snh_hessian_is_psd_projection(oracle_mod):
+    rng = np.random.default_rng(3)
+    u, r = 5e4, 2e5
+    for _ in range(20):
+        F = np.eye(3) + 0.6 * rng.standard_normal((3, 3))
+        P, H, psi = oracle_mod.snh(F, u, r)
+        w = np.linalg.eigvalsh(H)
+        assert w.min() > -1e-9 * max(1.0, w.max())
+        # PK1 is the derivative of the energy density
+        h = 1e-6
+        Pfd = np.zeros((3, 3))
+        for i in range(3):
+            for j in range(3):
+                E = np.zeros((3, 3)); E[i, j] = h
+                Pfd[i, j] = (oracle_mod.snh(F + E, u, r)[2] - oracle_mod.snh(F - E, u, r)[2]) / (2 * h)
+        assert np.allclose(P, Pfd, rtol=1e-5, atol=1e-4)
+
+
+def test_accd_is_conservative(oracle_mod):
+    # a point falling through a triangle: TOI must stop short of the plane
+    p = np.array([[0.2, 1.0, 0.2], [0, 0, 0], [1, 0, 0], [0, 0, 1]], float)
+    d = np.array([[0, -2.0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]], float)
+    t = oracle_mod.pt_ccd(p, d, 0.2)
+    assert 0.0 < t < 0.5
+    # separating motion gives the full step
+    assert oracle_mod.pt_ccd(p, -d, 0.2) == 1.0
+    a = np.array([[-1, 1, 0], [1, 1, 0], [0, 0, -1], [0, 0, 1]], float)
+    da = np.array([[0, -2, 0], [0, -2, 0], [0, 0, 0], [0, 0, 0]], float)
+    te = oracle_mod.ee_ccd(a, da, 0.2)
+    assert 0.0 < te < 0.5
+
+
+def _brute_pairs(x, faces, verts, edges, btype, gap):
+    lo_f = x[faces].min(1); hi_f = x[faces].max(1)
+    pt = set()
+    for si, v in enumerate(verts):
+        p = x[v]
+        ok = ~((lo_f - p > gap).any(1) | (p - hi_f > gap).any(1))
+        for f in np.nonzero(ok)[0]:
+            F = faces[f]
+            if v in F:
+                continue
+            if btype[v] >= 2 and (btype[F] >= 2).all():
+                continue
+            pt.add((-si - 1, int(f)))
+    lo_e = x[edges].min(1); hi_e = x[edges].max(1)
+    ee = set()
+    for i in range(len(edges)):
+        ok = ~((lo_e - hi_e[i] > gap).any(1) | (lo_e[i] - hi_e > gap).any(1))
+        for j in np.nonzero(ok)[0]:
+            if j <= i or len(set(edges[i]) & set(edges[j])):
+                continue
+            if (btype[edges[i]] >= 2).all() and (btype[edges[j]] >= 2).all():
+                continue
+            ee.add((i, int(j)))
+    return pt | ee
+
+
+def test_lbvh_candidates_equal_brute_force(oracle_mod):
+    sc = cipc.scene_two_cubes(2, gap=0.002)
+    o = oracle_mod.Oracle(sc)
+    rng = np.random.default_rng(0)
+    x = o.get("x") + 1e-3 * rng.standard_normal((o.nv, 3))
+    o.set("x", x)
+    s = o.collision_sets()
+    faces, verts, edges = o.surface()
+    gap = np.sqrt(o.scalars()["Hhat"]) * 30
+    got = set(map(tuple, s["ccd"].tolist()))
+    # the oracle's gap is sqrt(Hhat); rebuild the brute force with the same gap
+    want = _brute_pairs(x, faces, verts, edges, sc["btype"], np.sqrt(o.scalars()["Hhat"]))
+    assert got == want
