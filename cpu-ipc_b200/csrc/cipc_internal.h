@@ -149,7 +149,7 @@ struct Ctx {
     DBuf<unsigned char> sortTmp;
 
     // PCG
-    DBuf<double> rhs, sol, r, z, p, Ap, Dinv, red;
+    DBuf<double> rhs, sol, r, z, p, Ap, Dinv, red, corrX, corrR;
     DBuf<float> rF, zF, pF, ApF, xF, DinvF;
     int lastPcgIters = 0;
     double lastPcgRelRes = 0;

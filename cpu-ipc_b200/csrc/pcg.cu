@@ -9,6 +9,11 @@
 // one coalesced run) and combine with shuffles.  Dot products reduce per block
 // into partials; the next kernel sums the partials in a fixed order, so no
 // host round trip is needed inside an iteration and results are reproducible.
+//
+// Mixed precision: FP32 blocks, FP32 vectors and FP32 SpMV accumulation in an
+// inner PCG, wrapped in FP64 iterative refinement: the outer loop recomputes
+// the true residual b - A x in FP64 (FP32 blocks promoted) and stops on the
+// same FP64 criterion as the FP64 solver.
 #include "cipc_device.cuh"
 #include "cipc_internal.h"
 
@@ -126,16 +131,17 @@ __device__ __forceinline__ void applyDinv(const double* Dinv, const VT* r, VT* z
     z[3 * v + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
 }
 
-// scal layout: 0 rz, 1 (unused), 2 thr, 3 rr, 4 iterations, 5 converged flag (int view), 6 rhs2
-__global__ void pcgInitKernel(int nv, const double* b, const double* Dinv, double* x, double* r, double* z, double* p, double* part0, double* part1) {
+// scal layout: 0 rz, 1 beta, 2 thr, 3 rr, 4 iterations, 6 rhs2
+template <class VT>
+__global__ void pcgInitKernel(int nv, const VT* b, const double* Dinv, VT* x, VT* r, VT* z, VT* p, double* part0, double* part1) {
     double rr = 0, rz = 0;
     CIPC_KERNEL_LOOP(v, nv) {
-        for (int q = 0; q < 3; ++q) { x[3 * v + q] = 0.0; r[3 * v + q] = b[3 * v + q]; }
+        for (int q = 0; q < 3; ++q) { x[3 * v + q] = VT(0); r[3 * v + q] = b[3 * v + q]; }
         applyDinv(Dinv, r, z, v);
         for (int q = 0; q < 3; ++q) {
             p[3 * v + q] = z[3 * v + q];
-            rr += r[3 * v + q] * r[3 * v + q];
-            rz += r[3 * v + q] * z[3 * v + q];
+            rr += (double)r[3 * v + q] * (double)r[3 * v + q];
+            rz += (double)r[3 * v + q] * (double)z[3 * v + q];
         }
     }
     double a = blockReduce(rr, AddOp(), 0.0);
@@ -159,10 +165,11 @@ __global__ void pcgInitScalars(const double* part0, const double* part1, int np,
 }
 
 // x += a p ; r -= a Ap ; z = M r ; partials of r.r and r.z
-__global__ void pcgUpdateKernel(int nv, const double* pAp, int np, const double* scal, const double* Dinv, const double* p, const double* Ap, double* x,
-                                double* r, double* z, double* partRR, double* partRZ, const int* flag) {
+template <class VT>
+__global__ void pcgUpdateKernel(int nv, const double* pAp, int np, const double* scal, const double* Dinv, const VT* p, const VT* Ap, VT* x, VT* r,
+                                VT* z, double* partRR, double* partRZ, const int* flag) {
     if (*flag) return;
-    double alpha = scal[0] / sumPartials(pAp, np);
+    VT alpha = (VT)(scal[0] / sumPartials(pAp, np));
     double rr = 0, rz = 0;
     CIPC_KERNEL_LOOP(v, nv) {
         for (int q = 0; q < 3; ++q) {
@@ -170,7 +177,10 @@ __global__ void pcgUpdateKernel(int nv, const double* pAp, int np, const double*
             r[3 * v + q] -= alpha * Ap[3 * v + q];
         }
         applyDinv(Dinv, r, z, v);
-        for (int q = 0; q < 3; ++q) { rr += r[3 * v + q] * r[3 * v + q]; rz += r[3 * v + q] * z[3 * v + q]; }
+        for (int q = 0; q < 3; ++q) {
+            rr += (double)r[3 * v + q] * (double)r[3 * v + q];
+            rz += (double)r[3 * v + q] * (double)z[3 * v + q];
+        }
     }
     double a = blockReduce(rr, AddOp(), 0.0);
     __syncthreads();
@@ -193,9 +203,10 @@ __global__ void pcgScalarKernel(const double* partRR, const double* partRZ, int 
     }
 }
 
-__global__ void pcgDirKernel(int nv, const double* scal, const double* z, double* p, const int* flag) {
+template <class VT>
+__global__ void pcgDirKernel(int nv, const double* scal, const VT* z, VT* p, const int* flag) {
     if (*flag == 1) return;
-    double beta = scal[1];
+    VT beta = (VT)scal[1];
     CIPC_KERNEL_LOOP(i, 3 * nv) p[i] = z[i] + beta * p[i];
 }
 
@@ -206,6 +217,31 @@ __global__ void rhsKernel(int nv, const double* g, const int* btype, double* b) 
     }
 }
 
+// r = b - Ax (FP64), rF = (float) r, partial |r|^2
+__global__ void residualKernel(int n3, const double* b, const double* Ax, double* r, float* rF, double* part) {
+    double rr = 0;
+    CIPC_KERNEL_LOOP(i, n3) {
+        double v = b[i] - Ax[i];
+        r[i] = v;
+        rF[i] = (float)v;
+        rr += v * v;
+    }
+    double s = blockReduce(rr, AddOp(), 0.0);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void accumulateKernel(int n3, const float* d, double* x) {
+    CIPC_KERNEL_LOOP(i, n3) x[i] += (double)d[i];
+}
+
+__global__ void accumulateKernelD(int n3, const double* d, double* x) {
+    CIPC_KERNEL_LOOP(i, n3) x[i] += d[i];
+}
+
+__global__ void zeroKernel(int n3, double* x) {
+    CIPC_KERNEL_LOOP(i, n3) x[i] = 0.0;
+}
+
 }  // namespace
 
 void buildRhs(Ctx& c) {
@@ -214,43 +250,46 @@ void buildRhs(Ctx& c) {
     CIPC_CUDA(cudaGetLastError());
 }
 
-template <class MT>
-static void spmvT(Ctx& c, const MT* val, const MT* dval, const double* x, double* y, double* partial, const int* flag, int nblk) {
+template <class MT, class VT>
+static void spmvT(Ctx& c, const MT* val, const MT* dval, const VT* x, VT* y, double* partial, const int* flag, int nblk) {
     bool dyn = c.nDynB > 0;
-    launch(spmvKernel<MT, double>, nblk, VB, 0, c.s, c.nv, c.rowPtr, c.colIdx, val, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
-                                                 dyn ? c.dynCol.p : nullptr, dval, c.diagExtra, x, y, partial, flag);
+    launch(spmvKernel<MT, VT>, nblk, VB, 0, c.s, c.nv, c.rowPtr, c.colIdx, val, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
+           dyn ? c.dynCol.p : nullptr, dval, c.diagExtra, x, y, partial, flag);
 }
 
 static int spmvBlocks(Ctx& c) { return std::max(1, std::min((c.nv * GROUP + VB - 1) / VB, MAXPART)); }
 
 void spmv(Ctx& c, const double* x, double* y) {
-    if (c.mixed) spmvT<float>(c, c.valF, c.dynBF, x, y, nullptr, nullptr, spmvBlocks(c));
-    else spmvT<double>(c, c.valD, c.dynBD, x, y, nullptr, nullptr, spmvBlocks(c));
+    if (c.mixed) spmvT<float, double>(c, c.valF, c.dynBF, x, y, nullptr, nullptr, spmvBlocks(c));
+    else spmvT<double, double>(c, c.valD, c.dynBD, x, y, nullptr, nullptr, spmvBlocks(c));
     CIPC_CUDA(cudaGetLastError());
 }
 
-// FP64 PCG (mixed mode: FP32 matrix blocks promoted in the FP64 SpMV).
-int pcgSolve(Ctx& c) {
+static void computeDinv(Ctx& c) {
     int nv = c.nv;
-    size_t n3 = 3 * (size_t)nv;
-    c.sol.reserve(n3); c.r.reserve(n3); c.z.reserve(n3); c.p.reserve(n3); c.Ap.reserve(n3); c.Dinv.reserve(9 * (size_t)nv);
-    c.red.reserve(4 * MAXPART + 16);
-    c.scal.reserve(16);
-    c.counters.reserve(16);
     bool dyn = c.nDynB > 0;
+    c.Dinv.reserve(9 * (size_t)nv);
     if (c.mixed)
         launch(dinvKernel<float>, vecBlocks(nv), VB, 0, c.s, nv, c.diagSlot, c.valF, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
-                                                         dyn ? c.dynCol.p : nullptr, c.dynBF, c.diagExtra, c.Dinv);
+               dyn ? c.dynCol.p : nullptr, c.dynBF, c.diagExtra, c.Dinv);
     else
         launch(dinvKernel<double>, vecBlocks(nv), VB, 0, c.s, nv, c.diagSlot, c.valD, dyn ? c.dynRowStart.p : nullptr, dyn ? c.dynRowEnd.p : nullptr,
-                                                          dyn ? c.dynCol.p : nullptr, c.dynBD, c.diagExtra, c.Dinv);
+               dyn ? c.dynCol.p : nullptr, c.dynBD, c.diagExtra, c.Dinv);
+}
+
+// PCG on A x = b with vectors of type VT and blocks of type MT.  Returns the
+// iteration count; *relRes gets sqrt(rr/rhs2) of the last recursive residual.
+template <class MT, class VT>
+static int runPcg(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT* r, VT* z, VT* p, VT* Ap, double tol, int maxIter,
+                  int& flagOut, double& relRes) {
+    int nv = c.nv;
     int vb = vecBlocks(nv), sb = spmvBlocks(c);
     double* partA = c.red.p;
     double* partB = c.red.p + MAXPART;
     double* partC = c.red.p + 2 * MAXPART;
     int* flag = c.counters.p + 10;
-    launch(pcgInitKernel, vb, VB, 0, c.s, nv, c.rhs, c.Dinv, c.sol, c.r, c.z, c.p, partA, partB);
-    launch(pcgInitScalars, 1, VB, 0, c.s, partA, partB, vb, c.pcgTol, c.scal, flag);
+    launch(pcgInitKernel<VT>, vb, VB, 0, c.s, nv, b, c.Dinv, x, r, z, p, partA, partB);
+    launch(pcgInitScalars, 1, VB, 0, c.s, partA, partB, vb, tol, c.scal, flag);
     CIPC_CUDA(cudaGetLastError());
     const int chunk = 16;
     int it = 0;
@@ -259,12 +298,11 @@ int pcgSolve(Ctx& c) {
     while (true) {
         for (int k = 0; k < chunk; ++k) {
             profBegin(c, PROF_SPMV);
-            if (c.mixed) spmvT<float>(c, c.valF, c.dynBF, c.p, c.Ap, partC, flag, sb);
-            else spmvT<double>(c, c.valD, c.dynBD, c.p, c.Ap, partC, flag, sb);
+            spmvT<MT, VT>(c, val, dval, p, Ap, partC, flag, sb);
             profEnd(c, PROF_SPMV);
-            launch(pcgUpdateKernel, vb, VB, 0, c.s, nv, partC, sb, c.scal, c.Dinv, c.p, c.Ap, c.sol, c.r, c.z, partA, partB, flag);
-            launch(pcgScalarKernel, 1, VB, 0, c.s, partA, partB, vb, c.scal, flag, c.pcgMaxIter);
-            launch(pcgDirKernel, vb, VB, 0, c.s, nv, c.scal, c.z, c.p, flag);
+            launch(pcgUpdateKernel<VT>, vb, VB, 0, c.s, nv, partC, sb, c.scal, c.Dinv, p, Ap, x, r, z, partA, partB, flag);
+            launch(pcgScalarKernel, 1, VB, 0, c.s, partA, partB, vb, c.scal, flag, maxIter);
+            launch(pcgDirKernel<VT>, vb, VB, 0, c.s, nv, c.scal, z, p, flag);
         }
         CIPC_CUDA(cudaGetLastError());
         CIPC_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, c.s));
@@ -273,13 +311,89 @@ int pcgSolve(Ctx& c) {
         it = (int)hs[4];
         if (hflag) break;
     }
-    double rhs2 = 0;
-    CIPC_CUDA(cudaMemcpy(&rhs2, c.scal.p + 6, sizeof(double), cudaMemcpyDeviceToHost));
-    c.lastPcgIters = it;
-    c.lastPcgRelRes = rhs2 > 0 ? std::sqrt(hs[3] / rhs2) : 0.0;
-    c.pcgItersTotal += it;
-    if (hflag == 2) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
+    flagOut = hflag;
+    relRes = hs[6] > 0 ? std::sqrt(hs[3] / hs[6]) : 0.0;
     return it;
 }
+
+static void reservePcg(Ctx& c) {
+    size_t n3 = 3 * (size_t)c.nv;
+    c.sol.reserve(n3); c.r.reserve(n3); c.z.reserve(n3); c.p.reserve(n3); c.Ap.reserve(n3);
+    c.red.reserve(4 * MAXPART + 16);
+    c.scal.reserve(16);
+    c.counters.reserve(16);
+}
+
+static int pcgSolve64(Ctx& c) {
+    reservePcg(c);
+    computeDinv(c);
+    int flag = 0;
+    double rel = 0;
+    int it = runPcg<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol, c.pcgMaxIter, flag, rel);
+    c.lastPcgIters = it;
+    c.lastPcgRelRes = rel;
+    c.pcgItersTotal += it;
+    if (flag == 2) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
+    return it;
+}
+
+// FP32 inner PCG + FP64 iterative refinement on the true residual.
+static int pcgSolveMixed(Ctx& c) {
+    reservePcg(c);
+    computeDinv(c);
+    int nv = c.nv;
+    int n3 = 3 * nv;
+    c.rF.reserve(n3); c.zF.reserve(n3); c.pF.reserve(n3); c.ApF.reserve(n3); c.xF.reserve(n3); c.DinvF.reserve(n3);
+    float* bF = c.DinvF.p;  // FP32 copy of the current residual (right-hand side of the correction)
+    int vb = vecBlocks(n3 / 3 + 1);
+    double* part = c.red.p + 3 * MAXPART;
+    launch(zeroKernel, vb, VB, 0, c.s, n3, c.sol.p);
+    double rhs2 = deviceDot(c, c.rhs, c.rhs, n3);
+    c.lastPcgIters = 0;
+    if (rhs2 == 0.0) { c.lastPcgRelRes = 0; return 0; }
+    double thr = std::max(c.pcgTol * c.pcgTol * rhs2, 2.2250738585072014e-308);
+    int total = 0;
+    double rr = rhs2;
+    const double innerTol = 1e-3;
+    double prevRR = 1e308;
+    for (int outer = 0; outer < 40; ++outer) {
+        // true residual r = b - A x in FP64 (x = 0 on the first pass)
+        spmvT<float, double>(c, c.valF, c.dynBF, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
+        int nb = vecBlocks(nv);
+        launch(residualKernel, nb, VB, 0, c.s, n3, c.rhs.p, c.Ap.p, c.r.p, bF, part);
+        rr = deviceSum(c, part, nb);
+        if (rr < thr) break;
+        if (!(rr < 0.25 * prevRR) && outer > 2) break;  // refinement stagnates: finish in FP64 below
+        prevRR = rr;
+        int flag = 0;
+        double rel = 0;
+        int it = runPcg<float, float>(c, c.valF, c.dynBF, bF, c.xF.p, c.rF.p, c.zF.p, c.pF.p, c.ApF.p,
+                                      std::max(innerTol, 0.5 * std::sqrt(thr / rr)), c.pcgMaxIter, flag, rel);
+        total += it;
+        launch(accumulateKernel, vb, VB, 0, c.s, n3, c.xF.p, c.sol.p);
+        if (total >= c.pcgMaxIter) break;
+    }
+    if (!(rr < thr)) {
+        // refinement stalled: finish with an FP64-vector PCG on the residual
+        // (FP32 blocks promoted) and add the correction
+        c.corrX.reserve(n3); c.corrR.reserve(n3);
+        int flag = 0;
+        double rel = 0;
+        int it = runPcg<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, std::sqrt(thr / rr),
+                                       c.pcgMaxIter, flag, rel);
+        total += it;
+        launch(accumulateKernelD, vb, VB, 0, c.s, n3, c.corrX.p, c.sol.p);
+        spmvT<float, double>(c, c.valF, c.dynBF, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
+        launch(residualKernel, vecBlocks(nv), VB, 0, c.s, n3, c.rhs.p, c.Ap.p, c.r.p, bF, part);
+        rr = deviceSum(c, part, vecBlocks(nv));
+        if (flag == 2 && !(rr < thr)) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
+    }
+    c.lastPcgIters = total;
+    c.lastPcgRelRes = std::sqrt(rr / rhs2);
+    c.pcgItersTotal += total;
+    return total;
+}
+
+int pcgSolve(Ctx& c) { return c.mixed ? pcgSolveMixed(c) : pcgSolve64(c); }
 
 }  // namespace cipc

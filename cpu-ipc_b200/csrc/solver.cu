@@ -525,7 +525,8 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
         DBuf<double>* ds[] = {&c.x, &c.x0, &c.xt, &c.vp, &c.vel, &c.rest, &c.dir, &c.grad, &c.mass, &c.softTarget, &c.DmInv, &c.vol, &c.tetMu,
                               &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
                               &c.fricLambda, &c.fricCoord, &c.fricBasis, &c.fricGLambda, &c.closeGVal, &c.closeSVal, &c.dynGVal, &c.dynHValD,
-                              &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.sweptPt, &c.scratch, &c.scal, &c.energyBuf,
+                              &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.corrX, &c.corrR, &c.sweptPt, &c.scratch,
+                              &c.scal, &c.energyBuf,
                               &c.faceTree.lo, &c.faceTree.hi, &c.faceTree.primLo, &c.faceTree.primHi, &c.faceTree.sceneBox, &c.edgeTree.lo,
                               &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox};
         for (auto* d : ds) d->free();
@@ -542,6 +543,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();
         c.sortTmp.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
+        for (cudaEvent_t e : c.profEv) cudaEventDestroy(e);
         if (c.s) cudaStreamDestroy(c.s);
         delete h->c;
     }
