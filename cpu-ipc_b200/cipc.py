@@ -114,7 +114,7 @@ EXPORTED_SYMBOLS = [
     "cipc_gpu_kernel_launches",
 ]
 
-PROFILE_KINDS = {"spmv": 1, "tet": 2, "tri": 3, "slot": 4, "barrier": 5, "active": 6, "fullccd": 7}
+PROFILE_KINDS = {"spmv": 1, "tet": 2, "tri": 3, "slot": 4, "barrier": 5, "active": 6, "fullccd": 7, "pcg": 8}
 
 
 def kernel_launches():

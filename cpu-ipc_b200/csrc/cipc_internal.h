@@ -31,7 +31,9 @@ inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
 // Optional CUDA-event timing of one kernel family on the context's stream:
 // when enabled, launches of that family are bracketed by events from a
 // pool, read back after the timed region.
-enum ProfileKind { PROF_NONE = 0, PROF_SPMV = 1, PROF_TET = 2, PROF_TRI = 3, PROF_SLOT = 4, PROF_BARRIER = 5, PROF_ACTIVE = 6, PROF_FULLCCD = 7 };
+enum ProfileKind {
+    PROF_NONE = 0, PROF_SPMV = 1, PROF_TET = 2, PROF_TRI = 3, PROF_SLOT = 4, PROF_BARRIER = 5, PROF_ACTIVE = 6, PROF_FULLCCD = 7, PROF_PCG = 8
+};
 
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;

@@ -15,6 +15,7 @@
 // the true residual b - A x in FP64 (FP32 blocks promoted) and stops on the
 // same FP64 criterion as the FP64 solver.
 #include "cipc_device.cuh"
+#include "cipc_gpu.h"
 #include "cipc_internal.h"
 
 #include <algorithm>
@@ -234,6 +235,179 @@ __global__ void accumulateKernel(int n3, const float* d, double* x) {
     CIPC_KERNEL_LOOP(i, n3) x[i] += (double)d[i];
 }
 
+// ---------------------------------------------------------------------------
+// Persistent PCG: the whole CG loop in one cooperative launch.  Three grid
+// barriers per iteration (after SpMV, after the x/r/z update, after the p
+// update); every block sums the per-block partials in the same order, so all
+// blocks take the same branch and the result is reproducible.  The barrier
+// spin is bounded: on timeout it sets an error flag and the kernel returns.
+// ---------------------------------------------------------------------------
+template <class MT, class VT>
+struct PcgArgs {
+    int nv;
+    const int *rowPtr, *col;
+    const MT* val;
+    const int *dRowS, *dRowE, *dCol;
+    const MT* dVal;
+    const double* diagExtra;
+    const double* Dinv;
+    const VT* b;
+    VT *x, *r, *z, *p, *Ap;
+    double *partA, *partB, *partC;
+    double* scal;  // out: [3] rr, [4] iterations, [6] rhs2
+    int* flag;     // out: 1 converged, 2 iteration cap, 3 barrier timeout
+    unsigned *barCount, *barGen;
+    double tol;
+    int maxIter;
+};
+
+// sumPartials for partials written by other blocks of the same launch.
+__device__ __forceinline__ double sumPartialsCG(const double* p, int n) {
+    __shared__ double sh;
+    double v = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += __ldcg(p + i);
+    v = blockReduce(v, AddOp(), 0.0);
+    if (threadIdx.x == 0) sh = v;
+    __syncthreads();
+    return sh;
+}
+
+__device__ __forceinline__ bool gridBarrier(unsigned* count, unsigned* gen, int* flag, unsigned nblocks) {
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = gen;
+        unsigned g = *vgen;
+        __threadfence();
+        ok = 1;
+        if (atomicAdd(count, 1u) == nblocks - 1) {
+            atomicExch(count, 0u);
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            long long spins = 0;
+            while (*vgen == g) {
+                if (++spins > (1ll << 26)) { atomicExch(flag, 3); ok = 0; break; }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok && *(volatile int*)flag != 3;
+}
+
+template <class MT, class VT>
+__device__ __forceinline__ double spmvRows(const PcgArgs<MT, VT>& a, const VT* x, VT* y) {
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    int lane = threadIdx.x & (GROUP - 1);
+    int grp = (threadIdx.x & 31) / GROUP;
+    const int RPW = 32 / GROUP;
+    int nWarps = gridDim.x * blockDim.x / 32;
+    double dotAcc = 0;
+    for (int base = (gid / 32) * RPW; base < a.nv; base += nWarps * RPW) {
+        int row = base + grp;
+        bool active = row < a.nv;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        if (active) {
+            // vectors written by other blocks in this launch: L2 loads only
+            for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
+                int c = a.col[k];
+                VT xv[3] = {__ldcg(x + 3 * c), __ldcg(x + 3 * c + 1), __ldcg(x + 3 * c + 2)};
+                blockMulAdd(a.val + (size_t)9 * k, xv, acc);
+            }
+            if (a.dRowS) {
+                for (int k = a.dRowS[row] + lane; k < a.dRowE[row]; k += GROUP) {
+                    int c = a.dCol[k];
+                    VT xv[3] = {__ldcg(x + 3 * c), __ldcg(x + 3 * c + 1), __ldcg(x + 3 * c + 2)};
+                    blockMulAdd(a.dVal + (size_t)9 * k, xv, acc);
+                }
+            }
+        }
+        for (int o = GROUP / 2; o > 0; o >>= 1)
+            for (int q = 0; q < 3; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o, GROUP);
+        if (active && lane == 0) {
+            VT xv[3] = {__ldcg(x + 3 * row), __ldcg(x + 3 * row + 1), __ldcg(x + 3 * row + 2)};
+            const double* D = a.diagExtra + 9 * row;
+            for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)xv[0] + D[3 * q + 1] * (double)xv[1] + D[3 * q + 2] * (double)xv[2]);
+            for (int q = 0; q < 3; ++q) {
+                y[3 * row + q] = acc[q];
+                dotAcc += (double)xv[q] * (double)acc[q];
+            }
+        }
+    }
+    return dotAcc;
+}
+
+template <class MT, class VT>
+__global__ void __launch_bounds__(256) pcgPersistentKernel(PcgArgs<MT, VT> a) {
+    const unsigned nb = gridDim.x;
+    const int nv = a.nv;
+    // init: x = 0, r = b, z = M r, p = z
+    double rr = 0, rz = 0;
+    CIPC_KERNEL_LOOP(v, nv) {
+        for (int q = 0; q < 3; ++q) { a.x[3 * v + q] = VT(0); a.r[3 * v + q] = a.b[3 * v + q]; }
+        applyDinv(a.Dinv, a.r, a.z, v);
+        for (int q = 0; q < 3; ++q) {
+            a.p[3 * v + q] = a.z[3 * v + q];
+            rr += (double)a.r[3 * v + q] * (double)a.r[3 * v + q];
+            rz += (double)a.r[3 * v + q] * (double)a.z[3 * v + q];
+        }
+    }
+    {
+        double s1 = blockReduce(rr, AddOp(), 0.0);
+        __syncthreads();
+        double s2 = blockReduce(rz, AddOp(), 0.0);
+        if (threadIdx.x == 0) { a.partA[blockIdx.x] = s1; a.partB[blockIdx.x] = s2; }
+    }
+    if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
+    rr = sumPartialsCG(a.partA, nb);
+    rz = sumPartialsCG(a.partB, nb);
+    const double rhs2 = rr;
+    const double thr = fmax(a.tol * a.tol * rr, 2.2250738585072014e-308);
+    int it = 0;
+    int status = (rr == 0.0 || rr < thr) ? 1 : 0;
+    while (status == 0) {
+        // Ap = A p and p . Ap
+        double d = spmvRows(a, a.p, a.Ap);
+        double s = blockReduce(d, AddOp(), 0.0);
+        if (threadIdx.x == 0) a.partC[blockIdx.x] = s;
+        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
+        VT alpha = (VT)(rz / sumPartialsCG(a.partC, nb));
+        double lrr = 0, lrz = 0;
+        CIPC_KERNEL_LOOP(v, nv) {
+            for (int q = 0; q < 3; ++q) {
+                a.x[3 * v + q] += alpha * __ldcg(a.p + 3 * v + q);
+                a.r[3 * v + q] -= alpha * __ldcg(a.Ap + 3 * v + q);
+            }
+            applyDinv(a.Dinv, a.r, a.z, v);
+            for (int q = 0; q < 3; ++q) {
+                lrr += (double)a.r[3 * v + q] * (double)a.r[3 * v + q];
+                lrz += (double)a.r[3 * v + q] * (double)a.z[3 * v + q];
+            }
+        }
+        double s1 = blockReduce(lrr, AddOp(), 0.0);
+        __syncthreads();
+        double s2 = blockReduce(lrz, AddOp(), 0.0);
+        if (threadIdx.x == 0) { a.partA[blockIdx.x] = s1; a.partB[blockIdx.x] = s2; }
+        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
+        rr = sumPartialsCG(a.partA, nb);
+        double rzNew = sumPartialsCG(a.partB, nb);
+        ++it;
+        if (rr < thr) { status = 1; break; }
+        if (it >= a.maxIter) { status = 2; break; }
+        VT beta = (VT)(rzNew / rz);
+        rz = rzNew;
+        CIPC_KERNEL_LOOP(i, 3 * nv) a.p[i] = __ldcg(a.z + i) + beta * __ldcg(a.p + i);
+        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.scal[3] = rr;
+        a.scal[4] = it;
+        a.scal[6] = rhs2;
+        *a.flag = status;
+    }
+}
+
 __global__ void accumulateKernelD(int n3, const double* d, double* x) {
     CIPC_KERNEL_LOOP(i, n3) x[i] += d[i];
 }
@@ -316,10 +490,54 @@ static int runPcg(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT*
     return it;
 }
 
+constexpr int PMAX = 1024;  // max blocks of the persistent PCG
+
+// Whole PCG in one cooperative launch (grid sized to what is co-resident).
+template <class MT, class VT>
+static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT* r, VT* z, VT* p, VT* Ap, double tol, int maxIter,
+                            int& flagOut, double& relRes) {
+    static int smCount = 0, coop = -1;
+    if (coop < 0) {
+        int dev = 0;
+        CIPC_CUDA(cudaGetDevice(&dev));
+        CIPC_CUDA(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev));
+        CIPC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    }
+    if (!coop) return runPcg<MT, VT>(c, val, dval, b, x, r, z, p, Ap, tol, maxIter, flagOut, relRes);
+    int perSM = 0;
+    CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, pcgPersistentKernel<MT, VT>, VB, 0));
+    int needed = std::max(1, (c.nv * GROUP + VB - 1) / VB);
+    int grid = std::max(1, std::min(std::min(perSM * smCount, needed), PMAX));
+    bool dyn = c.nDynB > 0;
+    PcgArgs<MT, VT> a;
+    a.nv = c.nv; a.rowPtr = c.rowPtr; a.col = c.colIdx; a.val = val;
+    a.dRowS = dyn ? c.dynRowStart.p : nullptr; a.dRowE = dyn ? c.dynRowEnd.p : nullptr; a.dCol = dyn ? c.dynCol.p : nullptr; a.dVal = dval;
+    a.diagExtra = c.diagExtra; a.Dinv = c.Dinv; a.b = b; a.x = x; a.r = r; a.z = z; a.p = p; a.Ap = Ap;
+    a.partA = c.red.p; a.partB = c.red.p + PMAX; a.partC = c.red.p + 2 * PMAX;
+    a.scal = c.scal.p; a.flag = c.counters.p + 10;
+    a.barCount = reinterpret_cast<unsigned*>(c.counters.p + 11); a.barGen = reinterpret_cast<unsigned*>(c.counters.p + 12);
+    a.tol = tol; a.maxIter = maxIter;
+    CIPC_CUDA(cudaMemsetAsync(c.counters.p + 10, 0, 3 * sizeof(int), c.s));
+    void* args[] = {&a};
+    profBegin(c, PROF_PCG);
+    ++g_kernelLaunches;
+    CIPC_CUDA(cudaLaunchCooperativeKernel((const void*)pcgPersistentKernel<MT, VT>, dim3(grid), dim3(VB), args, 0, c.s));
+    profEnd(c, PROF_PCG);
+    int hflag = 0;
+    double hs[8];
+    CIPC_CUDA(cudaMemcpyAsync(&hflag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaMemcpyAsync(hs, c.scal.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    if (hflag == 3) throw std::runtime_error("device status in PCG: grid barrier timed out");
+    flagOut = hflag;
+    relRes = hs[6] > 0 ? std::sqrt(hs[3] / hs[6]) : 0.0;
+    return (int)hs[4];
+}
+
 static void reservePcg(Ctx& c) {
     size_t n3 = 3 * (size_t)c.nv;
     c.sol.reserve(n3); c.r.reserve(n3); c.z.reserve(n3); c.p.reserve(n3); c.Ap.reserve(n3);
-    c.red.reserve(4 * MAXPART + 16);
+    c.red.reserve(4 * PMAX + 16);
     c.scal.reserve(16);
     c.counters.reserve(16);
 }
@@ -329,7 +547,7 @@ static int pcgSolve64(Ctx& c) {
     computeDinv(c);
     int flag = 0;
     double rel = 0;
-    int it = runPcg<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol, c.pcgMaxIter, flag, rel);
+    int it = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol, c.pcgMaxIter, flag, rel);
     c.lastPcgIters = it;
     c.lastPcgRelRes = rel;
     c.pcgItersTotal += it;
@@ -367,7 +585,7 @@ static int pcgSolveMixed(Ctx& c) {
         prevRR = rr;
         int flag = 0;
         double rel = 0;
-        int it = runPcg<float, float>(c, c.valF, c.dynBF, bF, c.xF.p, c.rF.p, c.zF.p, c.pF.p, c.ApF.p,
+        int it = runPcgPersistent<float, float>(c, c.valF, c.dynBF, bF, c.xF.p, c.rF.p, c.zF.p, c.pF.p, c.ApF.p,
                                       std::max(innerTol, 0.5 * std::sqrt(thr / rr)), c.pcgMaxIter, flag, rel);
         total += it;
         launch(accumulateKernel, vb, VB, 0, c.s, n3, c.xF.p, c.sol.p);
@@ -379,7 +597,7 @@ static int pcgSolveMixed(Ctx& c) {
         c.corrX.reserve(n3); c.corrR.reserve(n3);
         int flag = 0;
         double rel = 0;
-        int it = runPcg<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, std::sqrt(thr / rr),
+        int it = runPcgPersistent<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, std::sqrt(thr / rr),
                                        c.pcgMaxIter, flag, rel);
         total += it;
         launch(accumulateKernelD, vb, VB, 0, c.s, n3, c.corrX.p, c.sol.p);
