@@ -101,6 +101,8 @@ def lib():
         L.cipc_gpu_profile.argtypes = [vp, C.c_int, C.c_int]
         L.cipc_gpu_profile_read.argtypes = [vp, C.POINTER(C.c_longlong), _dp]
         L.cipc_gpu_kernel_launches.restype = C.c_longlong
+        L.cipc_gpu_pcg_bsr_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                               C.c_void_p, _ip, _dp]
         _lib = L
     return _lib
 
@@ -111,8 +113,9 @@ EXPORTED_SYMBOLS = [
     "cipc_gpu_get_surface", "cipc_gpu_build_collision_sets", "cipc_gpu_get_active_sets", "cipc_gpu_friction_init",
     "cipc_gpu_assemble", "cipc_gpu_export_matrix", "cipc_gpu_solve", "cipc_gpu_energy", "cipc_gpu_step_bounds",
     "cipc_gpu_intersected", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
-    "cipc_gpu_kernel_launches",
+    "cipc_gpu_kernel_launches", "cipc_gpu_pcg_bsr_noalloc",
 ]
+NOALLOC_MAX_ROWS = 32768
 
 PROFILE_KINDS = {"spmv": 1, "tet": 2, "tri": 3, "slot": 4, "barrier": 5, "active": 6, "fullccd": 7, "pcg": 8}
 

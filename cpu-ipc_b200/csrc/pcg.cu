@@ -615,3 +615,102 @@ static int pcgSolveMixed(Ctx& c) {
 int pcgSolve(Ctx& c) { return c.mixed ? pcgSolveMixed(c) : pcgSolve64(c); }
 
 }  // namespace cipc
+
+// ---------------------------------------------------------------------------
+// Allocation-free stand-alone PCG.
+//
+// For callers that must not allocate device memory: code running where
+// cudaMalloc is forbidden or unwanted, e.g. a host whose device memory is
+// owned by its own allocator (a framework's caching allocator, a pre-sized
+// arena) or a loop that must not pay allocation latency.  The caller passes
+// device pointers for the matrix, right-hand side and solution; every scratch
+// vector lives in the file-scope array below.  The array is sized for at
+// most CIPC_NOALLOC_MAX_ROWS block rows (8.2 MB) and every GPU that loads
+// this library keeps it until the process exits.  All calls share it and it
+// keeps the last call's contents, so calls that overlap on the GPU (two
+// streams, two host threads) race; serialise them.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int NOALLOC_MAX_ROWS = 32768;
+constexpr int NOALLOC_PARTS = 3 * 512;
+// r, z, p, Ap (3 per row each), Dinv and a zero diagonal term (9 per row
+// each), partial sums, scalars, then int storage (diagonal slots, flag).
+constexpr size_t NOALLOC_VEC = 3 * (size_t)NOALLOC_MAX_ROWS;
+constexpr size_t NOALLOC_DOUBLES = 4 * NOALLOC_VEC + 18 * (size_t)NOALLOC_MAX_ROWS + NOALLOC_PARTS + 16 + (NOALLOC_MAX_ROWS + 64) / 2;
+}  // namespace
+
+static __device__ __align__(256) double g_noallocScratch[NOALLOC_DOUBLES];
+
+namespace {
+double* g_noallocAddr[256] = {nullptr};  // device address of the scratch, per device id
+
+__global__ void noallocDiagKernel(int nv, const int* rowPtr, const int* colIdx, int* diagSlot, double* zeroDiag) {
+    CIPC_KERNEL_LOOP(r, nv) {
+        int s = -1;
+        for (int k = rowPtr[r]; k < rowPtr[r + 1]; ++k)
+            if (colIdx[k] == r) { s = k; break; }
+        diagSlot[r] = s;
+        for (int q = 0; q < 9; ++q) zeroDiag[9 * r + q] = 0.0;
+    }
+}
+}  // namespace
+
+extern "C" int cipc_gpu_pcg_bsr_noalloc(int nv, const int* rowPtr, const int* colIdx, const double* vals, const double* rhs, double* sol,
+                                        double relativeTolerance, int maximumIterations, void* stream, int* iterations, double* relResidual) {
+    using namespace cipc;
+    if (nv <= 0 || !rowPtr || !colIdx || !vals || !rhs || !sol) return CIPC_ERR_INVALID_ARGUMENT;
+    if (nv > NOALLOC_MAX_ROWS) return CIPC_ERR_INVALID_ARGUMENT;
+    if (!(relativeTolerance > 0) || maximumIterations <= 0) return CIPC_ERR_INVALID_ARGUMENT;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return CIPC_ERR_CUDA;
+    if (!g_noallocAddr[dev]) {
+        // first call on this device: resolve the array's device address with
+        // this device current (the host symbol itself is not a device address)
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noallocScratch) != cudaSuccess || !p) return CIPC_ERR_CUDA;
+        g_noallocAddr[dev] = static_cast<double*>(p);
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* base = g_noallocAddr[dev];
+    double* r = base;
+    double* z = r + NOALLOC_VEC;
+    double* p = z + NOALLOC_VEC;
+    double* Ap = p + NOALLOC_VEC;
+    double* Dinv = Ap + NOALLOC_VEC;
+    double* zeroDiag = Dinv + 9 * (size_t)NOALLOC_MAX_ROWS;
+    double* parts = zeroDiag + 9 * (size_t)NOALLOC_MAX_ROWS;
+    double* scal = parts + NOALLOC_PARTS;
+    int* ints = reinterpret_cast<int*>(scal + 16);
+    int* flag = ints;
+    int* diagSlot = ints + 64;
+    double* partA = parts;
+    double* partB = parts + 512;
+    double* partC = parts + 1024;
+    int vb = vecBlocks(nv);
+    int sb = std::max(1, std::min((nv * GROUP + VB - 1) / VB, MAXPART));
+    launch(noallocDiagKernel, vb, VB, 0, s, nv, rowPtr, colIdx, diagSlot, zeroDiag);
+    launch(dinvKernel<double>, vb, VB, 0, s, nv, diagSlot, vals, (const int*)nullptr, (const int*)nullptr, (const int*)nullptr,
+           (const double*)nullptr, zeroDiag, Dinv);
+    launch(pcgInitKernel<double>, vb, VB, 0, s, nv, rhs, Dinv, sol, r, z, p, partA, partB);
+    launch(pcgInitScalars, 1, VB, 0, s, partA, partB, vb, relativeTolerance, scal, flag);
+    if (cudaGetLastError() != cudaSuccess) return CIPC_ERR_CUDA;
+    int hflag = 0;
+    double hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int guard = 0; guard < maximumIterations / 16 + 2; ++guard) {
+        for (int k = 0; k < 16; ++k) {
+            launch(spmvKernel<double, double>, sb, VB, 0, s, nv, rowPtr, colIdx, vals, (const int*)nullptr, (const int*)nullptr, (const int*)nullptr,
+                   (const double*)nullptr, zeroDiag, p, Ap, partC, flag);
+            launch(pcgUpdateKernel<double>, vb, VB, 0, s, nv, partC, sb, scal, Dinv, p, Ap, sol, r, z, partA, partB, flag);
+            launch(pcgScalarKernel, 1, VB, 0, s, partA, partB, vb, scal, flag, maximumIterations);
+            launch(pcgDirKernel<double>, vb, VB, 0, s, nv, scal, z, p, flag);
+        }
+        if (cudaGetLastError() != cudaSuccess) return CIPC_ERR_CUDA;
+        if (cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CIPC_ERR_CUDA;
+        if (cudaMemcpyAsync(hs, scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CIPC_ERR_CUDA;
+        if (cudaStreamSynchronize(s) != cudaSuccess) return CIPC_ERR_CUDA;
+        if (hflag) break;
+    }
+    if (iterations) *iterations = (int)hs[4];
+    if (relResidual) *relResidual = hs[6] > 0 ? std::sqrt(hs[3] / hs[6]) : 0.0;
+    return hflag == 1 ? CIPC_OK : CIPC_ERR_NOT_CONVERGED;
+}

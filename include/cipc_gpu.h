@@ -173,6 +173,24 @@ long long cipc_gpu_kernel_launches(void);
 int cipc_gpu_pcg_bsr(int nv, const int* rowPtr, const int* colIdx, const double* vals, const double* rhs, double* sol,
                      const cipc_linear_options* options, int* iterations, double* relResidual, char* err, int errlen);
 
+/* Allocation-free variant of cipc_gpu_pcg_bsr (no counterpart in the
+ * reference).  For callers that cannot or must not allocate device memory -
+ * e.g. a host whose device memory belongs to its own allocator, or a loop
+ * that must not pay cudaMalloc latency.  All array arguments are DEVICE
+ * pointers the caller owns (rowPtr nv+1, colIdx and vals as in
+ * cipc_gpu_pcg_bsr, rhs and sol 3*nv); the function allocates nothing and
+ * keeps its scratch vectors in a fixed array inside the library, sized for at
+ * most CIPC_NOALLOC_MAX_ROWS block rows (about 8.2 MB, held on every GPU that
+ * loads the library until the process exits); larger nv returns
+ * CIPC_ERR_INVALID_ARGUMENT.  The first call on a device resolves that array's
+ * device address with the device current, so make the first call on each
+ * device outside any stream capture.  Every call shares the array: calls
+ * that overlap on the GPU (other streams or threads) race and must be
+ * serialised.  stream is a cudaStream_t (NULL = legacy default stream). */
+#define CIPC_NOALLOC_MAX_ROWS 32768
+int cipc_gpu_pcg_bsr_noalloc(int nv, const int* rowPtr, const int* colIdx, const double* vals, const double* rhs, double* sol,
+                             double relativeTolerance, int maximumIterations, void* stream, int* iterations, double* relResidual);
+
 #ifdef __cplusplus
 }
 #endif
