@@ -13,9 +13,16 @@ generated here with the sizes the configuration states.
   e2e      same metric through the C ABI with host buffers: every step
            uploads x, v, V_prev, x_tilde from pinned host memory and reads x
            and v back; wall clock around the calls.
-  roofline achieved HBM bandwidth of the dominant kernel (PCG SpMV):
-           algorithmic bytes per launch / mean launch time, both measured
-           in the timed region.
+  roofline achieved bandwidth of the dominant kernel, the persistent PCG
+           solve: algorithmic bytes per launch (iterations x bytes per
+           iteration) / launch time, both from the timed region (CUDA events
+           on the library's stream around every launch).
+The learned preconditioner is trained online on the Newton systems of the
+first --train-steps steps (Adam on the GPU, not timed), then frozen.  Timing
+starts after --settle-steps untimed steps (40: the cloth has reached the
+cube), so the timed steps are in contact like most of the configuration's
+400 steps.  The same run also times the plain FP64 block-Jacobi GPU path on
+the same frames.
 Multi-GPU: replicas only (one independent simulation per rank, weak scaling).
 
 --impl reference times the reference's CPU path on the host cores.  The
@@ -46,8 +53,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cloth", type=int, default=128)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "learned"])
-    ap.add_argument("--roofline-kernel", default="spmv")
+    ap.add_argument("--precond", default="learned", choices=["jacobi", "learned", "fsai"])
+    ap.add_argument("--settle-steps", type=int, default=40, help="untimed steps before warm-up: the cloth reaches the cube")
+    ap.add_argument("--train-steps", type=int, default=40, help="settle steps whose last Newton system trains the network")
+    ap.add_argument("--train-iters", type=int, default=60)
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 block-Jacobi path")
+    ap.add_argument("--roofline-kernel", default="pcg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -129,6 +140,25 @@ def spmv_bytes(counts, mixed):
     return nnzb * (blk + 4) + (nv + 1) * 4 + ndyn * (blk + 4) + 2 * nv * 4 + nv * (72 + 24 + 24)
 
 
+def pcg_iteration_bytes(counts, mixed, learned):
+    """Algorithmic bytes of one iteration of the persistent PCG kernel: every
+    static and contact block with its column index once (SpMV), row pointers
+    and diagonal extras, the gathered direction, the per-row vector updates
+    (x, r, p, Ap read and written, z written) and the block-Jacobi inverse;
+    with the learned factor also its blocks (both triangles once), the
+    scaling blocks twice and the two extra gathered vectors."""
+    nv, nnzb, ndyn = counts[0], counts[7], counts[8]
+    blk = 36 if mixed else 72
+    vec = 12 if mixed else 24
+    b = (nnzb + ndyn) * (blk + 4) + (nv + 1) * 4 + nv * 72 + nv * vec
+    b += nv * (8 * vec + vec)
+    if learned:
+        b += (nnzb + ndyn) * (36 + 8) + nv * 36 + 2 * nv * 72 + 4 * nv * vec
+    else:
+        b += nv * 72
+    return b
+
+
 def cpu_baseline(scene, seconds, steps_cap=50):
     """The FP64 oracle on the same scene, all host cores, bounded by time."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -177,6 +207,30 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def device_timed(sim, steps, flush, kind, cipc, torch):
+    """Device time of `steps` single steps (CUDA events on the library's
+    stream), L2 flushed before each; profile of one kernel family."""
+    if kind:
+        sim.profile(kind, capacity=200000)
+    launches0 = cipc.kernel_launches()
+    total_ms = 0.0
+    newton = pcg = 0
+    ndyn = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        ms, st = sim.timed_steps(1)
+        total_ms += ms
+        newton += st["newtonIterations"]
+        pcg += st["pcgIterations"]
+        ndyn.append(sim.counts()[8])
+    launches = cipc.kernel_launches() - launches0
+    nprof, prof_ms = sim.profile_read() if kind else (0, 0.0)
+    if kind:
+        sim.profile(0)
+    return dict(ms=total_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -196,12 +250,35 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     scene = cipc.scene_cloth_drape(args.cloth, 10)
+    learned = args.precond == "learned"
     sim = cipc.Simulator(scene, precision=args.precision, precond=args.precond)
+    is_plain = args.precision == "fp64" and args.precond == "jacobi"
+    plain = None if (args.no_plain or is_plain) else cipc.Simulator(scene, precision="fp64", precond="jacobi")
     nv = sim.nv
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
 
+    # ---- settle into the contact phase (not timed); the learned
+    # preconditioner trains online on the Newton systems of these steps
+    # (free fall and first contact), then its weights are frozen ----
+    train = None
+    t0 = time.perf_counter()
+    first = last = None
+    for k in range(args.settle_steps):
+        sim.step()
+        if learned and k < args.train_steps:
+            a, b = sim.precond_train(args.train_iters, probes=4, lr=2e-3, seed=1000 + k)
+            first = a if first is None else first
+            last = b
+        if plain is not None:
+            plain.step()
+    torch.cuda.synchronize()
+    if learned:
+        train = {"steps": min(args.train_steps, args.settle_steps), "adam_iterations_per_step": args.train_iters, "probes": 4, "lr": 2e-3,
+                 "loss_first": first, "loss_last": last, "seconds_with_settle_steps": time.perf_counter() - t0}
     for _ in range(max(3, args.warmup)):
         sim.step()
+        if plain is not None:
+            plain.step()
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -209,24 +286,10 @@ def main():
     # ---- device-timed steps ----
     sampler = ClockSampler(dev)
     sampler.start()
-    sim.profile(args.roofline_kernel, capacity=200000)
-    launches0 = cipc.kernel_launches()
-    total_ms = 0.0
-    newton = pcg = 0
-    ndyn = []
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        ms, st = sim.timed_steps(1)
-        total_ms += ms
-        newton += st["newtonIterations"]
-        pcg += st["pcgIterations"]
-        ndyn.append(sim.counts()[8])
-    launches = cipc.kernel_launches() - launches0
-    nprof, prof_ms = sim.profile_read()
-    sim.profile(0)
+    r = device_timed(sim, args.steps, flush, args.roofline_kernel, cipc, torch)
     clocks = sampler.stop()
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    rp = device_timed(plain, args.steps, flush, None, cipc, torch) if plain is not None else None
+    t = torch.tensor([r["ms"]], dtype=torch.float64, device="cuda")
     if pg:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
     max_ms = float(t.item())
@@ -260,32 +323,45 @@ def main():
 
     if rank == 0:
         counts = sim.counts()
-        counts[8] = int(np.mean(ndyn)) if ndyn else counts[8]
+        counts[8] = int(np.mean(r["ndyn"])) if r["ndyn"] else counts[8]
         peak, peak_kind = measured_peak()
         roof = None
-        if nprof > 0 and args.roofline_kernel == "spmv":
-            avg_ms = prof_ms / nprof
-            bytes_ = spmv_bytes(counts, args.precision == "mixed")
+        if r["nprof"] > 0 and args.roofline_kernel == "pcg":
+            per_it = pcg_iteration_bytes(counts, args.precision == "mixed", learned)
+            bytes_ = per_it * r["pcg"] / r["nprof"]
+            avg_ms = r["prof_ms"] / r["nprof"]
             achieved = bytes_ / (avg_ms / 1000.0) / 1e9
-            roof = {"kernel": "spmvKernel (PCG SpMV)", "bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind,
-                    "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic("spmv"), "algorithmic_bytes_per_launch": bytes_,
-                    "launches": nprof, "mean_launch_us": 1000 * avg_ms}
+            roof = {"kernel": "pcgPersistentKernel (whole PCG solve, one cooperative launch)", "bound": "hbm", "achieved": achieved,
+                    "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic("pcg"),
+                    "algorithmic_bytes_per_launch": bytes_, "bytes_per_iteration": per_it, "launches": r["nprof"],
+                    "mean_launch_us": 1000 * avg_ms, "share_of_step_time": r["prof_ms"] / r["ms"]}
+        cfg = {"workload": f"cloth_drape_{args.cloth}: {args.cloth}x{args.cloth}-vertex 1 m cloth "
+                           f"({2 * (args.cloth - 1) ** 2} tris, BW membrane E=1e4, quadratic bending k_b=1e-3, mu=0.3) "
+                           "0.1 m above a fixed 0.5 m tet cube (10^3 cells x 6 tets), dt=0.005, dhat=1e-3",
+               "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
+               "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
+               "ms_per_newton_iteration": max_ms / max(1, r["newton"]),
+               "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
+               "vertices": nv, "static_blocks": counts[7], "contact_blocks_mean": counts[8]}
+        cfg["timed_frames"] = f"{args.settle_steps + max(3, args.warmup)}-{args.settle_steps + max(3, args.warmup) + args.steps - 1}"
+        if train:
+            cfg["training"] = train
+        if args.precond != "jacobi":
+            cfg["factor_fallbacks"] = sim.precond_stats()["fallbacks"]
+        if rp is not None:
+            plain_v = args.steps / (rp["ms"] / 1000.0)
+            cfg["plain_fp64_gpu"] = {"steps_per_s": plain_v, "ms_per_newton_iteration": rp["ms"] / max(1, rp["newton"]),
+                                     "newton_iterations": rp["newton"], "pcg_iterations": rp["pcg"],
+                                     "speedup_of_this_config": (value / world) / plain_v}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 blocks+SpMV / f64 barrier, CCD, energy" if args.precision == "mixed" else "f64",
             "data": "synthetic",
-            "config": {"workload": f"cloth_drape_{args.cloth}: {args.cloth}x{args.cloth}-vertex 1 m cloth "
-                                   f"({2 * (args.cloth - 1) ** 2} tris, BW membrane E=1e4, quadratic bending k_b=1e-3, mu=0.3) "
-                                   "0.1 m above a fixed 0.5 m tet cube (10^3 cells x 6 tets), dt=0.005, dhat=1e-3",
-                       "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
-                       "newton_iterations": newton, "pcg_iterations": pcg,
-                       "ms_per_newton_iteration": max_ms / max(1, newton),
-                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
-                       "vertices": nv, "static_blocks": counts[7], "contact_blocks_mean": counts[8]},
+            "config": cfg,
             "roofline": roof,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 4 * 24 * nv, "d2h_bytes_per_step": 2 * 24 * nv},
-            "gpu_launches": int(launches),
+            "gpu_launches": int(r["launches"]),
             "clocks": clocks,
         }
         if not args.no_cpu_baseline and world == 1:
@@ -295,6 +371,8 @@ def main():
                 line["cpu_baseline"] = {"error": str(e)}
         print(json.dumps(line), flush=True)
     sim.close()
+    if plain is not None:
+        plain.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

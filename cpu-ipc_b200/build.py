@@ -7,7 +7,8 @@ Every CUDA file is compiled by nvcc with
 compiled with ``--fmad=false`` so that box overlaps, closest-feature
 classification and distance thresholds round exactly like the FP64 oracle.
 The host-only set-up file is compiled by g++.  Outputs land in _build/ and
-the shared library beside this file.
+the shared library beside this file, with the headless runner
+(apps/cipc_headless_gpu.cpp, linked against the library) next to it.
 """
 import argparse
 import concurrent.futures as cf
@@ -19,6 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcipc_gpu.so")
+HEADLESS_SRC = os.path.join(HERE, "apps", "cipc_headless_gpu.cpp")
+HEADLESS = os.path.join(HERE, "cipc_headless_gpu")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I", SRC,
@@ -28,6 +31,8 @@ UNITS = {
     "collision.cu": ["--fmad=false"],
     "contact.cu": [],
     "pcg.cu": [],
+    "mpnn.cu": [],
+    "fsai.cu": [],
     "util.cu": [],
     "solver.cu": [],
 }
@@ -79,6 +84,13 @@ def build(jobs=8, force=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    # the headless runner links only against the C ABI library
+    if force or _stale(HEADLESS, [HEADLESS_SRC, LIB, os.path.join(HERE, "..", "include", "cipc_gpu.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), HEADLESS_SRC, "-o", HEADLESS,
+               "-L", HERE, "-lcipc_gpu", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("headless runner build failed:\n" + r.stdout + r.stderr)
     return LIB
 
 

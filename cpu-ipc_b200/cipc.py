@@ -18,7 +18,7 @@ CIPC_OK = 0
 ERRORS = {1: "invalid argument", 2: "runtime error", 3: "CUDA error", 4: "PCG not converged", 5: "device status"}
 LINEAR_GPU_PCG = 3
 PRECISION = {"fp64": 0, "mixed": 1}
-PRECOND = {"jacobi": 0, "learned": 1}
+PRECOND = {"jacobi": 0, "learned": 1, "fsai": 2}
 MOTION_NONE, MOTION_TWIST_X = 0, 1
 
 _dp = C.POINTER(C.c_double)
@@ -101,6 +101,15 @@ def lib():
         L.cipc_gpu_profile.argtypes = [vp, C.c_int, C.c_int]
         L.cipc_gpu_profile_read.argtypes = [vp, C.POINTER(C.c_longlong), _dp]
         L.cipc_gpu_kernel_launches.restype = C.c_longlong
+        _fp = C.POINTER(C.c_float)
+        L.cipc_gpu_export_bsr.argtypes = [vp, _ip, _ip, _ip, _dp, _ip, _ip, _ip, _dp, _dp]
+        L.cipc_gpu_precond_num_params.restype = C.c_int
+        L.cipc_gpu_precond_set_weights.argtypes = [vp, _fp, C.c_int]
+        L.cipc_gpu_precond_get_weights.argtypes = [vp, _fp, C.c_int]
+        L.cipc_gpu_precond_loss.argtypes = [vp, C.c_int, _fp, C.c_ulonglong, _dp, _fp]
+        L.cipc_gpu_precond_train.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_ulonglong, _dp, _dp]
+        L.cipc_gpu_precond_stats.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.cipc_gpu_precond_factor.argtypes = [vp, C.c_int, _fp, _fp]
         L.cipc_gpu_pcg_bsr_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                                C.c_void_p, _ip, _dp]
         _lib = L
@@ -113,7 +122,9 @@ EXPORTED_SYMBOLS = [
     "cipc_gpu_get_surface", "cipc_gpu_build_collision_sets", "cipc_gpu_get_active_sets", "cipc_gpu_friction_init",
     "cipc_gpu_assemble", "cipc_gpu_export_matrix", "cipc_gpu_solve", "cipc_gpu_energy", "cipc_gpu_step_bounds",
     "cipc_gpu_intersected", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
-    "cipc_gpu_kernel_launches", "cipc_gpu_pcg_bsr_noalloc",
+    "cipc_gpu_kernel_launches", "cipc_gpu_pcg_bsr_noalloc", "cipc_gpu_export_bsr", "cipc_gpu_precond_num_params",
+    "cipc_gpu_precond_set_weights", "cipc_gpu_precond_get_weights", "cipc_gpu_precond_loss", "cipc_gpu_precond_train",
+    "cipc_gpu_precond_stats", "cipc_gpu_precond_factor",
 ]
 NOALLOC_MAX_ROWS = 32768
 
@@ -130,6 +141,10 @@ def _d(a):
 
 def _i(a):
     return a.ctypes.data_as(_ip)
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 class CipcError(RuntimeError):
@@ -320,6 +335,62 @@ class Simulator:
         r = C.c_int(0)
         self._chk(self.L.cipc_gpu_intersected(self.h, C.byref(r)))
         return bool(r.value)
+
+    # ---- system dump and learned preconditioner ----
+    def export_bsr(self):
+        """The last assembled Newton matrix in the device block layout (a dict)."""
+        sz = np.zeros(2, np.int32)
+        self._chk(self.L.cipc_gpu_export_bsr(self.h, _i(sz), None, None, None, None, None, None, None, None))
+        nnzb, ndyn = int(sz[0]), int(sz[1])
+        nv = self.nv
+        rp = np.zeros(nv + 1, np.int32); col = np.zeros(max(nnzb, 1), np.int32); val = np.zeros((max(nnzb, 1), 9))
+        drs = np.zeros(nv, np.int32); dre = np.zeros(nv, np.int32)
+        dcol = np.zeros(max(ndyn, 1), np.int32); dval = np.zeros((max(ndyn, 1), 9)); dx = np.zeros((nv, 9))
+        self._chk(self.L.cipc_gpu_export_bsr(self.h, _i(sz), _i(rp), _i(col), _d(val), _i(drs), _i(dre), _i(dcol), _d(dval), _d(dx)))
+        return dict(nv=nv, rowPtr=rp, col=col[:nnzb], val=val[:nnzb], dRowS=drs, dRowE=dre, dCol=dcol[:ndyn], dVal=dval[:ndyn],
+                    diagExtra=dx)
+
+    def precond_weights(self):
+        n = self.L.cipc_gpu_precond_num_params()
+        w = np.zeros(n, np.float32)
+        self._chk(self.L.cipc_gpu_precond_get_weights(self.h, _f(w), n))
+        return w
+
+    def set_precond_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self._chk(self.L.cipc_gpu_precond_set_weights(self.h, _f(w), len(w)))
+
+    def precond_loss(self, probes=None, nprobes=4, seed=0, grad=False):
+        """(loss, gradient or None) on the last assembled system."""
+        pv = None
+        if probes is not None:
+            pv = np.ascontiguousarray(probes, np.float32).reshape(-1)
+            nprobes = len(pv) // (3 * self.nv)
+        loss = C.c_double(0)
+        g = np.zeros(self.L.cipc_gpu_precond_num_params(), np.float32) if grad else None
+        self._chk(self.L.cipc_gpu_precond_loss(self.h, nprobes, _f(pv) if pv is not None else None, seed, C.byref(loss),
+                                               _f(g) if grad else None))
+        return loss.value, g
+
+    def precond_train(self, iterations, probes=4, lr=1e-3, seed=0):
+        a = C.c_double(0); b = C.c_double(0)
+        self._chk(self.L.cipc_gpu_precond_train(self.h, iterations, probes, lr, seed, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def precond_factor(self, which="fsai"):
+        """The factor G on the last assembled system, slot-aligned with export_bsr:
+        (static blocks (nnzb, 9), contact blocks (ndyn, 9))."""
+        sz = np.zeros(2, np.int32)
+        self._chk(self.L.cipc_gpu_export_bsr(self.h, _i(sz), None, None, None, None, None, None, None, None))
+        gs = np.zeros((max(int(sz[0]), 1), 9), np.float32)
+        gd = np.zeros((max(int(sz[1]), 1), 9), np.float32)
+        self._chk(self.L.cipc_gpu_precond_factor(self.h, PRECOND[which], _f(gs), _f(gd)))
+        return gs[:int(sz[0])], gd[:int(sz[1])]
+
+    def precond_stats(self):
+        o = (C.c_longlong * 3)()
+        self._chk(self.L.cipc_gpu_precond_stats(self.h, o))
+        return dict(fallbacks=o[0], adam_steps=o[1], last_launch_iterations=o[2])
 
 
 def pcg_bsr(row_ptr, col_idx, vals, rhs, precision="fp64", tol=1e-6, max_iter=10000):

@@ -157,9 +157,27 @@ struct Ctx {
     double lastPcgRelRes = 0;
     long long pcgItersTotal = 0;
 
-    // learned preconditioner factor (IC(0) pattern of the lower static+dynamic BSR)
-    DBuf<float> icVal;
-    bool icReady = false;
+    int lastPcgLaunchIters = 0;
+    bool assembled = false;             // a Newton system has been assembled
+
+    // learned preconditioner: network weights (FP32 master, BF16 copy, Adam
+    // state), graph features and activations of the current system, and the
+    // factor G on the IC(0) pattern (slot-aligned with the static and contact
+    // BSR: lower slots G_ij, mirror slots G_ij^T, diagonal slots G_ii)
+    DBuf<float> mpW, mpG, mpM, mpV;
+    DBuf<unsigned short> mpWb;
+    int mpStep = 0;
+    bool mpReady = false, mpMirrorReady = false, mpFactorReady = false;
+    long long mpFallbacks = 0;
+    DBuf<double> mpS;                   // 9 per vertex: inverse Cholesky factor of the diagonal block
+    DBuf<double> mpT;                   // PCG temporary (3 per vertex)
+    DBuf<float> mpNodeF, mpEdgeF, mpEdgeFD;
+    DBuf<int> mpMirS, mpMirD, mpDeg, mpRowS, mpRowE;
+    DBuf<float> mpH, mpAgg, mpES, mpED, mpHeadD;
+    DBuf<float> mpGS, mpGD;
+    DBuf<float> mpVec, mpDGS, mpDGD, mpDH, mpDES, mpDED, mpDAgg, mpDS, mpDSD;
+    DBuf<float> mpBD, mpBX, mpPart;     // backward: per-item gradients, second input block, split-K partials
+    DBuf<unsigned char> mpLowS, mpLowD; // 1 for lower slots of the static / contact pattern
 
     // collision structures
     DevBvh faceTree, edgeTree;

@@ -17,9 +17,13 @@
 #include "cipc_device.cuh"
 #include "cipc_gpu.h"
 #include "cipc_internal.h"
+#include "fsai.h"
+#include "mpnn.h"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 
 namespace cipc {
 
@@ -28,6 +32,7 @@ namespace {
 constexpr int VB = 256;          // threads per block for vector kernels
 constexpr int GROUP = 8;         // lanes per block row in SpMV
 constexpr int MAXPART = 512;
+constexpr int PB = 512;          // threads per block of the persistent PCG
 
 inline int vecBlocks(int n) { return std::max(1, std::min((n + VB - 1) / VB, MAXPART)); }
 
@@ -236,11 +241,21 @@ __global__ void accumulateKernel(int n3, const float* d, double* x) {
 }
 
 // ---------------------------------------------------------------------------
-// Persistent PCG: the whole CG loop in one cooperative launch.  Three grid
-// barriers per iteration (after SpMV, after the x/r/z update, after the p
-// update); every block sums the per-block partials in the same order, so all
-// blocks take the same branch and the result is reproducible.  The barrier
-// spin is bounded: on timeout it sets an error flag and the kernel returns.
+// Persistent PCG: the whole CG loop in one cooperative launch.
+//
+// Two grid barriers per iteration with block-Jacobi.  The direction update is
+// folded into the SpMV phase through A p' = A z + beta A p, so each phase only
+// reads vectors that the previous phase finished:
+//   phase 1: p = z + beta p, Ap = A z + beta Ap, partial p.Ap     | barrier
+//   phase 2: x += alpha p, r -= alpha Ap, z = M r, partial r.r, r.z | barrier
+// With the learned factorised approximate inverse M = S^T G^T G S, phase 2
+// splits in three (r and S r | t = G S r | z = S^T G^T t), four barriers per
+// iteration.  A group of GROUP lanes owns one block row in every phase, so a
+// row's x, r, p, Ap are only touched by their owner; z, S r and t are read by
+// neighbours through L2 (__ldcg) after a barrier.  Every block sums the
+// per-block partials in the same order, so all blocks take the same branch and
+// results are reproducible.  The barrier spin is bounded: on timeout it sets
+// an error flag and the kernel returns.
 // ---------------------------------------------------------------------------
 template <class MT, class VT>
 struct PcgArgs {
@@ -251,6 +266,10 @@ struct PcgArgs {
     const MT* dVal;
     const double* diagExtra;
     const double* Dinv;
+    // learned factor (null for block-Jacobi): S 9 per vertex, G slot-aligned
+    const double* S;
+    const float *gS, *gD;
+    VT* t;
     const VT* b;
     VT *x, *r, *z, *p, *Ap;
     double *partA, *partB, *partC;
@@ -287,7 +306,7 @@ __device__ __forceinline__ bool gridBarrier(unsigned* count, unsigned* gen, int*
         } else {
             long long spins = 0;
             while (*vgen == g) {
-                if (++spins > (1ll << 26)) { atomicExch(flag, 3); ok = 0; break; }
+                if (++spins > (1ll << 25)) { atomicExch(flag, 3); ok = 0; break; }
             }
         }
         __threadfence();
@@ -296,113 +315,223 @@ __device__ __forceinline__ bool gridBarrier(unsigned* count, unsigned* gen, int*
     return ok && *(volatile int*)flag != 3;
 }
 
-template <class MT, class VT>
-__device__ __forceinline__ double spmvRows(const PcgArgs<MT, VT>& a, const VT* x, VT* y) {
-    int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    int lane = threadIdx.x & (GROUP - 1);
-    int grp = (threadIdx.x & 31) / GROUP;
-    const int RPW = 32 / GROUP;
-    int nWarps = gridDim.x * blockDim.x / 32;
-    double dotAcc = 0;
-    for (int base = (gid / 32) * RPW; base < a.nv; base += nWarps * RPW) {
-        int row = base + grp;
-        bool active = row < a.nv;
-        VT acc[3] = {VT(0), VT(0), VT(0)};
-        if (active) {
-            // vectors written by other blocks in this launch: L2 loads only
-            for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
-                int c = a.col[k];
-                VT xv[3] = {__ldcg(x + 3 * c), __ldcg(x + 3 * c + 1), __ldcg(x + 3 * c + 2)};
-                blockMulAdd(a.val + (size_t)9 * k, xv, acc);
-            }
-            if (a.dRowS) {
-                for (int k = a.dRowS[row] + lane; k < a.dRowE[row]; k += GROUP) {
-                    int c = a.dCol[k];
-                    VT xv[3] = {__ldcg(x + 3 * c), __ldcg(x + 3 * c + 1), __ldcg(x + 3 * c + 2)};
-                    blockMulAdd(a.dVal + (size_t)9 * k, xv, acc);
-                }
-            }
-        }
-        for (int o = GROUP / 2; o > 0; o >>= 1)
-            for (int q = 0; q < 3; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o, GROUP);
-        if (active && lane == 0) {
-            VT xv[3] = {__ldcg(x + 3 * row), __ldcg(x + 3 * row + 1), __ldcg(x + 3 * row + 2)};
-            const double* D = a.diagExtra + 9 * row;
-            for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)xv[0] + D[3 * q + 1] * (double)xv[1] + D[3 * q + 2] * (double)xv[2]);
-            for (int q = 0; q < 3; ++q) {
-                y[3 * row + q] = acc[q];
-                dotAcc += (double)xv[q] * (double)acc[q];
-            }
-        }
+// Row-group iteration shared by every phase: the same (block, lane group)
+// owns the same rows in all phases.
+struct RowIter {
+    int lane, grp, first, stride;
+    __device__ RowIter() {
+        int gid = blockIdx.x * blockDim.x + threadIdx.x;
+        lane = threadIdx.x & (GROUP - 1);
+        grp = (threadIdx.x & 31) / GROUP;
+        first = (gid / 32) * (32 / GROUP);
+        stride = gridDim.x * blockDim.x / 32 * (32 / GROUP);
     }
-    return dotAcc;
+};
+
+template <class VT>
+__device__ __forceinline__ void groupReduce3(VT acc[3]) {
+    for (int o = GROUP / 2; o > 0; o >>= 1)
+        for (int q = 0; q < 3; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o, GROUP);
 }
 
+// acc += (A u)_row over the row's static and contact blocks (lane-strided)
 template <class MT, class VT>
-__global__ void __launch_bounds__(256) pcgPersistentKernel(PcgArgs<MT, VT> a) {
+__device__ __forceinline__ void rowSpmv(const PcgArgs<MT, VT>& a, int row, int lane, const VT* u, VT acc[3]) {
+    for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
+        int c = a.col[k];
+        VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+        blockMulAdd(a.val + (size_t)9 * k, xv, acc);
+    }
+    if (a.dRowS) {
+        for (int k = a.dRowS[row] + lane; k < a.dRowE[row]; k += GROUP) {
+            int c = a.dCol[k];
+            VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+            blockMulAdd(a.dVal + (size_t)9 * k, xv, acc);
+        }
+    }
+}
+
+// acc += (G u)_row (TR = false: lower slots and the diagonal block) or
+// (G^T u)_row (TR = true: mirror slots and the transposed diagonal block)
+template <bool TR, class MT, class VT>
+__device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int lane, const VT* u, VT acc[3]) {
+    for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
+        int c = a.col[k];
+        if (TR ? c < row : c > row) continue;
+        VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+        const float* B = a.gS + (size_t)9 * k;
+        if (TR && c == row) {
+            for (int q = 0; q < 3; ++q) acc[q] += (VT)B[q] * xv[0] + (VT)B[3 + q] * xv[1] + (VT)B[6 + q] * xv[2];
+        } else {
+            blockMulAdd(B, xv, acc);
+        }
+    }
+    if (a.dRowS) {
+        for (int k = a.dRowS[row] + lane; k < a.dRowE[row]; k += GROUP) {
+            int c = a.dCol[k];
+            if (TR ? c <= row : c >= row) continue;
+            VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+            blockMulAdd(a.gD + (size_t)9 * k, xv, acc);
+        }
+    }
+}
+
+// z = M r for the learned factor, phases after r is final: writes S r into
+// z, t = G (S r), z = S^T G^T t; returns this thread's r.z contribution
+// (valid on lane 0 of each group).  Three barriers; false on barrier timeout.
+template <class MT, class VT>
+__device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double& rz, double* partRR, double rrLocal) {
     const unsigned nb = gridDim.x;
-    const int nv = a.nv;
-    // init: x = 0, r = b, z = M r, p = z
-    double rr = 0, rz = 0;
-    CIPC_KERNEL_LOOP(v, nv) {
-        for (int q = 0; q < 3; ++q) { a.x[3 * v + q] = VT(0); a.r[3 * v + q] = a.b[3 * v + q]; }
-        applyDinv(a.Dinv, a.r, a.z, v);
-        for (int q = 0; q < 3; ++q) {
-            a.p[3 * v + q] = a.z[3 * v + q];
-            rr += (double)a.r[3 * v + q] * (double)a.r[3 * v + q];
-            rz += (double)a.r[3 * v + q] * (double)a.z[3 * v + q];
+    for (int base = it.first; base < a.nv; base += it.stride) {
+        int row = base + it.grp;
+        if (row < a.nv && it.lane == 0) {
+            const double* S = a.S + 9 * row;
+            double r0 = a.r[3 * row], r1 = a.r[3 * row + 1], r2 = a.r[3 * row + 2];
+            a.z[3 * row] = (VT)(S[0] * r0);
+            a.z[3 * row + 1] = (VT)(S[3] * r0 + S[4] * r1);
+            a.z[3 * row + 2] = (VT)(S[6] * r0 + S[7] * r1 + S[8] * r2);
         }
     }
     {
+        double s = blockReduce(rrLocal, AddOp(), 0.0);
+        if (threadIdx.x == 0) partRR[blockIdx.x] = s;
+    }
+    if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return false;
+    for (int base = it.first; base < a.nv; base += it.stride) {
+        int row = base + it.grp;
+        bool active = row < a.nv;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        if (active) rowFactor<false>(a, row, it.lane, (const VT*)a.z, acc);
+        groupReduce3(acc);
+        if (active && it.lane == 0)
+            for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
+    }
+    if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return false;
+    rz = 0;
+    for (int base = it.first; base < a.nv; base += it.stride) {
+        int row = base + it.grp;
+        bool active = row < a.nv;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        if (active) rowFactor<true>(a, row, it.lane, (const VT*)a.t, acc);
+        groupReduce3(acc);
+        if (active && it.lane == 0) {
+            const double* S = a.S + 9 * row;
+            double y0 = acc[0], y1 = acc[1], y2 = acc[2];
+            VT z0 = (VT)(S[0] * y0 + S[3] * y1 + S[6] * y2);
+            VT z1 = (VT)(S[4] * y1 + S[7] * y2);
+            VT z2 = (VT)(S[8] * y2);
+            a.z[3 * row] = z0; a.z[3 * row + 1] = z1; a.z[3 * row + 2] = z2;
+            rz += (double)a.r[3 * row] * (double)z0 + (double)a.r[3 * row + 1] * (double)z1 + (double)a.r[3 * row + 2] * (double)z2;
+        }
+    }
+    return true;
+}
+
+template <class MT, class VT, bool LEARNED>
+__global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
+    const unsigned nb = gridDim.x;
+    const int nv = a.nv;
+    const RowIter it;
+    // init: x = 0, r = b, z = M r, p = 0, Ap = 0 (the first beta is 0)
+    double rr = 0, rz = 0;
+    for (int base = it.first; base < nv; base += it.stride) {
+        int row = base + it.grp;
+        if (row < nv && it.lane == 0) {
+            for (int q = 0; q < 3; ++q) {
+                a.x[3 * row + q] = VT(0); a.p[3 * row + q] = VT(0); a.Ap[3 * row + q] = VT(0);
+                a.r[3 * row + q] = a.b[3 * row + q];
+                rr += (double)a.r[3 * row + q] * (double)a.r[3 * row + q];
+            }
+            if (!LEARNED) {
+                applyDinv(a.Dinv, a.r, a.z, row);
+                for (int q = 0; q < 3; ++q) rz += (double)a.r[3 * row + q] * (double)a.z[3 * row + q];
+            }
+        }
+    }
+    if (LEARNED) {
+        if (!learnedApply(a, it, rz, a.partA, rr)) return;
+    } else {
         double s1 = blockReduce(rr, AddOp(), 0.0);
-        __syncthreads();
+        if (threadIdx.x == 0) a.partA[blockIdx.x] = s1;
+    }
+    {
         double s2 = blockReduce(rz, AddOp(), 0.0);
-        if (threadIdx.x == 0) { a.partA[blockIdx.x] = s1; a.partB[blockIdx.x] = s2; }
+        if (threadIdx.x == 0) a.partB[blockIdx.x] = s2;
     }
     if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
     rr = sumPartialsCG(a.partA, nb);
     rz = sumPartialsCG(a.partB, nb);
     const double rhs2 = rr;
     const double thr = fmax(a.tol * a.tol * rr, 2.2250738585072014e-308);
-    int it = 0;
+    int iter = 0;
     int status = (rr == 0.0 || rr < thr) ? 1 : 0;
+    VT beta = VT(0);
     while (status == 0) {
-        // Ap = A p and p . Ap
-        double d = spmvRows(a, a.p, a.Ap);
-        double s = blockReduce(d, AddOp(), 0.0);
-        if (threadIdx.x == 0) a.partC[blockIdx.x] = s;
-        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
-        VT alpha = (VT)(rz / sumPartialsCG(a.partC, nb));
-        double lrr = 0, lrz = 0;
-        CIPC_KERNEL_LOOP(v, nv) {
-            for (int q = 0; q < 3; ++q) {
-                a.x[3 * v + q] += alpha * __ldcg(a.p + 3 * v + q);
-                a.r[3 * v + q] -= alpha * __ldcg(a.Ap + 3 * v + q);
-            }
-            applyDinv(a.Dinv, a.r, a.z, v);
-            for (int q = 0; q < 3; ++q) {
-                lrr += (double)a.r[3 * v + q] * (double)a.r[3 * v + q];
-                lrz += (double)a.r[3 * v + q] * (double)a.z[3 * v + q];
+        // phase 1: p = z + beta p ; Ap = A z + beta Ap ; p . Ap
+        double d = 0;
+        for (int base = it.first; base < nv; base += it.stride) {
+            int row = base + it.grp;
+            bool active = row < nv;
+            VT acc[3] = {VT(0), VT(0), VT(0)};
+            if (active) rowSpmv(a, row, it.lane, (const VT*)a.z, acc);
+            groupReduce3(acc);
+            if (active && it.lane == 0) {
+                const double* D = a.diagExtra + 9 * row;
+                VT zv[3] = {a.z[3 * row], a.z[3 * row + 1], a.z[3 * row + 2]};
+                for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)zv[0] + D[3 * q + 1] * (double)zv[1] + D[3 * q + 2] * (double)zv[2]);
+                for (int q = 0; q < 3; ++q) {
+                    VT pv = zv[q] + beta * a.p[3 * row + q];
+                    VT apv = acc[q] + beta * a.Ap[3 * row + q];
+                    a.p[3 * row + q] = pv;
+                    a.Ap[3 * row + q] = apv;
+                    d += (double)pv * (double)apv;
+                }
             }
         }
-        double s1 = blockReduce(lrr, AddOp(), 0.0);
-        __syncthreads();
-        double s2 = blockReduce(lrz, AddOp(), 0.0);
-        if (threadIdx.x == 0) { a.partA[blockIdx.x] = s1; a.partB[blockIdx.x] = s2; }
+        {
+            double s = blockReduce(d, AddOp(), 0.0);
+            if (threadIdx.x == 0) a.partC[blockIdx.x] = s;
+        }
+        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
+        VT alpha = (VT)(rz / sumPartialsCG(a.partC, nb));
+        // phase 2: x += alpha p ; r -= alpha Ap ; z = M r
+        double lrr = 0, lrz = 0;
+        for (int base = it.first; base < nv; base += it.stride) {
+            int row = base + it.grp;
+            if (row < nv && it.lane == 0) {
+                for (int q = 0; q < 3; ++q) {
+                    a.x[3 * row + q] += alpha * a.p[3 * row + q];
+                    a.r[3 * row + q] -= alpha * a.Ap[3 * row + q];
+                    lrr += (double)a.r[3 * row + q] * (double)a.r[3 * row + q];
+                }
+                if (!LEARNED) {
+                    applyDinv(a.Dinv, a.r, a.z, row);
+                    for (int q = 0; q < 3; ++q) lrz += (double)a.r[3 * row + q] * (double)a.z[3 * row + q];
+                }
+            }
+        }
+        if (LEARNED) {
+            if (!learnedApply(a, it, lrz, a.partA, lrr)) return;
+        } else {
+            double s1 = blockReduce(lrr, AddOp(), 0.0);
+            if (threadIdx.x == 0) a.partA[blockIdx.x] = s1;
+        }
+        {
+            double s2 = blockReduce(lrz, AddOp(), 0.0);
+            if (threadIdx.x == 0) a.partB[blockIdx.x] = s2;
+        }
         if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
         rr = sumPartialsCG(a.partA, nb);
         double rzNew = sumPartialsCG(a.partB, nb);
-        ++it;
+        ++iter;
         if (rr < thr) { status = 1; break; }
-        if (it >= a.maxIter) { status = 2; break; }
-        VT beta = (VT)(rzNew / rz);
+        if (iter >= a.maxIter) { status = 2; break; }
+        beta = (VT)(rzNew / rz);
         rz = rzNew;
-        CIPC_KERNEL_LOOP(i, 3 * nv) a.p[i] = __ldcg(a.z + i) + beta * __ldcg(a.p + i);
-        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.scal[3] = rr;
-        a.scal[4] = it;
+        a.scal[4] = iter;
         a.scal[6] = rhs2;
         *a.flag = status;
     }
@@ -492,10 +621,34 @@ static int runPcg(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT*
 
 constexpr int PMAX = 1024;  // max blocks of the persistent PCG
 
+// Blocks per SM of the persistent PCG: CIPC_PCG_BLOCKS_PER_SM (1-8) or 2.
+static int pcgBlocksPerSm() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("CIPC_PCG_BLOCKS_PER_SM");
+        int k = e ? std::atoi(e) : 2;
+        v = std::min(8, std::max(1, k));
+    }
+    return v;
+}
+
+template <class MT, class VT, bool LEARNED>
+static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount) {
+    int perSM = 0;
+    CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, pcgPersistentKernel<MT, VT, LEARNED>, PB, 0));
+    if (perSM < 1) throw std::runtime_error("persistent PCG kernel does not fit on an SM");
+    int needed = std::max(1, (c.nv * GROUP + PB - 1) / PB);
+    int grid = std::max(1, std::min(std::min(std::min(perSM, pcgBlocksPerSm()) * smCount, needed), PMAX));
+    void* args[] = {&a};
+    ++g_kernelLaunches;
+    CIPC_CUDA(cudaLaunchCooperativeKernel((const void*)pcgPersistentKernel<MT, VT, LEARNED>, dim3(grid), dim3(PB), args, 0, c.s));
+}
+
 // Whole PCG in one cooperative launch (grid sized to what is co-resident).
+// learned: apply the factor in c.mpS / c.mpGS / c.mpGD instead of block-Jacobi.
 template <class MT, class VT>
 static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT* r, VT* z, VT* p, VT* Ap, double tol, int maxIter,
-                            int& flagOut, double& relRes) {
+                            int& flagOut, double& relRes, bool learned = false) {
     static int smCount = 0, coop = -1;
     if (coop < 0) {
         int dev = 0;
@@ -503,25 +656,28 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
         CIPC_CUDA(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev));
         CIPC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     }
-    if (!coop) return runPcg<MT, VT>(c, val, dval, b, x, r, z, p, Ap, tol, maxIter, flagOut, relRes);
-    int perSM = 0;
-    CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, pcgPersistentKernel<MT, VT>, VB, 0));
-    int needed = std::max(1, (c.nv * GROUP + VB - 1) / VB);
-    int grid = std::max(1, std::min(std::min(perSM * smCount, needed), PMAX));
+    if (!coop) {
+        if (learned) throw std::runtime_error("the learned preconditioner needs cooperative launch support");
+        return runPcg<MT, VT>(c, val, dval, b, x, r, z, p, Ap, tol, maxIter, flagOut, relRes);
+    }
     bool dyn = c.nDynB > 0;
     PcgArgs<MT, VT> a;
     a.nv = c.nv; a.rowPtr = c.rowPtr; a.col = c.colIdx; a.val = val;
     a.dRowS = dyn ? c.dynRowStart.p : nullptr; a.dRowE = dyn ? c.dynRowEnd.p : nullptr; a.dCol = dyn ? c.dynCol.p : nullptr; a.dVal = dval;
     a.diagExtra = c.diagExtra; a.Dinv = c.Dinv; a.b = b; a.x = x; a.r = r; a.z = z; a.p = p; a.Ap = Ap;
+    a.S = nullptr; a.gS = nullptr; a.gD = nullptr; a.t = nullptr;
+    if (learned) {
+        c.mpT.reserve(3 * (size_t)c.nv);
+        a.S = c.mpS.p; a.gS = c.mpGS.p; a.gD = c.mpGD.p; a.t = reinterpret_cast<VT*>(c.mpT.p);
+    }
     a.partA = c.red.p; a.partB = c.red.p + PMAX; a.partC = c.red.p + 2 * PMAX;
     a.scal = c.scal.p; a.flag = c.counters.p + 10;
     a.barCount = reinterpret_cast<unsigned*>(c.counters.p + 11); a.barGen = reinterpret_cast<unsigned*>(c.counters.p + 12);
     a.tol = tol; a.maxIter = maxIter;
     CIPC_CUDA(cudaMemsetAsync(c.counters.p + 10, 0, 3 * sizeof(int), c.s));
-    void* args[] = {&a};
     profBegin(c, PROF_PCG);
-    ++g_kernelLaunches;
-    CIPC_CUDA(cudaLaunchCooperativeKernel((const void*)pcgPersistentKernel<MT, VT>, dim3(grid), dim3(VB), args, 0, c.s));
+    if (learned) launchPersistent<MT, VT, true>(c, a, smCount);
+    else launchPersistent<MT, VT, false>(c, a, smCount);
     profEnd(c, PROF_PCG);
     int hflag = 0;
     double hs[8];
@@ -531,6 +687,7 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
     if (hflag == 3) throw std::runtime_error("device status in PCG: grid barrier timed out");
     flagOut = hflag;
     relRes = hs[6] > 0 ? std::sqrt(hs[3] / hs[6]) : 0.0;
+    c.lastPcgLaunchIters = (int)hs[4];
     return (int)hs[4];
 }
 
@@ -542,12 +699,72 @@ static void reservePcg(Ctx& c) {
     c.counters.reserve(16);
 }
 
+// CIPC_DEBUG_PCG=1 prints every inner solve and fallback to stderr.
+static bool debugPcg() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_DEBUG_PCG"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+
+// Builds the factor for the current system (network forward, or the exact
+// FSAI); false when block-Jacobi is selected.
+static bool prepareLearned(Ctx& c) {
+    if (c.precond == CIPC_PRECOND_FSAI) {
+        mpnnPrepare(c, false);
+        fsaiBuild(c);
+        return true;
+    }
+    if (c.precond != CIPC_PRECOND_LEARNED) return false;
+    if (!c.mpReady) mpnnInitWeights(c, 1);
+    mpnnPrepare(c);
+    mpnnForward(c);
+    return true;
+}
+
+// ||rhs - A sol||^2 in FP64 (FP32 blocks promoted in mixed mode)
+static double trueResidual2(Ctx& c) {
+    int nv = c.nv, n3 = 3 * nv;
+    c.rF.reserve(n3);
+    double* part = c.red.p + 3 * MAXPART;
+    if (c.mixed) spmvT<float, double>(c, c.valF, c.dynBF, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
+    else spmvT<double, double>(c, c.valD, c.dynBD, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
+    int nb = vecBlocks(nv);
+    launch(residualKernel, nb, VB, 0, c.s, n3, c.rhs.p, c.Ap.p, c.r.p, c.rF.p, part);
+    return deviceSum(c, part, nb);
+}
+
+// Iteration cap of one solve with a factor preconditioner before block-Jacobi
+// takes over (CIPC_FACTOR_CAP, default 1000): a factor that does not reach
+// the inner tolerance within it is rejected rather than iterated further.
+static int factorCap() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("CIPC_FACTOR_CAP");
+        v = e ? std::max(10, std::atoi(e)) : 1000;
+    }
+    return v;
+}
+
 static int pcgSolve64(Ctx& c) {
     reservePcg(c);
     computeDinv(c);
+    bool learned = prepareLearned(c);
     int flag = 0;
     double rel = 0;
-    int it = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol, c.pcgMaxIter, flag, rel);
+    int it = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol,
+                                              learned ? std::min(c.pcgMaxIter, factorCap()) : c.pcgMaxIter, flag, rel, learned);
+    if (learned) {
+        // the true FP64 residual judges the factor solve; block-Jacobi is the fallback
+        double rhs2 = deviceDot(c, c.rhs, c.rhs, 3 * c.nv);
+        double thr = std::max(c.pcgTol * c.pcgTol * rhs2, 2.2250738585072014e-308);
+        double tr2 = trueResidual2(c);
+        if (debugPcg()) std::fprintf(stderr, "[pcg] fp64 factor it %d flag %d true rr/b2 %.3e\n", it, flag, tr2 / rhs2);
+        if (flag != 1 || !(tr2 < thr)) {
+            c.mpFallbacks++;
+            it += runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol,
+                                                   std::max(1, c.pcgMaxIter - it), flag, rel, false);
+        }
+    }
     c.lastPcgIters = it;
     c.lastPcgRelRes = rel;
     c.pcgItersTotal += it;
@@ -555,61 +772,90 @@ static int pcgSolve64(Ctx& c) {
     return it;
 }
 
-// FP32 inner PCG + FP64 iterative refinement on the true residual.
-static int pcgSolveMixed(Ctx& c) {
-    reservePcg(c);
-    computeDinv(c);
+// r = b - A sol in FP64 (FP32 blocks promoted), bF = (float) r; returns |r|^2
+static double mixedResidual(Ctx& c, float* bF) {
+    int nv = c.nv, n3 = 3 * nv;
+    double* part = c.red.p + 3 * MAXPART;
+    spmvT<float, double>(c, c.valF, c.dynBF, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
+    int nb = vecBlocks(nv);
+    launch(residualKernel, nb, VB, 0, c.s, n3, c.rhs.p, c.Ap.p, c.r.p, bF, part);
+    return deviceSum(c, part, nb);
+}
+
+// FP32 inner PCG + FP64 iterative refinement on the true residual, starting
+// from the current c.sol.  Returns false when a factor preconditioner was
+// rejected (inner solve over its cap, or the true residual not reached).
+static bool refineMixed(Ctx& c, bool learned, double thr, double rhs2, int& total, double& rr) {
+    int nv = c.nv, n3 = 3 * nv;
+    float* bF = c.DinvF.p;  // FP32 copy of the current residual (right-hand side of the correction)
+    int vb = vecBlocks(nv + 1);
+    const double innerTol = 1e-3;
+    double prevRR = 1e308;
+    rr = mixedResidual(c, bF);
+    for (int outer = 0; outer < 40 && !(rr < thr); ++outer) {
+        if (!(rr < 0.25 * prevRR) && outer > 2) break;  // refinement stagnates: finish in FP64 below
+        prevRR = rr;
+        int budget = c.pcgMaxIter - total;
+        if (budget <= 0) break;
+        int cap = learned ? std::min(budget, factorCap()) : budget;
+        int flag = 0;
+        double rel = 0;
+        int it = runPcgPersistent<float, float>(c, c.valF, c.dynBF, bF, c.xF.p, c.rF.p, c.zF.p, c.pF.p, c.ApF.p,
+                                                std::max(innerTol, 0.5 * std::sqrt(thr / rr)), cap, flag, rel, learned);
+        total += it;
+        launch(accumulateKernel, vb, VB, 0, c.s, n3, c.xF.p, c.sol.p);
+        rr = mixedResidual(c, bF);
+        if (debugPcg()) std::fprintf(stderr, "[pcg] mixed outer %d inner it %d flag %d rel %.3e -> rr/b2 %.3e learned %d\n", outer, it, flag, rel, rr / rhs2,
+                                     (int)learned);
+        if (learned && flag != 1) return false;
+    }
+    if (!(rr < thr) && total < c.pcgMaxIter) {
+        // refinement stalled: finish with an FP64-vector PCG on the residual
+        // (FP32 blocks promoted) and add the correction
+        c.corrX.reserve(n3); c.corrR.reserve(n3);
+        int budget = c.pcgMaxIter - total;
+        int flag = 0;
+        double rel = 0;
+        int it = runPcgPersistent<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, std::sqrt(thr / rr),
+                                                 learned ? std::min(budget, factorCap()) : budget, flag, rel, learned);
+        total += it;
+        launch(accumulateKernelD, vb, VB, 0, c.s, n3, c.corrX.p, c.sol.p);
+        rr = mixedResidual(c, bF);
+        if (debugPcg()) std::fprintf(stderr, "[pcg] mixed FP64-vector run it %d flag %d -> rr/b2 %.3e learned %d\n", it, flag, rr / rhs2, (int)learned);
+    }
+    return !learned || rr < thr;
+}
+
+static int pcgSolveMixed(Ctx& c, bool learned) {
     int nv = c.nv;
     int n3 = 3 * nv;
     c.rF.reserve(n3); c.zF.reserve(n3); c.pF.reserve(n3); c.ApF.reserve(n3); c.xF.reserve(n3); c.DinvF.reserve(n3);
-    float* bF = c.DinvF.p;  // FP32 copy of the current residual (right-hand side of the correction)
-    int vb = vecBlocks(n3 / 3 + 1);
-    double* part = c.red.p + 3 * MAXPART;
-    launch(zeroKernel, vb, VB, 0, c.s, n3, c.sol.p);
+    launch(zeroKernel, vecBlocks(nv + 1), VB, 0, c.s, n3, c.sol.p);
     double rhs2 = deviceDot(c, c.rhs, c.rhs, n3);
     c.lastPcgIters = 0;
     if (rhs2 == 0.0) { c.lastPcgRelRes = 0; return 0; }
     double thr = std::max(c.pcgTol * c.pcgTol * rhs2, 2.2250738585072014e-308);
     int total = 0;
     double rr = rhs2;
-    const double innerTol = 1e-3;
-    double prevRR = 1e308;
-    for (int outer = 0; outer < 40; ++outer) {
-        // true residual r = b - A x in FP64 (x = 0 on the first pass)
-        spmvT<float, double>(c, c.valF, c.dynBF, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
-        int nb = vecBlocks(nv);
-        launch(residualKernel, nb, VB, 0, c.s, n3, c.rhs.p, c.Ap.p, c.r.p, bF, part);
-        rr = deviceSum(c, part, nb);
-        if (rr < thr) break;
-        if (!(rr < 0.25 * prevRR) && outer > 2) break;  // refinement stagnates: finish in FP64 below
-        prevRR = rr;
-        int flag = 0;
-        double rel = 0;
-        int it = runPcgPersistent<float, float>(c, c.valF, c.dynBF, bF, c.xF.p, c.rF.p, c.zF.p, c.pF.p, c.ApF.p,
-                                      std::max(innerTol, 0.5 * std::sqrt(thr / rr)), c.pcgMaxIter, flag, rel);
-        total += it;
-        launch(accumulateKernel, vb, VB, 0, c.s, n3, c.xF.p, c.sol.p);
-        if (total >= c.pcgMaxIter) break;
+    if (!refineMixed(c, learned, thr, rhs2, total, rr)) {
+        // the factor was rejected (cap or true FP64 residual): block-Jacobi
+        // continues the refinement from the current iterate
+        c.mpFallbacks++;
+        if (debugPcg()) std::fprintf(stderr, "[pcg] factor rejected after %d iterations (rr/b2 %.3e): block-Jacobi\n", total, rr / rhs2);
+        refineMixed(c, false, thr, rhs2, total, rr);
     }
-    if (!(rr < thr)) {
-        // refinement stalled: finish with an FP64-vector PCG on the residual
-        // (FP32 blocks promoted) and add the correction
-        c.corrX.reserve(n3); c.corrR.reserve(n3);
-        int flag = 0;
-        double rel = 0;
-        int it = runPcgPersistent<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, std::sqrt(thr / rr),
-                                       c.pcgMaxIter, flag, rel);
-        total += it;
-        launch(accumulateKernelD, vb, VB, 0, c.s, n3, c.corrX.p, c.sol.p);
-        spmvT<float, double>(c, c.valF, c.dynBF, c.sol.p, c.Ap.p, nullptr, nullptr, spmvBlocks(c));
-        launch(residualKernel, vecBlocks(nv), VB, 0, c.s, n3, c.rhs.p, c.Ap.p, c.r.p, bF, part);
-        rr = deviceSum(c, part, vecBlocks(nv));
-        if (flag == 2 && !(rr < thr)) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
-    }
+    if (!(rr < thr)) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
     c.lastPcgIters = total;
     c.lastPcgRelRes = std::sqrt(rr / rhs2);
     c.pcgItersTotal += total;
     return total;
+}
+
+static int pcgSolveMixed(Ctx& c) {
+    reservePcg(c);
+    computeDinv(c);
+    bool learned = prepareLearned(c);
+    return pcgSolveMixed(c, learned);
 }
 
 int pcgSolve(Ctx& c) { return c.mixed ? pcgSolveMixed(c) : pcgSolve64(c); }

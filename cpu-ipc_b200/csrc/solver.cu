@@ -11,6 +11,8 @@
 #include "../../include/cipc_gpu.h"
 #include "cipc_device.cuh"
 #include "cipc_internal.h"
+#include "fsai.h"
+#include "mpnn.h"
 #include "scene_setup.h"
 
 #include <algorithm>
@@ -192,7 +194,12 @@ int assembleAll(Ctx& c) {
     int coll = contactAssemble(c);
     gatherGradient(c);
     checkStatus(c, "assembly");
+    c.assembled = true;
     return coll;
+}
+
+static void requireSystem(const Ctx& c) {
+    if (!c.assembled) throw InvalidArgument("no assembled Newton system: step or assemble first");
 }
 
 void linearSolve(Ctx& c) {
@@ -361,6 +368,9 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
     if (s->nv >= (1 << 21) - 2) throw InvalidArgument("vertex count exceeds the 2^21 limit of the packed contact keys");
     if (!(s->dt > 0) || !(s->relDhat > 0)) throw InvalidArgument("time step and dHat must be positive");
     if (o && o->backend != CIPC_LINEAR_GPU_PCG) throw InvalidArgument("only the GPU PCG backend is implemented by this library");
+    if (o && o->precision != CIPC_PRECISION_FP64 && o->precision != CIPC_PRECISION_MIXED) throw InvalidArgument("unknown precision");
+    if (o && o->preconditioner != CIPC_PRECOND_BLOCK_JACOBI && o->preconditioner != CIPC_PRECOND_LEARNED && o->preconditioner != CIPC_PRECOND_FSAI)
+        throw InvalidArgument("unknown preconditioner");
     for (int i = 0; i < 4 * s->nt; ++i)
         if (s->tets[i] < 0 || s->tets[i] >= s->nv) throw InvalidArgument("tetrahedron references an out-of-range vertex");
     for (int i = 0; i < 3 * s->nf; ++i)
@@ -453,6 +463,9 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
         CIPC_CUDA(cudaGetLastError());
         // rebuildCollisionSets (Simulator.cpp:532-540)
         buildCollisionSets(*c, true);
+        // the learned preconditioner starts from its deterministic initial
+        // weights (the first-order factor); hosts load trained ones
+        if (c->precond == CIPC_PRECOND_LEARNED) mpnnInitWeights(*c, 1);
         sync(*c);
         return c;
     } catch (...) {
@@ -526,19 +539,24 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                               &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
                               &c.fricLambda, &c.fricCoord, &c.fricBasis, &c.fricGLambda, &c.closeGVal, &c.closeSVal, &c.dynGVal, &c.dynHValD,
                               &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.corrX, &c.corrR, &c.sweptPt, &c.scratch,
-                              &c.scal, &c.energyBuf,
+                              &c.scal, &c.energyBuf, &c.mpS, &c.mpT,
                               &c.faceTree.lo, &c.faceTree.hi, &c.faceTree.primLo, &c.faceTree.primHi, &c.faceTree.sceneBox, &c.edgeTree.lo,
                               &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox};
         for (auto* d : ds) d->free();
-        DBuf<float>* fs[] = {&c.valF, &c.elemHF, &c.dynHValF, &c.dynBF, &c.rF, &c.zF, &c.pF, &c.ApF, &c.xF, &c.DinvF, &c.icVal};
+        DBuf<float>* fs[] = {&c.valF, &c.elemHF, &c.dynHValF, &c.dynBF, &c.rF, &c.zF, &c.pF, &c.ApF, &c.xF, &c.DinvF, &c.mpW, &c.mpG, &c.mpM, &c.mpV,
+                             &c.mpNodeF, &c.mpEdgeF, &c.mpEdgeFD, &c.mpH, &c.mpAgg, &c.mpES, &c.mpED, &c.mpHeadD, &c.mpGS, &c.mpGD,
+                             &c.mpVec, &c.mpDGS, &c.mpDGD, &c.mpDH, &c.mpDES, &c.mpDED, &c.mpDAgg, &c.mpDS, &c.mpDSD,
+                             &c.mpBD, &c.mpBX, &c.mpPart};
         for (auto* d : fs) d->free();
         DBuf<int>* is[] = {&c.btype, &c.softIdx, &c.dirIdx, &c.tets, &c.tris, &c.bendV, &c.faces, &c.surfVerts, &c.edges, &c.rowPtr, &c.colIdx,
                            &c.diagSlot, &c.hcPtr, &c.hcIdx, &c.gcPtr, &c.gcIdx, &c.selfActive, &c.selfEE, &c.eeIe, &c.ground, &c.counts, &c.runs,
                            &c.counters, &c.fricSet, &c.fricGround, &c.closeG, &c.closeS, &c.dynGKey, &c.dynGKeyAlt, &c.dynGIdx, &c.dynGIdxAlt,
                            &c.dynGStart, &c.dynGEnd, &c.dynHIdx, &c.dynHIdxAlt, &c.dynRowStart, &c.dynRowEnd, &c.dynCol, &c.dynSrcStart, &c.status,
                            &c.faceTree.left, &c.faceTree.right, &c.faceTree.parent, &c.faceTree.leafPrim, &c.faceTree.flags, &c.faceTree.escape,
-                           &c.edgeTree.left, &c.edgeTree.right, &c.edgeTree.parent, &c.edgeTree.leafPrim, &c.edgeTree.flags, &c.edgeTree.escape};
+                           &c.edgeTree.left, &c.edgeTree.right, &c.edgeTree.parent, &c.edgeTree.leafPrim, &c.edgeTree.flags, &c.edgeTree.escape, &c.mpMirS, &c.mpMirD, &c.mpDeg,
+                           &c.mpRowS, &c.mpRowE};
         for (auto* d : is) d->free();
+        c.mpWb.free(); c.mpLowS.free(); c.mpLowD.free();
         DBuf<uint64_t>* us[] = {&c.ccdPT, &c.ccdEE, &c.kPT, &c.kEE, &c.kMoll, &c.kPPE, &c.kTmp, &c.uniq, &c.dynHKey, &c.dynHKeyAlt,
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();
@@ -657,6 +675,7 @@ int cipc_gpu_assemble(cipc_gpu_context* h, double* grad, int* collisions) {
 
 int cipc_gpu_export_matrix(cipc_gpu_context* h, long long* count, int* rows, int* cols, double* vals) {
     return guarded(h, [&](Ctx& c) {
+        requireSystem(c);
         sync(c);
         long long n = 9LL * (c.nnzb + c.nDynB + c.nv);
         if (count) *count = n;
@@ -701,6 +720,7 @@ int cipc_gpu_export_matrix(cipc_gpu_context* h, long long* count, int* rows, int
 
 int cipc_gpu_solve(cipc_gpu_context* h, double* direction, int* iterations, double* relRes) {
     return guarded(h, [&](Ctx& c) {
+        requireSystem(c);
         linearSolve(c);
         sync(c);
         if (direction) CIPC_CUDA(cudaMemcpy(direction, c.dir.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToHost));
@@ -785,6 +805,112 @@ int cipc_gpu_intersected(cipc_gpu_context* h, int* result) {
     return guarded(h, [&](Ctx& c) {
         rebuildTrees(c);
         *result = isIntersected(c) ? 1 : 0;
+    });
+}
+
+int cipc_gpu_export_bsr(cipc_gpu_context* h, int* sizes, int* rowPtr, int* col, double* val, int* dynRowStart, int* dynRowEnd, int* dynCol,
+                        double* dynVal, double* diagExtra) {
+    return guarded(h, [&](Ctx& c) {
+        requireSystem(c);
+        sync(c);
+        if (sizes) { sizes[0] = c.nnzb; sizes[1] = c.nDynB; }
+        if (!rowPtr) return;
+        int nv = c.nv;
+        CIPC_CUDA(cudaMemcpy(rowPtr, c.rowPtr.p, sizeof(int) * (nv + 1), cudaMemcpyDeviceToHost));
+        CIPC_CUDA(cudaMemcpy(col, c.colIdx.p, sizeof(int) * c.nnzb, cudaMemcpyDeviceToHost));
+        auto blocks = [&](double* out, const DBuf<double>& d, const DBuf<float>& f, size_t n) {
+            if (!n) return;
+            if (c.mixed) {
+                std::vector<float> t(9 * n);
+                CIPC_CUDA(cudaMemcpy(t.data(), f.p, sizeof(float) * t.size(), cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < t.size(); ++i) out[i] = t[i];
+            } else {
+                CIPC_CUDA(cudaMemcpy(out, d.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
+            }
+        };
+        blocks(val, c.valD, c.valF, c.nnzb);
+        if (c.nDynB) {
+            CIPC_CUDA(cudaMemcpy(dynRowStart, c.dynRowStart.p, sizeof(int) * nv, cudaMemcpyDeviceToHost));
+            CIPC_CUDA(cudaMemcpy(dynRowEnd, c.dynRowEnd.p, sizeof(int) * nv, cudaMemcpyDeviceToHost));
+            CIPC_CUDA(cudaMemcpy(dynCol, c.dynCol.p, sizeof(int) * c.nDynB, cudaMemcpyDeviceToHost));
+            blocks(dynVal, c.dynBD, c.dynBF, c.nDynB);
+        } else {
+            for (int i = 0; i < nv; ++i) dynRowStart[i] = dynRowEnd[i] = 0;
+        }
+        CIPC_CUDA(cudaMemcpy(diagExtra, c.diagExtra.p, sizeof(double) * 9 * nv, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cipc_gpu_precond_num_params(void) { return MP_NPARAM; }
+
+int cipc_gpu_precond_set_weights(cipc_gpu_context* h, const float* weights, int n) {
+    return guarded(h, [&](Ctx& c) {
+        if (!weights) throw InvalidArgument("weights pointer is null");
+        mpnnSetWeights(c, weights, n);
+    });
+}
+
+int cipc_gpu_precond_get_weights(cipc_gpu_context* h, float* weights, int n) {
+    return guarded(h, [&](Ctx& c) {
+        if (!weights || n != MP_NPARAM) throw InvalidArgument("expected a buffer of " + std::to_string(MP_NPARAM) + " parameters");
+        if (!c.mpReady) mpnnInitWeights(c, 1);
+        mpnnGetWeights(c, weights);
+    });
+}
+
+int cipc_gpu_precond_loss(cipc_gpu_context* h, int probes, const float* probeVectors, unsigned long long seed, double* loss, float* grad) {
+    return guarded(h, [&](Ctx& c) {
+        requireSystem(c);
+        if (!c.mpReady) mpnnInitWeights(c, 1);
+        mpnnPrepare(c);
+        mpnnForward(c);
+        double l = mpnnLoss(c, probes, probeVectors, seed, grad != nullptr);
+        if (loss) *loss = l;
+        if (grad) mpnnGetGrad(c, grad);
+    });
+}
+
+int cipc_gpu_precond_train(cipc_gpu_context* h, int iterations, int probes, double learningRate, unsigned long long seed, double* lossFirst,
+                           double* lossLast) {
+    return guarded(h, [&](Ctx& c) {
+        if (iterations < 1 || probes < 1 || !(learningRate > 0)) throw InvalidArgument("training needs iterations, probes and a positive rate");
+        requireSystem(c);
+        if (!c.mpReady) mpnnInitWeights(c, 1);
+        mpnnPrepare(c);
+        for (int it = 0; it < iterations; ++it) {
+            mpnnForward(c);
+            double l = mpnnLoss(c, probes, nullptr, seed + 104729ull * (unsigned long long)(c.mpStep + 1), true);
+            if (it == 0 && lossFirst) *lossFirst = l;
+            if (lossLast) *lossLast = l;
+            mpnnAdam(c, learningRate);
+        }
+        sync(c);
+    });
+}
+
+int cipc_gpu_precond_factor(cipc_gpu_context* h, int which, float* gStatic, float* gContact) {
+    return guarded(h, [&](Ctx& c) {
+        requireSystem(c);
+        if (which != CIPC_PRECOND_LEARNED && which != CIPC_PRECOND_FSAI) throw InvalidArgument("which must be a factor preconditioner");
+        if (which == CIPC_PRECOND_FSAI) {
+            mpnnPrepare(c, false);
+            fsaiBuild(c);
+        } else {
+            if (!c.mpReady) mpnnInitWeights(c, 1);
+            mpnnPrepare(c);
+            mpnnForward(c);
+        }
+        sync(c);
+        if (gStatic) CIPC_CUDA(cudaMemcpy(gStatic, c.mpGS.p, sizeof(float) * 9 * (size_t)c.nnzb, cudaMemcpyDeviceToHost));
+        if (gContact && c.nDynB) CIPC_CUDA(cudaMemcpy(gContact, c.mpGD.p, sizeof(float) * 9 * (size_t)c.nDynB, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cipc_gpu_precond_stats(cipc_gpu_context* h, long long* out) {
+    return guarded(h, [&](Ctx& c) {
+        out[0] = c.mpFallbacks;
+        out[1] = c.mpStep;
+        out[2] = c.lastPcgLaunchIters;
     });
 }
 

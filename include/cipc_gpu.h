@@ -37,7 +37,7 @@ enum {
     CIPC_LINEAR_GPU_PCG = 3
 };
 enum { CIPC_PRECISION_FP64 = 0, CIPC_PRECISION_MIXED = 1 };
-enum { CIPC_PRECOND_BLOCK_JACOBI = 0, CIPC_PRECOND_LEARNED = 1 };
+enum { CIPC_PRECOND_BLOCK_JACOBI = 0, CIPC_PRECOND_LEARNED = 1, CIPC_PRECOND_FSAI = 2 };
 /* Prescribed motions of boundary vertices (twistingBoundaryDirection,
  * Simulator.cpp:24-46, with the angular rate as a parameter). */
 enum { CIPC_MOTION_NONE = 0, CIPC_MOTION_TWIST_X = 1 };
@@ -157,15 +157,58 @@ int cipc_gpu_intersected(cipc_gpu_context* ctx, int* result);
 int cipc_gpu_timed_steps(cipc_gpu_context* ctx, int nsteps, cipc_step_stats* last, double* deviceMs);
 /* Kernel timing for measurement: kind selects one kernel family
  * (1 PCG SpMV, 2 tetrahedra, 3 cloth triangles, 4 BSR slot reduction,
- * 5 self-contact barrier, 6 active-set traversal, 7 full CCD); its launches
- * are bracketed by CUDA events on the context's stream (up to `capacity`
- * launches).  kind 0 disables.  _read returns the number of timed launches
- * and their summed device time. */
+ * 5 self-contact barrier, 6 active-set traversal, 7 full CCD, 8 persistent
+ * PCG solve); its launches are bracketed by CUDA events on the context's
+ * stream (up to `capacity` launches).  kind 0 disables.  _read returns the
+ * number of timed launches and their summed device time. */
 int cipc_gpu_profile(cipc_gpu_context* ctx, int kind, int capacity);
 int cipc_gpu_profile_read(cipc_gpu_context* ctx, long long* launches, double* totalMs);
 /* Kernel launches this library has issued since it was loaded (library
  * sorts/scans excluded). */
 long long cipc_gpu_kernel_launches(void);
+
+/* System dump at the NewtonLinearSystem::solve seam (NewtonLinearSystem.cpp:39,
+ * after assembly): the last assembled Newton matrix in the device layout.
+ * sizes[0] = static blocks, sizes[1] = contact blocks; call with rowPtr NULL
+ * to get the sizes.  rowPtr nv+1, col and val (9 per block, row-major) for
+ * the full symmetric static pattern; dynRowStart/dynRowEnd nv, dynCol and
+ * dynVal for the contact pattern; diagExtra 9 per vertex (inertia, ground
+ * and soft-target terms on the diagonal).  A = static + contact + diagExtra. */
+int cipc_gpu_export_bsr(cipc_gpu_context* ctx, int* sizes, int* rowPtr, int* col, double* val, int* dynRowStart, int* dynRowEnd, int* dynCol,
+                        double* dynVal, double* diagExtra);
+
+/* Learned preconditioner (no counterpart in the reference; the closest is
+ * the Eigen IncompleteCholesky option, NewtonLinearSystem.cpp:186-192).  A
+ * 3-layer width-32 message-passing network over the matrix block graph
+ * emits a lower-triangular factor G on the IC(0) pattern of the
+ * block-Jacobi-scaled matrix; PCG applies M^-1 = S^T G^T G S.  Selected by
+ * CIPC_PRECOND_LEARNED; block-Jacobi takes over when the true FP64 residual
+ * rejects a learned solve.  CIPC_PRECOND_FSAI applies the exact
+ * factorised sparse approximate inverse of the same pattern instead (the
+ * optimum of the network's loss).  Weights are FP32 arrays of
+ * cipc_gpu_precond_num_params() values. */
+int cipc_gpu_precond_num_params(void);
+int cipc_gpu_precond_set_weights(cipc_gpu_context* ctx, const float* weights, int n);
+int cipc_gpu_precond_get_weights(cipc_gpu_context* ctx, float* weights, int n);
+/* Loss (log Kaporin number of G Â G^T, trace by probes) on the last
+ * assembled system and, when grad is not NULL, its gradient with respect to
+ * the weights.  probeVectors: probes x 3*nv host floats, or NULL for the
+ * device generator seeded by seed. */
+int cipc_gpu_precond_loss(cipc_gpu_context* ctx, int probes, const float* probeVectors, unsigned long long seed, double* loss, float* grad);
+/* `iterations` Adam steps (rate learningRate) on the last assembled system,
+ * `probes` probe vectors per step; losses of the first and last step. */
+int cipc_gpu_precond_train(cipc_gpu_context* ctx, int iterations, int probes, double learningRate, unsigned long long seed, double* lossFirst,
+                           double* lossLast);
+/* Builds the factor of preconditioner `which` (CIPC_PRECOND_LEARNED: the
+ * network forward; CIPC_PRECOND_FSAI: the exact factorised sparse
+ * approximate inverse of the same pattern) on the last assembled system and
+ * copies it out slot-aligned with cipc_gpu_export_bsr: 9 floats per static
+ * block (lower slots G_ij, upper slots G_ji^T, diagonal slots G_ii) and per
+ * contact block.  Either pointer may be NULL. */
+int cipc_gpu_precond_factor(cipc_gpu_context* ctx, int which, float* gStatic, float* gContact);
+/* out[0] block-Jacobi fallbacks taken, out[1] Adam steps since the weights
+ * were set, out[2] iterations of the last PCG launch. */
+int cipc_gpu_precond_stats(cipc_gpu_context* ctx, long long* out3);
 
 /* Stand-alone GPU PCG on a caller-given matrix (full symmetric 3x3-block CSR,
  * FP64 values, 9 per block row-major) - the backend switch of
