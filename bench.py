@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 block-Jacobi path")
     ap.add_argument("--roofline-kernel", default="pcg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-timed", action="store_true",
+                    help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
 
@@ -207,6 +209,21 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(value, pg, device):
+    """The slowest rank's time (all ranks take part; pg None means one rank)."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(steps_per_rank, world, max_ms):
+    """Steps per second of the whole job: every rank ran `steps_per_rank`
+    independent replica steps; the job took as long as its slowest rank."""
+    return world * steps_per_rank / (max_ms / 1000.0)
+
+
 def device_timed(sim, steps, flush, kind, cipc, torch):
     """Device time of `steps` single steps (CUDA events on the library's
     stream), L2 flushed before each; profile of one kernel family."""
@@ -286,14 +303,15 @@ def main():
     # ---- device-timed steps ----
     sampler = ClockSampler(dev)
     sampler.start()
+    if args.profile_timed:
+        torch.cuda.cudart().cudaProfilerStart()
     r = device_timed(sim, args.steps, flush, args.roofline_kernel, cipc, torch)
+    if args.profile_timed:
+        torch.cuda.cudart().cudaProfilerStop()
     clocks = sampler.stop()
     rp = device_timed(plain, args.steps, flush, None, cipc, torch) if plain is not None else None
-    t = torch.tensor([r["ms"]], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms / 1000.0)
+    max_ms = max_over_ranks(r["ms"], pg, "cuda")
+    value = whole_job_rate(args.steps, world, max_ms)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     pins = {k: torch.empty((nv, 3), dtype=torch.float64, pin_memory=True).numpy() for k in ("x", "vel", "vprev", "xtilde")}
@@ -316,10 +334,7 @@ def main():
         pins["vprev"][:] = pins["x"]
         pins["xtilde"][:] = pins["x"] + pins["vel"] * dt + gdt2
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(te, op=pg.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / float(te.item())
+    e2e_value = whole_job_rate(e2e_steps, world, 1000.0 * max_over_ranks(e2e_s, pg, "cuda"))
 
     if rank == 0:
         counts = sim.counts()

@@ -158,6 +158,7 @@ struct Ctx {
     long long pcgItersTotal = 0;
 
     int lastPcgLaunchIters = 0;
+    DBuf<unsigned> pcgBar;              // grid-barrier counters of the persistent PCG
     bool assembled = false;             // a Newton system has been assembled
 
     // learned preconditioner: network weights (FP32 master, BF16 copy, Adam

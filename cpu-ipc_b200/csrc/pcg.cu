@@ -275,35 +275,82 @@ struct PcgArgs {
     double *partA, *partB, *partC;
     double* scal;  // out: [3] rr, [4] iterations, [6] rhs2
     int* flag;     // out: 1 converged, 2 iteration cap, 3 barrier timeout
-    unsigned *barCount, *barGen;
+    unsigned* bar;  // BAR_WORDS words: grid-barrier counters and generation
     double tol;
     int maxIter;
 };
 
-// sumPartials for partials written by other blocks of the same launch.
-__device__ __forceinline__ double sumPartialsCG(const double* p, int n) {
-    __shared__ double sh;
-    double v = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v += __ldcg(p + i);
-    v = blockReduce(v, AddOp(), 0.0);
-    if (threadIdx.x == 0) sh = v;
+// Two block sums with one pair of __syncthreads; the result is valid in
+// every thread.  Partial sums follow a fixed order (reproducible).
+__device__ __forceinline__ void blockReduce2(double& a, double& b) {
+    __shared__ double s0[32], s1[32], r2[2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    __syncthreads();  // earlier readers of s0/s1/r2 are done
+    if (lane == 0) { s0[w] = a; s1[w] = b; }
     __syncthreads();
-    return sh;
+    if (w == 0) {
+        double x = lane < nw ? s0[lane] : 0.0, y = lane < nw ? s1[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_xor_sync(0xffffffffu, x, o);
+            y += __shfl_xor_sync(0xffffffffu, y, o);
+        }
+        if (lane == 0) { r2[0] = x; r2[1] = y; }
+    }
+    __syncthreads();
+    a = r2[0];
+    b = r2[1];
 }
 
-__device__ __forceinline__ bool gridBarrier(unsigned* count, unsigned* gen, int* flag, unsigned nblocks) {
+// Sums of per-block partials written by other blocks of the same launch
+// (L2 loads), every block in the same order.
+__device__ __forceinline__ void sumPartials2CG(const double* pa, const double* pb, int n, double& a, double& b) {
+    a = 0; b = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) { a += __ldcg(pa + i); b += __ldcg(pb + i); }
+    blockReduce2(a, b);
+}
+__device__ __forceinline__ double sumPartialsCG(const double* p, int n) {
+    double a = 0, b = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a += __ldcg(p + i);
+    blockReduce2(a, b);
+    return a;
+}
+
+// Grid barrier with a two-level arrival: blocks arrive on one of BAR_SUB
+// sub-counters (each on its own 128-byte line), the last arrival of a
+// sub-counter arrives on the top counter, the last top arrival releases the
+// generation word.  A single counter serialises one atomic per block on one
+// L2 address; this keeps each address to about nblocks / BAR_SUB arrivals.
+// The spin is bounded: on timeout it sets flag = 3 and the kernel returns.
+constexpr int BAR_SUB = 16;
+constexpr int BAR_STRIDE = 32;                     // unsigned words per 128-byte line
+constexpr int BAR_WORDS = BAR_STRIDE * (BAR_SUB + 2);  // sub-counters, top counter, generation
+__device__ __forceinline__ bool gridBarrier(unsigned* bar, int* flag, unsigned nblocks) {
     __syncthreads();
     __shared__ int ok;
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = gen;
+        volatile unsigned* vgen = bar + BAR_STRIDE * (BAR_SUB + 1);
+        unsigned* top = bar + BAR_STRIDE * BAR_SUB;
         unsigned g = *vgen;
         __threadfence();
         ok = 1;
-        if (atomicAdd(count, 1u) == nblocks - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
+        const unsigned sub = blockIdx.x % BAR_SUB;
+        const unsigned subSize = (nblocks - sub + BAR_SUB - 1) / BAR_SUB;
+        const unsigned nsub = nblocks < (unsigned)BAR_SUB ? nblocks : (unsigned)BAR_SUB;
+        bool released = false;
+        if (atomicAdd(bar + BAR_STRIDE * sub, 1u) == subSize - 1) {
+            atomicExch(bar + BAR_STRIDE * sub, 0u);
+            if (atomicAdd(top, 1u) == nsub - 1) {
+                atomicExch(top, 0u);
+                __threadfence();
+                atomicAdd((unsigned*)vgen, 1u);
+                released = true;
+            }
+        }
+        if (!released) {
             long long spins = 0;
             while (*vgen == g) {
                 if (++spins > (1ll << 25)) { atomicExch(flag, 3); ok = 0; break; }
@@ -393,10 +440,11 @@ __device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double
         }
     }
     {
-        double s = blockReduce(rrLocal, AddOp(), 0.0);
-        if (threadIdx.x == 0) partRR[blockIdx.x] = s;
+        double dummy = 0;
+        blockReduce2(rrLocal, dummy);
+        if (threadIdx.x == 0) partRR[blockIdx.x] = rrLocal;
     }
-    if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return false;
+    if (!gridBarrier(a.bar, a.flag, nb)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
         bool active = row < a.nv;
@@ -406,7 +454,7 @@ __device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double
         if (active && it.lane == 0)
             for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
     }
-    if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return false;
+    if (!gridBarrier(a.bar, a.flag, nb)) return false;
     rz = 0;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
@@ -450,17 +498,15 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
     }
     if (LEARNED) {
         if (!learnedApply(a, it, rz, a.partA, rr)) return;
+        double dummy = 0;
+        blockReduce2(rz, dummy);
+        if (threadIdx.x == 0) a.partB[blockIdx.x] = rz;
     } else {
-        double s1 = blockReduce(rr, AddOp(), 0.0);
-        if (threadIdx.x == 0) a.partA[blockIdx.x] = s1;
+        blockReduce2(rr, rz);
+        if (threadIdx.x == 0) { a.partA[blockIdx.x] = rr; a.partB[blockIdx.x] = rz; }
     }
-    {
-        double s2 = blockReduce(rz, AddOp(), 0.0);
-        if (threadIdx.x == 0) a.partB[blockIdx.x] = s2;
-    }
-    if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
-    rr = sumPartialsCG(a.partA, nb);
-    rz = sumPartialsCG(a.partB, nb);
+    if (!gridBarrier(a.bar, a.flag, nb)) return;
+    sumPartials2CG(a.partA, a.partB, nb, rr, rz);
     const double rhs2 = rr;
     const double thr = fmax(a.tol * a.tol * rr, 2.2250738585072014e-308);
     int iter = 0;
@@ -489,10 +535,11 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
             }
         }
         {
-            double s = blockReduce(d, AddOp(), 0.0);
-            if (threadIdx.x == 0) a.partC[blockIdx.x] = s;
+            double dummy = 0;
+            blockReduce2(d, dummy);
+            if (threadIdx.x == 0) a.partC[blockIdx.x] = d;
         }
-        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
+        if (!gridBarrier(a.bar, a.flag, nb)) return;
         VT alpha = (VT)(rz / sumPartialsCG(a.partC, nb));
         // phase 2: x += alpha p ; r -= alpha Ap ; z = M r
         double lrr = 0, lrz = 0;
@@ -512,17 +559,16 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
         }
         if (LEARNED) {
             if (!learnedApply(a, it, lrz, a.partA, lrr)) return;
+            double dummy = 0;
+            blockReduce2(lrz, dummy);
+            if (threadIdx.x == 0) a.partB[blockIdx.x] = lrz;
         } else {
-            double s1 = blockReduce(lrr, AddOp(), 0.0);
-            if (threadIdx.x == 0) a.partA[blockIdx.x] = s1;
+            blockReduce2(lrr, lrz);
+            if (threadIdx.x == 0) { a.partA[blockIdx.x] = lrr; a.partB[blockIdx.x] = lrz; }
         }
-        {
-            double s2 = blockReduce(lrz, AddOp(), 0.0);
-            if (threadIdx.x == 0) a.partB[blockIdx.x] = s2;
-        }
-        if (!gridBarrier(a.barCount, a.barGen, a.flag, nb)) return;
-        rr = sumPartialsCG(a.partA, nb);
-        double rzNew = sumPartialsCG(a.partB, nb);
+        if (!gridBarrier(a.bar, a.flag, nb)) return;
+        double rzNew;
+        sumPartials2CG(a.partA, a.partB, nb, rr, rzNew);
         ++iter;
         if (rr < thr) { status = 1; break; }
         if (iter >= a.maxIter) { status = 2; break; }
@@ -672,9 +718,11 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
     }
     a.partA = c.red.p; a.partB = c.red.p + PMAX; a.partC = c.red.p + 2 * PMAX;
     a.scal = c.scal.p; a.flag = c.counters.p + 10;
-    a.barCount = reinterpret_cast<unsigned*>(c.counters.p + 11); a.barGen = reinterpret_cast<unsigned*>(c.counters.p + 12);
+    c.pcgBar.reserve(BAR_WORDS);
+    a.bar = c.pcgBar.p;
     a.tol = tol; a.maxIter = maxIter;
-    CIPC_CUDA(cudaMemsetAsync(c.counters.p + 10, 0, 3 * sizeof(int), c.s));
+    CIPC_CUDA(cudaMemsetAsync(c.counters.p + 10, 0, sizeof(int), c.s));
+    CIPC_CUDA(cudaMemsetAsync(c.pcgBar.p, 0, BAR_WORDS * sizeof(unsigned), c.s));
     profBegin(c, PROF_PCG);
     if (learned) launchPersistent<MT, VT, true>(c, a, smCount);
     else launchPersistent<MT, VT, false>(c, a, smCount);

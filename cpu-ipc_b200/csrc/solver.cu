@@ -556,7 +556,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                            &c.edgeTree.left, &c.edgeTree.right, &c.edgeTree.parent, &c.edgeTree.leafPrim, &c.edgeTree.flags, &c.edgeTree.escape, &c.mpMirS, &c.mpMirD, &c.mpDeg,
                            &c.mpRowS, &c.mpRowE};
         for (auto* d : is) d->free();
-        c.mpWb.free(); c.mpLowS.free(); c.mpLowD.free();
+        c.mpWb.free(); c.mpLowS.free(); c.mpLowD.free(); c.pcgBar.free();
         DBuf<uint64_t>* us[] = {&c.ccdPT, &c.ccdEE, &c.kPT, &c.kEE, &c.kMoll, &c.kPPE, &c.kTmp, &c.uniq, &c.dynHKey, &c.dynHKeyAlt,
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();

@@ -1,0 +1,59 @@
+"""The CUDA path on the reference's own demo scenes, against the answers the
+reference's documentation quotes for them (tests/golden/kat_values.json):
+twisting-mat (1 and 5 steps), twisting-mat-soft (5 steps) and cloth-bunny
+(1 step), FP64, PCG at 1e-10 relative so that the linear solves are as exact
+as the reference's direct solver.
+
+The scenes are read from the reference's Assets directory, located by
+CIPC_REFERENCE_ASSETS (oracle/ref_scenes.py); the tests skip where it is
+absent."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cipc
+import ref_scenes
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref_scenes.assets_available(), reason="reference assets not available")]
+
+KAT = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "kat_values.json")))
+
+
+def _run(scene, steps):
+    sim = cipc.Simulator(scene, precision="fp64", precond="jacobi", tol=1e-10)
+    for _ in range(steps):
+        st = sim.step()
+    return sim.get("x"), st
+
+
+def test_twisting_mat_one_step():
+    x, st = _run(ref_scenes.twisting_mat(False), 1)
+    k = KAT["twisting_mat_1_step"]
+    assert st["newtonIterations"] == k["newton"]
+    assert abs((x ** 2).sum() - k["squared_norm_sum"]) <= 1e-12 * k["squared_norm_sum"]
+
+
+def test_twisting_mat_five_steps():
+    x, st = _run(ref_scenes.twisting_mat(False), 5)
+    k = KAT["twisting_mat_5_steps"]
+    assert st["newtonIterations"] == k["newton_last"]
+    ref = float(k["squared_norm_sum_prefix"])  # quoted to 12 decimals
+    assert abs((x ** 2).sum() - ref) <= 1e-12 * ref
+
+
+def test_twisting_mat_soft_five_steps():
+    x, st = _run(ref_scenes.twisting_mat(True), 5)
+    k = KAT["twisting_mat_soft_5_steps"]
+    assert st["newtonIterations"] == k["newton_last"]
+    assert abs((x ** 2).sum() - k["squared_norm_sum"]) <= 1e-9 * k["squared_norm_sum"]
+
+
+def test_cloth_bunny_one_step():
+    _, st = _run(ref_scenes.cloth_bunny(), 1)
+    k = KAT["cloth_bunny_1_step"]
+    assert st["newtonIterations"] == k["newton"]
+    assert st["energyBacktracks"] == k["energy_backtracks"]
+    assert st["intersectionBacktracks"] == k["intersection_backtracks"]
+    assert abs(st["minConstraintDistance2"] - k["min_distance2"]) <= 1e-9 * k["min_distance2"]
