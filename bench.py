@@ -142,19 +142,20 @@ def spmv_bytes(counts, mixed):
     return nnzb * (blk + 4) + (nv + 1) * 4 + ndyn * (blk + 4) + 2 * nv * 4 + nv * (72 + 24 + 24)
 
 
-def pcg_iteration_bytes(counts, mixed, learned):
-    """Algorithmic bytes of one iteration of the persistent PCG kernel: every
-    static and contact block with its column index once (SpMV), row pointers
-    and diagonal extras, the gathered direction, the per-row vector updates
-    (x, r, p, Ap read and written, z written) and the block-Jacobi inverse;
-    with the learned factor also its blocks (both triangles once), the
-    scaling blocks twice and the two extra gathered vectors."""
+def pcg_iteration_bytes(counts, mixed, factor):
+    """Algorithmic bytes of one iteration of the pipelined PCG kernel: every
+    static and contact block with its column index once (A m), row pointers,
+    the diagonal extras and the block-Jacobi inverse, the gathered m, the
+    per-row recurrence vectors (z, q, s, p, x, r, u, w read and written, m
+    read and the next m written; FP64 vectors); with a factor also its
+    blocks (both triangles once), the scaling blocks twice and the extra
+    gathered vectors of its two passes."""
     nv, nnzb, ndyn = counts[0], counts[7], counts[8]
     blk = 36 if mixed else 72
-    vec = 12 if mixed else 24
+    vec = 24
     b = (nnzb + ndyn) * (blk + 4) + (nv + 1) * 4 + nv * 72 + nv * vec
-    b += nv * (8 * vec + vec)
-    if learned:
+    b += nv * vec * 18
+    if factor:
         b += (nnzb + ndyn) * (36 + 8) + nv * 36 + 2 * nv * 72 + 4 * nv * vec
     else:
         b += nv * 72
@@ -342,11 +343,11 @@ def main():
         peak, peak_kind = measured_peak()
         roof = None
         if r["nprof"] > 0 and args.roofline_kernel == "pcg":
-            per_it = pcg_iteration_bytes(counts, args.precision == "mixed", learned)
+            per_it = pcg_iteration_bytes(counts, args.precision == "mixed", args.precond != "jacobi")
             bytes_ = per_it * r["pcg"] / r["nprof"]
             avg_ms = r["prof_ms"] / r["nprof"]
             achieved = bytes_ / (avg_ms / 1000.0) / 1e9
-            roof = {"kernel": "pcgPersistentKernel (whole PCG solve, one cooperative launch)", "bound": "hbm", "achieved": achieved,
+            roof = {"kernel": "pcgPipelinedKernel (whole PCG solve, one cooperative launch)", "bound": "hbm", "achieved": achieved,
                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic("pcg"),
                     "algorithmic_bytes_per_launch": bytes_, "bytes_per_iteration": per_it, "launches": r["nprof"],
                     "mean_launch_us": 1000 * avg_ms, "share_of_step_time": r["prof_ms"] / r["ms"]}

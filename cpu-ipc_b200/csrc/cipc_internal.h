@@ -159,6 +159,7 @@ struct Ctx {
 
     int lastPcgLaunchIters = 0;
     DBuf<unsigned> pcgBar;              // grid-barrier counters of the persistent PCG
+    DBuf<double> pcgPipe, pcgParts;     // pipelined PCG: six recurrence vectors, two sets of partial sums
     bool assembled = false;             // a Newton system has been assembled
 
     // learned preconditioner: network weights (FP32 master, BF16 copy, Adam

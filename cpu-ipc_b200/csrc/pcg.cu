@@ -33,6 +33,7 @@ constexpr int VB = 256;          // threads per block for vector kernels
 constexpr int GROUP = 8;         // lanes per block row in SpMV
 constexpr int MAXPART = 512;
 constexpr int PB = 512;          // threads per block of the persistent PCG
+constexpr int PIPE_PMAX = 1024;  // partial-sum slots per array of the pipelined PCG (>= its grid)
 
 inline int vecBlocks(int n) { return std::max(1, std::min((n + VB - 1) / VB, MAXPART)); }
 
@@ -272,7 +273,9 @@ struct PcgArgs {
     VT* t;
     const VT* b;
     VT *x, *r, *z, *p, *Ap;
+    VT *u, *w, *mA, *mB, *q, *s;  // pipelined variant only
     double *partA, *partB, *partC;
+    double* pp;                   // pipelined variant: two sets of three partial arrays, PIPE_PMAX each
     double* scal;  // out: [3] rr, [4] iterations, [6] rhs2
     int* flag;     // out: 1 converged, 2 iteration cap, 3 barrier timeout
     unsigned* bar;  // BAR_WORDS words: grid-barrier counters and generation
@@ -305,12 +308,44 @@ __device__ __forceinline__ void blockReduce2(double& a, double& b) {
     b = r2[1];
 }
 
+// Three block sums with one pair of __syncthreads (as blockReduce2).
+__device__ __forceinline__ void blockReduce3(double& a, double& b, double& c) {
+    __shared__ double s0[32], s1[32], s2[32], r3[3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    __syncthreads();
+    if (lane == 0) { s0[w] = a; s1[w] = b; s2[w] = c; }
+    __syncthreads();
+    if (w == 0) {
+        double x = lane < nw ? s0[lane] : 0.0, y = lane < nw ? s1[lane] : 0.0, z = lane < nw ? s2[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_xor_sync(0xffffffffu, x, o);
+            y += __shfl_xor_sync(0xffffffffu, y, o);
+            z += __shfl_xor_sync(0xffffffffu, z, o);
+        }
+        if (lane == 0) { r3[0] = x; r3[1] = y; r3[2] = z; }
+    }
+    __syncthreads();
+    a = r3[0];
+    b = r3[1];
+    c = r3[2];
+}
+
 // Sums of per-block partials written by other blocks of the same launch
 // (L2 loads), every block in the same order.
 __device__ __forceinline__ void sumPartials2CG(const double* pa, const double* pb, int n, double& a, double& b) {
     a = 0; b = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) { a += __ldcg(pa + i); b += __ldcg(pb + i); }
     blockReduce2(a, b);
+}
+__device__ __forceinline__ void sumPartials3CG(const double* pa, const double* pb, const double* pc, int n, double& a, double& b, double& c) {
+    a = 0; b = 0; c = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) { a += __ldcg(pa + i); b += __ldcg(pb + i); c += __ldcg(pc + i); }
+    blockReduce3(a, b, c);
 }
 __device__ __forceinline__ double sumPartialsCG(const double* p, int n) {
     double a = 0, b = 0;
@@ -583,6 +618,189 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined PCG (Ghysels and Vanroose's recurrences): the dot products of an
+// iteration are formed in the same pass as its vector updates, and the
+// preconditioned direction's product n = A m is carried by recurrences, so
+// one iteration is one pass over the rows and ONE grid barrier with
+// block-Jacobi (three with a factor: S w | G (S w) | S^T G^T t).
+//   gamma = (r,u), delta = (w,u);  beta = gamma/gamma_old,
+//   alpha = gamma / (delta - beta gamma / alpha_old)
+//   n = A m;  z = n + beta z;  q = m + beta q;  s = w + beta s;  p = u + beta p
+//   x += alpha p;  r -= alpha s;  u -= alpha q;  w -= alpha z;  m = M w
+// With block-Jacobi the new m is written to the other of two buffers, since
+// neighbours read the current one in the same pass; the partial sums also
+// alternate between two sets, so a set is rewritten only two barriers after
+// its last read.  The recurrences drift from the true residual in finite
+// precision; the callers judge every solve by the true FP64 residual.
+// ---------------------------------------------------------------------------
+template <class MT, class VT>
+__device__ __forceinline__ void rowAx(const PcgArgs<MT, VT>& a, const RowIter& it, int row, const VT* u, VT acc[3]) {
+    if (row < a.nv) rowSpmv(a, row, it.lane, u, acc);
+    groupReduce3(acc);
+    if (row < a.nv && it.lane == 0) {
+        const double* D = a.diagExtra + 9 * row;
+        VT uv[3] = {__ldcg(u + 3 * row), __ldcg(u + 3 * row + 1), __ldcg(u + 3 * row + 2)};
+        for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)uv[0] + D[3 * q + 1] * (double)uv[1] + D[3 * q + 2] * (double)uv[2]);
+    }
+}
+
+// out = M^-1 in for the factor: S in -> tmp (own rows), barrier, t = G tmp,
+// barrier, out = S^T G^T t.  Ends without a barrier; false on timeout.
+template <class MT, class VT>
+__device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const VT* in, VT* tmp, VT* out) {
+    const unsigned nb = gridDim.x;
+    for (int base = it.first; base < a.nv; base += it.stride) {
+        int row = base + it.grp;
+        if (row < a.nv && it.lane == 0) {
+            const double* S = a.S + 9 * row;
+            double r0 = in[3 * row], r1 = in[3 * row + 1], r2 = in[3 * row + 2];
+            tmp[3 * row] = (VT)(S[0] * r0);
+            tmp[3 * row + 1] = (VT)(S[3] * r0 + S[4] * r1);
+            tmp[3 * row + 2] = (VT)(S[6] * r0 + S[7] * r1 + S[8] * r2);
+        }
+    }
+    if (!gridBarrier(a.bar, a.flag, nb)) return false;
+    for (int base = it.first; base < a.nv; base += it.stride) {
+        int row = base + it.grp;
+        bool active = row < a.nv;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        if (active) rowFactor<false>(a, row, it.lane, (const VT*)tmp, acc);
+        groupReduce3(acc);
+        if (active && it.lane == 0)
+            for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
+    }
+    if (!gridBarrier(a.bar, a.flag, nb)) return false;
+    for (int base = it.first; base < a.nv; base += it.stride) {
+        int row = base + it.grp;
+        bool active = row < a.nv;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        if (active) rowFactor<true>(a, row, it.lane, (const VT*)a.t, acc);
+        groupReduce3(acc);
+        if (active && it.lane == 0) {
+            const double* S = a.S + 9 * row;
+            double y0 = acc[0], y1 = acc[1], y2 = acc[2];
+            out[3 * row] = (VT)(S[0] * y0 + S[3] * y1 + S[6] * y2);
+            out[3 * row + 1] = (VT)(S[4] * y1 + S[7] * y2);
+            out[3 * row + 2] = (VT)(S[8] * y2);
+        }
+    }
+    return true;
+}
+
+template <class VT>
+__device__ __forceinline__ void jacobiRow(const double* Dinv, const VT* in, VT* out, int row) {
+    const double* D = Dinv + 9 * row;
+    double r0 = in[3 * row], r1 = in[3 * row + 1], r2 = in[3 * row + 2];
+    out[3 * row] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
+    out[3 * row + 1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
+    out[3 * row + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
+}
+
+template <class MT, class VT, bool LEARNED>
+__global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
+    const unsigned nb = gridDim.x;
+    const int nv = a.nv;
+    const RowIter it;
+    VT* sw = a.Ap;  // S w for the factor passes
+    auto part = [&](int set, int k) { return a.pp + (size_t)(3 * set + k) * PIPE_PMAX; };
+    // x = 0, r = b, u = M r; the recurrence vectors start at 0
+    double rr = 0;
+    for (int base = it.first; base < nv; base += it.stride) {
+        int row = base + it.grp;
+        if (row < nv && it.lane == 0) {
+            for (int q = 0; q < 3; ++q) {
+                int i = 3 * row + q;
+                a.x[i] = VT(0); a.z[i] = VT(0); a.q[i] = VT(0); a.s[i] = VT(0); a.p[i] = VT(0);
+                a.r[i] = a.b[i];
+                rr += (double)a.r[i] * (double)a.r[i];
+            }
+            if (!LEARNED) jacobiRow(a.Dinv, (const VT*)a.r, a.u, row);
+        }
+    }
+    if (LEARNED && !factorPasses(a, it, (const VT*)a.r, sw, a.u)) return;
+    if (!gridBarrier(a.bar, a.flag, nb)) return;
+    // w = A u, m = M w, gamma = (r,u), delta = (w,u)
+    double g = 0, dl = 0;
+    for (int base = it.first; base < nv; base += it.stride) {
+        int row = base + it.grp;
+        VT acc[3] = {VT(0), VT(0), VT(0)};
+        rowAx(a, it, row, (const VT*)a.u, acc);
+        if (row < nv && it.lane == 0) {
+            for (int q = 0; q < 3; ++q) {
+                int i = 3 * row + q;
+                a.w[i] = acc[q];
+                g += (double)a.r[i] * (double)a.u[i];
+                dl += (double)acc[q] * (double)a.u[i];
+            }
+            if (!LEARNED) jacobiRow(a.Dinv, (const VT*)a.w, a.mA, row);
+        }
+    }
+    blockReduce3(rr, g, dl);
+    if (threadIdx.x == 0) { part(0, 0)[blockIdx.x] = rr; part(0, 1)[blockIdx.x] = g; part(0, 2)[blockIdx.x] = dl; }
+    if (LEARNED && !factorPasses(a, it, (const VT*)a.w, sw, a.mA)) return;
+    if (!gridBarrier(a.bar, a.flag, nb)) return;
+    sumPartials3CG(part(0, 0), part(0, 1), part(0, 2), nb, rr, g, dl);
+    const double rhs2 = rr;
+    const double thr = fmax(a.tol * a.tol * rr, 2.2250738585072014e-308);
+    int iter = 0;
+    int status = (rr == 0.0 || rr < thr) ? 1 : 0;
+    double gPrev = 1.0, alphaPrev = 1.0;
+    while (status == 0) {
+        double beta = iter == 0 ? 0.0 : g / gPrev;
+        double den = iter == 0 ? dl : dl - beta * g / alphaPrev;
+        if (!(den != 0.0) || !isfinite(den)) { status = 2; break; }  // breakdown: the caller's true residual decides
+        double alpha = g / den;
+        const VT* mCur = (LEARNED || (iter & 1) == 0) ? a.mA : a.mB;
+        VT* mNext = LEARNED ? a.mA : ((iter & 1) == 0 ? a.mB : a.mA);
+        const VT bt = (VT)beta, al = (VT)alpha;
+        double lrr = 0, lg = 0, ld = 0;
+        for (int base = it.first; base < nv; base += it.stride) {
+            int row = base + it.grp;
+            VT acc[3] = {VT(0), VT(0), VT(0)};
+            rowAx(a, it, row, mCur, acc);
+            if (row < nv && it.lane == 0) {
+                for (int q = 0; q < 3; ++q) {
+                    int i = 3 * row + q;
+                    VT zv = acc[q] + bt * a.z[i];
+                    VT qv = __ldcg(mCur + i) + bt * a.q[i];
+                    VT sv = a.w[i] + bt * a.s[i];
+                    VT pv = a.u[i] + bt * a.p[i];
+                    a.z[i] = zv; a.q[i] = qv; a.s[i] = sv; a.p[i] = pv;
+                    a.x[i] += al * pv;
+                    VT rv = a.r[i] - al * sv;
+                    VT uv = a.u[i] - al * qv;
+                    VT wv = a.w[i] - al * zv;
+                    a.r[i] = rv; a.u[i] = uv; a.w[i] = wv;
+                    lrr += (double)rv * (double)rv;
+                    lg += (double)rv * (double)uv;
+                    ld += (double)wv * (double)uv;
+                }
+                if (!LEARNED) jacobiRow(a.Dinv, (const VT*)a.w, mNext, row);
+            }
+        }
+        const int set = (iter + 1) & 1;
+        blockReduce3(lrr, lg, ld);
+        if (threadIdx.x == 0) { part(set, 0)[blockIdx.x] = lrr; part(set, 1)[blockIdx.x] = lg; part(set, 2)[blockIdx.x] = ld; }
+        // the factor's m is replaced only in its third pass, two barriers
+        // after every row read it
+        if (LEARNED && !factorPasses(a, it, (const VT*)a.w, sw, mNext)) return;
+        if (!gridBarrier(a.bar, a.flag, nb)) return;
+        gPrev = g;
+        alphaPrev = alpha;
+        sumPartials3CG(part(set, 0), part(set, 1), part(set, 2), nb, rr, g, dl);
+        ++iter;
+        if (rr < thr) { status = 1; break; }
+        if (iter >= a.maxIter || !isfinite(rr)) { status = 2; break; }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.scal[3] = rr;
+        a.scal[4] = iter;
+        a.scal[6] = rhs2;
+        *a.flag = status;
+    }
+}
+
 __global__ void accumulateKernelD(int n3, const double* d, double* x) {
     CIPC_KERNEL_LOOP(i, n3) x[i] += d[i];
 }
@@ -678,23 +896,32 @@ static int pcgBlocksPerSm() {
     return v;
 }
 
+// CIPC_PCG_CLASSIC=1 selects the textbook recurrences (two barriers per
+// iteration with block-Jacobi); the default is the pipelined kernel.
+static bool pcgClassic() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_PCG_CLASSIC"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+
 template <class MT, class VT, bool LEARNED>
-static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount) {
+static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool classic) {
+    const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED>;
     int perSM = 0;
-    CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, pcgPersistentKernel<MT, VT, LEARNED>, PB, 0));
+    CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, 0));
     if (perSM < 1) throw std::runtime_error("persistent PCG kernel does not fit on an SM");
     int needed = std::max(1, (c.nv * GROUP + PB - 1) / PB);
-    int grid = std::max(1, std::min(std::min(std::min(perSM, pcgBlocksPerSm()) * smCount, needed), PMAX));
+    int grid = std::max(1, std::min(std::min(std::min(perSM, pcgBlocksPerSm()) * smCount, needed), std::min(PMAX, PIPE_PMAX)));
     void* args[] = {&a};
     ++g_kernelLaunches;
-    CIPC_CUDA(cudaLaunchCooperativeKernel((const void*)pcgPersistentKernel<MT, VT, LEARNED>, dim3(grid), dim3(PB), args, 0, c.s));
+    CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PB), args, 0, c.s));
 }
 
 // Whole PCG in one cooperative launch (grid sized to what is co-resident).
 // learned: apply the factor in c.mpS / c.mpGS / c.mpGD instead of block-Jacobi.
 template <class MT, class VT>
 static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT* r, VT* z, VT* p, VT* Ap, double tol, int maxIter,
-                            int& flagOut, double& relRes, bool learned = false) {
+                            int& flagOut, double& relRes, bool learned = false, bool classic = false) {
     static int smCount = 0, coop = -1;
     if (coop < 0) {
         int dev = 0;
@@ -717,6 +944,13 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
         a.S = c.mpS.p; a.gS = c.mpGS.p; a.gD = c.mpGD.p; a.t = reinterpret_cast<VT*>(c.mpT.p);
     }
     a.partA = c.red.p; a.partB = c.red.p + PMAX; a.partC = c.red.p + 2 * PMAX;
+    // pipelined kernel: six more vectors and two sets of partial sums
+    size_t n3 = 3 * (size_t)c.nv;
+    c.pcgPipe.reserve(6 * n3 * sizeof(VT) / sizeof(double) + 6);
+    VT* pv = reinterpret_cast<VT*>(c.pcgPipe.p);
+    a.u = pv; a.w = pv + n3; a.mA = pv + 2 * n3; a.mB = pv + 3 * n3; a.q = pv + 4 * n3; a.s = pv + 5 * n3;
+    c.pcgParts.reserve(6 * (size_t)PIPE_PMAX);
+    a.pp = c.pcgParts.p;
     a.scal = c.scal.p; a.flag = c.counters.p + 10;
     c.pcgBar.reserve(BAR_WORDS);
     a.bar = c.pcgBar.p;
@@ -724,8 +958,9 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
     CIPC_CUDA(cudaMemsetAsync(c.counters.p + 10, 0, sizeof(int), c.s));
     CIPC_CUDA(cudaMemsetAsync(c.pcgBar.p, 0, BAR_WORDS * sizeof(unsigned), c.s));
     profBegin(c, PROF_PCG);
-    if (learned) launchPersistent<MT, VT, true>(c, a, smCount);
-    else launchPersistent<MT, VT, false>(c, a, smCount);
+    classic = classic || pcgClassic();
+    if (learned) launchPersistent<MT, VT, true>(c, a, smCount, classic);
+    else launchPersistent<MT, VT, false>(c, a, smCount, classic);
     profEnd(c, PROF_PCG);
     int hflag = 0;
     double hs[8];
@@ -797,26 +1032,40 @@ static int pcgSolve64(Ctx& c) {
     reservePcg(c);
     computeDinv(c);
     bool learned = prepareLearned(c);
+    int n3 = 3 * c.nv;
     int flag = 0;
     double rel = 0;
-    int it = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol,
+    // the pipelined recurrences are asked for no more than 1e-8 relative
+    // (their attainable accuracy); tighter tolerances are reached by the
+    // corrections below
+    int it = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p,
+                                              pcgClassic() ? c.pcgTol : std::max(c.pcgTol, 1e-8),
                                               learned ? std::min(c.pcgMaxIter, factorCap()) : c.pcgMaxIter, flag, rel, learned);
-    if (learned) {
-        // the true FP64 residual judges the factor solve; block-Jacobi is the fallback
-        double rhs2 = deviceDot(c, c.rhs, c.rhs, 3 * c.nv);
-        double thr = std::max(c.pcgTol * c.pcgTol * rhs2, 2.2250738585072014e-308);
-        double tr2 = trueResidual2(c);
-        if (debugPcg()) std::fprintf(stderr, "[pcg] fp64 factor it %d flag %d true rr/b2 %.3e\n", it, flag, tr2 / rhs2);
-        if (flag != 1 || !(tr2 < thr)) {
-            c.mpFallbacks++;
-            it += runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p, c.pcgTol,
-                                                   std::max(1, c.pcgMaxIter - it), flag, rel, false);
-        }
+    // the true FP64 residual judges every solve; corrections restart from
+    // the current iterate (residual replacement) with the textbook
+    // recurrences, block-Jacobi taking over from a rejected factor
+    double rhs2 = deviceDot(c, c.rhs, c.rhs, n3);
+    double thr = std::max(c.pcgTol * c.pcgTol * rhs2, 2.2250738585072014e-308);
+    double tr2 = trueResidual2(c);
+    if (debugPcg()) std::fprintf(stderr, "[pcg] fp64 it %d flag %d true rr/b2 %.3e factor %d\n", it, flag, tr2 / rhs2, (int)learned);
+    if (learned && (flag != 1 || !(tr2 < thr))) {
+        c.mpFallbacks++;
+        learned = false;
+    }
+    c.corrX.reserve(n3); c.corrR.reserve(n3);
+    for (int k = 0; k < 8 && !(tr2 < thr) && it < c.pcgMaxIter; ++k) {
+        int f2 = 0;
+        int it2 = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p,
+                                                   0.5 * std::sqrt(thr / tr2), c.pcgMaxIter - it, f2, rel, learned, true);
+        it += it2;
+        launch(accumulateKernelD, vecBlocks(c.nv + 1), VB, 0, c.s, n3, (const double*)c.corrX.p, c.sol.p);
+        tr2 = trueResidual2(c);
+        if (debugPcg()) std::fprintf(stderr, "[pcg] fp64 correction it %d flag %d true rr/b2 %.3e\n", it2, f2, tr2 / rhs2);
     }
     c.lastPcgIters = it;
-    c.lastPcgRelRes = rel;
+    c.lastPcgRelRes = rhs2 > 0 ? std::sqrt(tr2 / rhs2) : 0.0;
     c.pcgItersTotal += it;
-    if (flag == 2) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
+    if (!(tr2 < thr) && rhs2 > 0) throw std::runtime_error("GPU PCG did not converge within " + std::to_string(c.pcgMaxIter) + " iterations");
     return it;
 }
 
@@ -840,7 +1089,12 @@ static bool refineMixed(Ctx& c, bool learned, double thr, double rhs2, int& tota
     const double innerTol = 1e-3;
     double prevRR = 1e308;
     rr = mixedResidual(c, bF);
-    for (int outer = 0; outer < 40 && !(rr < thr); ++outer) {
+    // The pipelined kernel's recurrences stagnate with FP32 vectors on these
+    // systems (measured), so with it the corrections run FP64 vectors over
+    // the FP32 blocks below; the FP32-vector inner loop serves the classic
+    // kernel.
+    const int outerMax = pcgClassic() ? 40 : 0;
+    for (int outer = 0; outer < outerMax && !(rr < thr); ++outer) {
         if (!(rr < 0.25 * prevRR) && outer > 2) break;  // refinement stagnates: finish in FP64 below
         prevRR = rr;
         int budget = c.pcgMaxIter - total;
@@ -857,19 +1111,23 @@ static bool refineMixed(Ctx& c, bool learned, double thr, double rhs2, int& tota
                                      (int)learned);
         if (learned && flag != 1) return false;
     }
-    if (!(rr < thr) && total < c.pcgMaxIter) {
-        // refinement stalled: finish with an FP64-vector PCG on the residual
-        // (FP32 blocks promoted) and add the correction
-        c.corrX.reserve(n3); c.corrR.reserve(n3);
+    // FP64-vector PCG on the true residual (FP32 blocks promoted), repeated
+    // as residual replacement until the true FP64 residual passes; the
+    // repeats use the textbook recurrences, free of pipelining drift
+    c.corrX.reserve(n3); c.corrR.reserve(n3);
+    for (int k = 0; k < 8 && !(rr < thr) && total < c.pcgMaxIter; ++k) {
         int budget = c.pcgMaxIter - total;
         int flag = 0;
         double rel = 0;
-        int it = runPcgPersistent<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, std::sqrt(thr / rr),
-                                                 learned ? std::min(budget, factorCap()) : budget, flag, rel, learned);
+        double tol = 0.5 * std::sqrt(thr / rr);
+        if (k == 0 && !pcgClassic()) tol = std::max(tol, 1e-8);
+        int it = runPcgPersistent<float, double>(c, c.valF, c.dynBF, c.r.p, c.corrX.p, c.corrR.p, c.z.p, c.p.p, c.Ap.p, tol,
+                                                 learned ? std::min(budget, factorCap()) : budget, flag, rel, learned, k > 0);
         total += it;
         launch(accumulateKernelD, vb, VB, 0, c.s, n3, c.corrX.p, c.sol.p);
         rr = mixedResidual(c, bF);
         if (debugPcg()) std::fprintf(stderr, "[pcg] mixed FP64-vector run it %d flag %d -> rr/b2 %.3e learned %d\n", it, flag, rr / rhs2, (int)learned);
+        if (learned && flag != 1) return false;
     }
     return !learned || rr < thr;
 }

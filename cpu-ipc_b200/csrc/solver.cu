@@ -539,7 +539,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                               &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
                               &c.fricLambda, &c.fricCoord, &c.fricBasis, &c.fricGLambda, &c.closeGVal, &c.closeSVal, &c.dynGVal, &c.dynHValD,
                               &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.corrX, &c.corrR, &c.sweptPt, &c.scratch,
-                              &c.scal, &c.energyBuf, &c.mpS, &c.mpT,
+                              &c.scal, &c.energyBuf, &c.mpS, &c.mpT, &c.pcgPipe, &c.pcgParts,
                               &c.faceTree.lo, &c.faceTree.hi, &c.faceTree.primLo, &c.faceTree.primHi, &c.faceTree.sceneBox, &c.edgeTree.lo,
                               &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox};
         for (auto* d : ds) d->free();
