@@ -107,6 +107,7 @@ struct Ctx {
     // static symmetric BSR pattern (elements), full storage
     int nnzb = 0;
     DBuf<int> rowPtr, colIdx, diagSlot;
+    std::vector<int> hRowPtr;  // host copy of rowPtr (static pattern)
     DBuf<int> hcPtr, hcIdx;    // per slot: element-block contributions (bit 31 = transpose)
     DBuf<int> gcPtr, gcIdx;    // per vertex: element gradient contributions
     DBuf<double> valD, constD;  // static values (FP64) and the constant bending part
@@ -160,6 +161,7 @@ struct Ctx {
     int lastPcgLaunchIters = 0;
     DBuf<unsigned> pcgBar;              // grid-barrier counters of the persistent PCG
     DBuf<double> pcgPipe, pcgParts;     // pipelined PCG: six recurrence vectors, two sets of partial sums
+    int pcgSliceMax = -1;               // cached pipelined PCG: largest static-slot count of a block's rows
     bool assembled = false;             // a Newton system has been assembled
 
     // learned preconditioner: network weights (FP32 master, BF16 copy, Adam

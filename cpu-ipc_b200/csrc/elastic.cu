@@ -426,6 +426,7 @@ void buildStaticPattern(Ctx& c, const std::vector<int>& tets, const std::vector<
         if (!h.empty()) CIPC_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
     };
     up(c.rowPtr, rowPtr); up(c.colIdx, col); up(c.diagSlot, diag); up(c.hcPtr, hcPtr); up(c.hcIdx, hcIdx);
+    c.hRowPtr = rowPtr;
     up(c.gcPtr, gcPtr); up(c.gcIdx, gcIdx);
     c.valD.reserve((size_t)9 * c.nnzb);
     c.valF.reserve((size_t)9 * c.nnzb);

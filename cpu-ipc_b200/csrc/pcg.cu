@@ -276,6 +276,7 @@ struct PcgArgs {
     VT *u, *w, *mA, *mB, *q, *s;  // pipelined variant only
     double *partA, *partB, *partC;
     double* pp;                   // pipelined variant: two sets of three partial arrays, PIPE_PMAX each
+    int sliceMax;                 // cached variant: static slots of the largest block row range
     double* scal;  // out: [3] rr, [4] iterations, [6] rhs2
     int* flag;     // out: 1 converged, 2 iteration cap, 3 barrier timeout
     unsigned* bar;  // BAR_WORDS words: grid-barrier counters and generation
@@ -634,6 +635,80 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
 // its last read.  The recurrences drift from the true residual in finite
 // precision; the callers judge every solve by the true FP64 residual.
 // ---------------------------------------------------------------------------
+// Rows a block owns in a single-pass launch (PB / GROUP consecutive rows)
+// and their static slots, diagonal extras and block-Jacobi inverses, staged
+// once per solve in shared memory: every iteration then reads the matrix
+// rows from shared memory and only the gathered vector from L2.
+constexpr int ROWS_PER_BLOCK = PB / GROUP;
+template <class MT>
+struct RowCache {
+    int row0, s0;
+    const int* rp;       // ROWS_PER_BLOCK + 1 slot offsets (global slot indices)
+    const int* col;
+    const MT* val;
+    const double* dex;   // 9 per row
+    const double* dinv;  // 9 per row
+};
+
+// shared-memory bytes of the cache for a given slice size
+template <class MT>
+__host__ __device__ constexpr size_t rowCacheBytes(int sliceMax) {
+    return (size_t)ROWS_PER_BLOCK * 9 * sizeof(double) * 2 + (size_t)sliceMax * 9 * sizeof(MT) + (size_t)sliceMax * sizeof(int) +
+           (ROWS_PER_BLOCK + 1) * sizeof(int);
+}
+
+template <class MT, class VT>
+__device__ RowCache<MT> loadRowCache(const PcgArgs<MT, VT>& a, unsigned char* smem) {
+    RowCache<MT> rc;
+    double* dex = reinterpret_cast<double*>(smem);
+    double* dinv = dex + ROWS_PER_BLOCK * 9;
+    MT* val = reinterpret_cast<MT*>(dinv + ROWS_PER_BLOCK * 9);
+    int* col = reinterpret_cast<int*>(val + (size_t)a.sliceMax * 9);
+    int* rp = col + a.sliceMax;
+    rc.row0 = blockIdx.x * ROWS_PER_BLOCK;
+    const int nrows = min(ROWS_PER_BLOCK, a.nv - rc.row0);
+    for (int i = threadIdx.x; i <= nrows; i += blockDim.x) rp[i] = a.rowPtr[rc.row0 + i];
+    __syncthreads();
+    rc.s0 = rp[0];
+    const int ns = rp[nrows] - rc.s0;  // <= sliceMax (host-computed maximum over blocks)
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) col[k] = a.col[rc.s0 + k];
+    for (int k = threadIdx.x; k < 9 * ns; k += blockDim.x) val[k] = a.val[(size_t)9 * rc.s0 + k];
+    for (int k = threadIdx.x; k < 9 * nrows; k += blockDim.x) {
+        dex[k] = a.diagExtra[(size_t)9 * rc.row0 + k];
+        dinv[k] = a.Dinv[(size_t)9 * rc.row0 + k];
+    }
+    __syncthreads();
+    rc.rp = rp; rc.col = col; rc.val = val; rc.dex = dex; rc.dinv = dinv;
+    return rc;
+}
+
+// acc = (A u)_row with the row's static part from the cache
+template <class MT, class VT>
+__device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowCache<MT>& rc, const RowIter& it, int row, const VT* u, VT acc[3]) {
+    const int lr = row - rc.row0;
+    if (row < a.nv) {
+        for (int k = rc.rp[lr] + it.lane; k < rc.rp[lr + 1]; k += GROUP) {
+            int kk = k - rc.s0;
+            int c = rc.col[kk];
+            VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+            blockMulAdd(rc.val + (size_t)9 * kk, xv, acc);
+        }
+        if (a.dRowS) {
+            for (int k = a.dRowS[row] + it.lane; k < a.dRowE[row]; k += GROUP) {
+                int c = a.dCol[k];
+                VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+                blockMulAdd(a.dVal + (size_t)9 * k, xv, acc);
+            }
+        }
+    }
+    groupReduce3(acc);
+    if (row < a.nv && it.lane == 0) {
+        const double* D = rc.dex + 9 * lr;
+        VT uv[3] = {__ldcg(u + 3 * row), __ldcg(u + 3 * row + 1), __ldcg(u + 3 * row + 2)};
+        for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)uv[0] + D[3 * q + 1] * (double)uv[1] + D[3 * q + 2] * (double)uv[2]);
+    }
+}
+
 template <class MT, class VT>
 __device__ __forceinline__ void rowAx(const PcgArgs<MT, VT>& a, const RowIter& it, int row, const VT* u, VT acc[3]) {
     if (row < a.nv) rowSpmv(a, row, it.lane, u, acc);
@@ -697,11 +772,30 @@ __device__ __forceinline__ void jacobiRow(const double* Dinv, const VT* in, VT* 
     out[3 * row + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
 }
 
-template <class MT, class VT, bool LEARNED>
+template <class MT, class VT, bool LEARNED, bool CACHED>
 __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
+    extern __shared__ __align__(16) unsigned char pipeSmem[];
     const unsigned nb = gridDim.x;
     const int nv = a.nv;
     const RowIter it;
+    RowCache<MT> rc{};
+    if (CACHED) rc = loadRowCache(a, pipeSmem);
+    auto Ax = [&](int row, const VT* u, VT acc[3]) {
+        if (CACHED) rowAxCached(a, rc, it, row, u, acc);
+        else rowAx(a, it, row, u, acc);
+    };
+    auto jac = [&](const VT* in, VT* out, int row) {
+        if (CACHED) {
+            // block-Jacobi inverse from the cache
+            const double* D = rc.dinv + 9 * (row - rc.row0);
+            double r0 = in[3 * row], r1 = in[3 * row + 1], r2 = in[3 * row + 2];
+            out[3 * row] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
+            out[3 * row + 1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
+            out[3 * row + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
+        } else {
+            jacobiRow(a.Dinv, in, out, row);
+        }
+    };
     VT* sw = a.Ap;  // S w for the factor passes
     auto part = [&](int set, int k) { return a.pp + (size_t)(3 * set + k) * PIPE_PMAX; };
     // x = 0, r = b, u = M r; the recurrence vectors start at 0
@@ -715,7 +809,7 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
                 a.r[i] = a.b[i];
                 rr += (double)a.r[i] * (double)a.r[i];
             }
-            if (!LEARNED) jacobiRow(a.Dinv, (const VT*)a.r, a.u, row);
+            if (!LEARNED) jac((const VT*)a.r, a.u, row);
         }
     }
     if (LEARNED && !factorPasses(a, it, (const VT*)a.r, sw, a.u)) return;
@@ -725,7 +819,7 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     for (int base = it.first; base < nv; base += it.stride) {
         int row = base + it.grp;
         VT acc[3] = {VT(0), VT(0), VT(0)};
-        rowAx(a, it, row, (const VT*)a.u, acc);
+        Ax(row, (const VT*)a.u, acc);
         if (row < nv && it.lane == 0) {
             for (int q = 0; q < 3; ++q) {
                 int i = 3 * row + q;
@@ -733,7 +827,7 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
                 g += (double)a.r[i] * (double)a.u[i];
                 dl += (double)acc[q] * (double)a.u[i];
             }
-            if (!LEARNED) jacobiRow(a.Dinv, (const VT*)a.w, a.mA, row);
+            if (!LEARNED) jac((const VT*)a.w, a.mA, row);
         }
     }
     blockReduce3(rr, g, dl);
@@ -758,7 +852,7 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         for (int base = it.first; base < nv; base += it.stride) {
             int row = base + it.grp;
             VT acc[3] = {VT(0), VT(0), VT(0)};
-            rowAx(a, it, row, mCur, acc);
+            Ax(row, mCur, acc);
             if (row < nv && it.lane == 0) {
                 for (int q = 0; q < 3; ++q) {
                     int i = 3 * row + q;
@@ -776,7 +870,7 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
                     lg += (double)rv * (double)uv;
                     ld += (double)wv * (double)uv;
                 }
-                if (!LEARNED) jacobiRow(a.Dinv, (const VT*)a.w, mNext, row);
+                if (!LEARNED) jac((const VT*)a.w, mNext, row);
             }
         }
         const int set = (iter + 1) & 1;
@@ -904,15 +998,58 @@ static bool pcgClassic() {
     return v == 1;
 }
 
+// CIPC_PCG_NOCACHE=1 keeps the pipelined kernel's matrix rows in global memory.
+static bool pcgNoCache() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_PCG_NOCACHE"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+
+// Largest number of static slots over the row ranges the cached kernel's
+// blocks own (computed once per context from the static pattern).
+static int pcgSliceMax(Ctx& c) {
+    if (c.pcgSliceMax < 0) {
+        int m = 0;
+        for (int r0 = 0; r0 < c.nv; r0 += ROWS_PER_BLOCK) {
+            int r1 = std::min(c.nv, r0 + ROWS_PER_BLOCK);
+            m = std::max(m, c.hRowPtr[r1] - c.hRowPtr[r0]);
+        }
+        c.pcgSliceMax = m;
+    }
+    return c.pcgSliceMax;
+}
+
 template <class MT, class VT, bool LEARNED>
 static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool classic) {
-    const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED>;
+    int needed = std::max(1, (c.nv * GROUP + PB - 1) / PB);
+    int cap = std::min(PMAX, PIPE_PMAX);
+    void* args[] = {&a};
+    if (!classic && !pcgNoCache() && !c.hRowPtr.empty() && needed <= cap) {
+        // single-pass launch: each block owns ROWS_PER_BLOCK rows for the whole
+        // solve and stages them in shared memory
+        a.sliceMax = pcgSliceMax(c);
+        size_t smem = rowCacheBytes<MT>(a.sliceMax);
+        const void* fn = (const void*)pcgPipelinedKernel<MT, VT, LEARNED, true>;
+        int maxOptin = 0, dev = 0;
+        CIPC_CUDA(cudaGetDevice(&dev));
+        CIPC_CUDA(cudaDeviceGetAttribute(&maxOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (smem + 4096 <= (size_t)maxOptin) {
+            CIPC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int perSM = 0;
+            CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, smem));
+            if (perSM >= 1 && needed <= perSM * smCount) {
+                ++g_kernelLaunches;
+                CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(needed), dim3(PB), args, smem, c.s));
+                return;
+            }
+        }
+    }
+    a.sliceMax = 0;
+    const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false>;
     int perSM = 0;
     CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, 0));
     if (perSM < 1) throw std::runtime_error("persistent PCG kernel does not fit on an SM");
-    int needed = std::max(1, (c.nv * GROUP + PB - 1) / PB);
-    int grid = std::max(1, std::min(std::min(std::min(perSM, pcgBlocksPerSm()) * smCount, needed), std::min(PMAX, PIPE_PMAX)));
-    void* args[] = {&a};
+    int grid = std::max(1, std::min(std::min(std::min(perSM, pcgBlocksPerSm()) * smCount, needed), cap));
     ++g_kernelLaunches;
     CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PB), args, 0, c.s));
 }
