@@ -210,6 +210,10 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# host-clock stage timers of IPCStepStats (IPCSolver.cpp:1286-1315), per step
+STAGES = ("assemblyMilliseconds", "linearSolveMilliseconds", "ccdMilliseconds", "lineSearchMilliseconds", "postLineSearchMilliseconds")
+
+
 def max_over_ranks(value, pg, device):
     """The slowest rank's time (all ranks take part; pg None means one rank)."""
     import torch
@@ -233,6 +237,7 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
     launches0 = cipc.kernel_launches()
     total_ms = 0.0
     newton = pcg = 0
+    stages = {k: 0.0 for k in STAGES}
     ndyn = []
     for _ in range(steps):
         flush.fill_(1.0)
@@ -241,12 +246,15 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
         total_ms += ms
         newton += st["newtonIterations"]
         pcg += st["pcgIterations"]
+        for k in STAGES:
+            stages[k] += st[k]
         ndyn.append(sim.counts()[8])
     launches = cipc.kernel_launches() - launches0
     nprof, prof_ms = sim.profile_read() if kind else (0, 0.0)
     if kind:
         sim.profile(0)
-    return dict(ms=total_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches)
+    return dict(ms=total_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches,
+                stages={k: v / max(1, steps) for k, v in stages.items()})
 
 
 def main():
@@ -359,6 +367,7 @@ def main():
                "ms_per_newton_iteration": max_ms / max(1, r["newton"]),
                "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
                "vertices": nv, "static_blocks": counts[7], "contact_blocks_mean": counts[8]}
+        cfg["stage_ms_per_step"] = {k.replace("Milliseconds", ""): round(v, 3) for k, v in r["stages"].items()}
         cfg["timed_frames"] = f"{args.settle_steps + max(3, args.warmup)}-{args.settle_steps + max(3, args.warmup) + args.steps - 1}"
         if train:
             cfg["training"] = train

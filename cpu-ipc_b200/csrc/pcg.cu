@@ -364,15 +364,18 @@ __device__ __forceinline__ double sumPartialsCG(const double* p, int n) {
 constexpr int BAR_SUB = 16;
 constexpr int BAR_STRIDE = 32;                     // unsigned words per 128-byte line
 constexpr int BAR_WORDS = BAR_STRIDE * (BAR_SUB + 2);  // sub-counters, top counter, generation
-__device__ __forceinline__ bool gridBarrier(unsigned* bar, int* flag, unsigned nblocks) {
+__device__ __forceinline__ bool gridBarrier(unsigned* bar, int* flag, unsigned nblocks, unsigned& epoch) {
+    // epoch counts the barriers this block has passed in this launch; the
+    // generation word (zeroed before the launch) reaches it when all blocks
+    // have arrived, so no read of the generation precedes the arrival
+    const unsigned target = ++epoch;
     __syncthreads();
     __shared__ int ok;
     if (threadIdx.x == 0) {
         volatile unsigned* vgen = bar + BAR_STRIDE * (BAR_SUB + 1);
         unsigned* top = bar + BAR_STRIDE * BAR_SUB;
-        unsigned g = *vgen;
         __threadfence();
-        ok = 1;
+        int good = 1;
         const unsigned sub = blockIdx.x % BAR_SUB;
         const unsigned subSize = (nblocks - sub + BAR_SUB - 1) / BAR_SUB;
         const unsigned nsub = nblocks < (unsigned)BAR_SUB ? nblocks : (unsigned)BAR_SUB;
@@ -388,14 +391,16 @@ __device__ __forceinline__ bool gridBarrier(unsigned* bar, int* flag, unsigned n
         }
         if (!released) {
             long long spins = 0;
-            while (*vgen == g) {
-                if (++spins > (1ll << 25)) { atomicExch(flag, 3); ok = 0; break; }
+            while ((int)(*vgen - target) < 0) {
+                if (++spins > (1ll << 25)) { atomicExch(flag, 3); good = 0; break; }
             }
         }
         __threadfence();
+        if (good && *(volatile int*)flag == 3) good = 0;  // another block timed out
+        ok = good;
     }
     __syncthreads();
-    return ok && *(volatile int*)flag != 3;
+    return ok != 0;
 }
 
 // Row-group iteration shared by every phase: the same (block, lane group)
@@ -463,7 +468,7 @@ __device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int
 // z, t = G (S r), z = S^T G^T t; returns this thread's r.z contribution
 // (valid on lane 0 of each group).  Three barriers; false on barrier timeout.
 template <class MT, class VT>
-__device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double& rz, double* partRR, double rrLocal) {
+__device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double& rz, double* partRR, double rrLocal, unsigned& ep) {
     const unsigned nb = gridDim.x;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
@@ -480,7 +485,7 @@ __device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double
         blockReduce2(rrLocal, dummy);
         if (threadIdx.x == 0) partRR[blockIdx.x] = rrLocal;
     }
-    if (!gridBarrier(a.bar, a.flag, nb)) return false;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
         bool active = row < a.nv;
@@ -490,7 +495,7 @@ __device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double
         if (active && it.lane == 0)
             for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
     }
-    if (!gridBarrier(a.bar, a.flag, nb)) return false;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     rz = 0;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
@@ -514,6 +519,7 @@ __device__ bool learnedApply(const PcgArgs<MT, VT>& a, const RowIter& it, double
 template <class MT, class VT, bool LEARNED>
 __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
     const unsigned nb = gridDim.x;
+    unsigned ep = 0;
     const int nv = a.nv;
     const RowIter it;
     // init: x = 0, r = b, z = M r, p = 0, Ap = 0 (the first beta is 0)
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
         }
     }
     if (LEARNED) {
-        if (!learnedApply(a, it, rz, a.partA, rr)) return;
+        if (!learnedApply(a, it, rz, a.partA, rr, ep)) return;
         double dummy = 0;
         blockReduce2(rz, dummy);
         if (threadIdx.x == 0) a.partB[blockIdx.x] = rz;
@@ -541,7 +547,7 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
         blockReduce2(rr, rz);
         if (threadIdx.x == 0) { a.partA[blockIdx.x] = rr; a.partB[blockIdx.x] = rz; }
     }
-    if (!gridBarrier(a.bar, a.flag, nb)) return;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
     sumPartials2CG(a.partA, a.partB, nb, rr, rz);
     const double rhs2 = rr;
     const double thr = fmax(a.tol * a.tol * rr, 2.2250738585072014e-308);
@@ -575,7 +581,7 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
             blockReduce2(d, dummy);
             if (threadIdx.x == 0) a.partC[blockIdx.x] = d;
         }
-        if (!gridBarrier(a.bar, a.flag, nb)) return;
+        if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
         VT alpha = (VT)(rz / sumPartialsCG(a.partC, nb));
         // phase 2: x += alpha p ; r -= alpha Ap ; z = M r
         double lrr = 0, lrz = 0;
@@ -594,7 +600,7 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
             }
         }
         if (LEARNED) {
-            if (!learnedApply(a, it, lrz, a.partA, lrr)) return;
+            if (!learnedApply(a, it, lrz, a.partA, lrr, ep)) return;
             double dummy = 0;
             blockReduce2(lrz, dummy);
             if (threadIdx.x == 0) a.partB[blockIdx.x] = lrz;
@@ -602,7 +608,7 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
             blockReduce2(lrr, lrz);
             if (threadIdx.x == 0) { a.partA[blockIdx.x] = lrr; a.partB[blockIdx.x] = lrz; }
         }
-        if (!gridBarrier(a.bar, a.flag, nb)) return;
+        if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
         double rzNew;
         sumPartials2CG(a.partA, a.partB, nb, rr, rzNew);
         ++iter;
@@ -723,7 +729,7 @@ __device__ __forceinline__ void rowAx(const PcgArgs<MT, VT>& a, const RowIter& i
 // out = M^-1 in for the factor: S in -> tmp (own rows), barrier, t = G tmp,
 // barrier, out = S^T G^T t.  Ends without a barrier; false on timeout.
 template <class MT, class VT>
-__device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const VT* in, VT* tmp, VT* out) {
+__device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const VT* in, VT* tmp, VT* out, unsigned& ep) {
     const unsigned nb = gridDim.x;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
@@ -735,7 +741,7 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
             tmp[3 * row + 2] = (VT)(S[6] * r0 + S[7] * r1 + S[8] * r2);
         }
     }
-    if (!gridBarrier(a.bar, a.flag, nb)) return false;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
         bool active = row < a.nv;
@@ -745,7 +751,7 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
         if (active && it.lane == 0)
             for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
     }
-    if (!gridBarrier(a.bar, a.flag, nb)) return false;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
         bool active = row < a.nv;
@@ -776,6 +782,7 @@ template <class MT, class VT, bool LEARNED, bool CACHED>
 __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     extern __shared__ __align__(16) unsigned char pipeSmem[];
     const unsigned nb = gridDim.x;
+    unsigned ep = 0;
     const int nv = a.nv;
     const RowIter it;
     RowCache<MT> rc{};
@@ -812,8 +819,8 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
             if (!LEARNED) jac((const VT*)a.r, a.u, row);
         }
     }
-    if (LEARNED && !factorPasses(a, it, (const VT*)a.r, sw, a.u)) return;
-    if (!gridBarrier(a.bar, a.flag, nb)) return;
+    if (LEARNED && !factorPasses(a, it, (const VT*)a.r, sw, a.u, ep)) return;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
     // w = A u, m = M w, gamma = (r,u), delta = (w,u)
     double g = 0, dl = 0;
     for (int base = it.first; base < nv; base += it.stride) {
@@ -832,8 +839,8 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     }
     blockReduce3(rr, g, dl);
     if (threadIdx.x == 0) { part(0, 0)[blockIdx.x] = rr; part(0, 1)[blockIdx.x] = g; part(0, 2)[blockIdx.x] = dl; }
-    if (LEARNED && !factorPasses(a, it, (const VT*)a.w, sw, a.mA)) return;
-    if (!gridBarrier(a.bar, a.flag, nb)) return;
+    if (LEARNED && !factorPasses(a, it, (const VT*)a.w, sw, a.mA, ep)) return;
+    if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
     sumPartials3CG(part(0, 0), part(0, 1), part(0, 2), nb, rr, g, dl);
     const double rhs2 = rr;
     const double thr = fmax(a.tol * a.tol * rr, 2.2250738585072014e-308);
@@ -878,8 +885,8 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         if (threadIdx.x == 0) { part(set, 0)[blockIdx.x] = lrr; part(set, 1)[blockIdx.x] = lg; part(set, 2)[blockIdx.x] = ld; }
         // the factor's m is replaced only in its third pass, two barriers
         // after every row read it
-        if (LEARNED && !factorPasses(a, it, (const VT*)a.w, sw, mNext)) return;
-        if (!gridBarrier(a.bar, a.flag, nb)) return;
+        if (LEARNED && !factorPasses(a, it, (const VT*)a.w, sw, mNext, ep)) return;
+        if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
         gPrev = g;
         alphaPrev = alpha;
         sumPartials3CG(part(set, 0), part(set, 1), part(set, 2), nb, rr, g, dl);
