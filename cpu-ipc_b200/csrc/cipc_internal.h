@@ -182,6 +182,10 @@ struct Ctx {
     DBuf<float> mpVec, mpDGS, mpDGD, mpDH, mpDES, mpDED, mpDAgg, mpDS, mpDSD;
     DBuf<float> mpBD, mpBX, mpPart;     // backward: per-item gradients, second input block, split-K partials
     DBuf<unsigned char> mpLowS, mpLowD; // 1 for lower slots of the static / contact pattern
+    DBuf<int> mpFlatS, mpFlatD;         // flat lower-edge lists: slot, row, column (3 arrays each, packed)
+    int nFlatS = -1, nFlatD = 0;
+    DBuf<int> mpScanTmpI;               // row counts and offsets of the flat lists
+    DBuf<unsigned char> mpScanTmp;
 
     // collision structures
     DevBvh faceTree, edgeTree;

@@ -29,6 +29,7 @@
 #include "mpnn.h"
 
 #include <cuda_bf16.h>
+#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -189,49 +190,6 @@ __global__ void degreeKernel(int nv, const int* rowPtr, const int* col, const in
     }
 }
 
-// ---------------------------------------------------------------------------
-// forward
-// ---------------------------------------------------------------------------
-// out[H] = relu(W in + b), W row-major [H][IN]
-template <int IN>
-__device__ __forceinline__ void denseRelu(const bf16* Wm, const bf16* b, const float* in, float* out) {
-    for (int o = 0; o < MPNN_H; ++o) {
-        float s = W(b, o);
-#pragma unroll 8
-        for (int i = 0; i < IN; ++i) s += W(Wm, o * IN + i) * in[i];
-        out[o] = relu(s);
-    }
-}
-
-__global__ void embedNodeKernel(int nv, const float* f, const bf16* w, float* h0) {
-    CIPC_KERNEL_LOOP(v, nv) denseRelu<MPNN_NF>(w + MP_WN0, w + MP_BN0, f + MPNN_NF * v, h0 + (size_t)MPNN_H * v);
-}
-
-__global__ void embedEdgeKernel(int nv, const int* rowS, const int* rowE, const int* col, const float* g, const bf16* w, float* e0) {
-    CIPC_KERNEL_LOOP(v, nv) {
-        for (int k = rowS[v]; k < rowE[v]; ++k) {
-            if (col[k] >= v) continue;
-            denseRelu<MPNN_EF>(w + MP_WE0, w + MP_BE0, g + (size_t)9 * k, e0 + (size_t)MPNN_H * k);
-        }
-    }
-}
-
-__global__ void edgeLayerKernel(int nv, const int* rowS, const int* rowE, const int* col, const float* ePrev, const float* hPrev, const bf16* Wm,
-                                const bf16* b, float* eNext) {
-    CIPC_KERNEL_LOOP(v, nv) {
-        for (int k = rowS[v]; k < rowE[v]; ++k) {
-            int c = col[k];
-            if (c >= v) continue;
-            float in[2 * MPNN_H];
-            for (int t = 0; t < MPNN_H; ++t) {
-                in[t] = ePrev[(size_t)MPNN_H * k + t];
-                in[MPNN_H + t] = hPrev[(size_t)MPNN_H * v + t] + hPrev[(size_t)MPNN_H * c + t];
-            }
-            denseRelu<2 * MPNN_H>(Wm, b, in, eNext + (size_t)MPNN_H * k);
-        }
-    }
-}
-
 // mean of incident edge states; an edge is read at its lower slot
 __global__ void aggregateKernel(int nv, const int* rowPtr, const int* col, const int* mirS, const float* eS, const int* dRowS, const int* dRowE,
                                 const int* dCol, const int* mirD, const float* eD, const int* deg, float* agg) {
@@ -258,65 +216,145 @@ __global__ void aggregateKernel(int nv, const int* rowPtr, const int* col, const
     }
 }
 
-__global__ void nodeLayerKernel(int nv, const float* hPrev, const float* agg, const bf16* Wm, const bf16* b, float* hNext) {
-    CIPC_KERNEL_LOOP(v, nv) {
-        float in[2 * MPNN_H];
-        for (int t = 0; t < MPNN_H; ++t) { in[t] = hPrev[(size_t)MPNN_H * v + t]; in[MPNN_H + t] = agg[(size_t)MPNN_H * v + t]; }
-        denseRelu<2 * MPNN_H>(Wm, b, in, hNext + (size_t)MPNN_H * v);
+// ---------------------------------------------------------------------------
+// Tiled dense layers of the forward pass.  A CTA stages one weight matrix
+// (transposed, FP32 from the BF16 copy) and a tile of DT_ITEMS input rows in
+// shared memory; two threads per item split the outputs and accumulate in
+// FP32 registers.  Items are nodes or the lower edges of a flat edge list;
+// gather and emit functors read the layer's inputs and write its outputs.
+// ---------------------------------------------------------------------------
+constexpr int DT_ITEMS = 64;
+constexpr int DT_THREADS = 2 * DT_ITEMS;
+
+template <int IN, int OUT, class G, class E>
+__global__ void __launch_bounds__(DT_THREADS) denseTiledKernel(int n, G gather, E emit, const bf16* Wm, const bf16* bias) {
+    constexpr int HALF = (OUT + 1) / 2;
+    __shared__ float sW[IN][OUT + 1];
+    __shared__ float sB[OUT];
+    __shared__ float sX[DT_ITEMS][IN + 1];
+    for (int t = threadIdx.x; t < IN * OUT; t += DT_THREADS) sW[t % IN][t / IN] = W(Wm, t);
+    for (int t = threadIdx.x; t < OUT; t += DT_THREADS) sB[t] = W(bias, t);
+    for (int base = blockIdx.x * DT_ITEMS; base < n; base += gridDim.x * DT_ITEMS) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < DT_ITEMS * IN; t += DT_THREADS) {
+            int r = t / IN, i = t % IN, item = base + r;
+            sX[r][i] = item < n ? gather(item, i) : 0.f;
+        }
+        __syncthreads();
+        const int r = threadIdx.x >> 1, h = threadIdx.x & 1, item = base + r;
+        float acc[HALF];
+#pragma unroll
+        for (int q = 0; q < HALF; ++q) {
+            int o = h * HALF + q;
+            acc[q] = o < OUT ? sB[o] : 0.f;
+        }
+        for (int i = 0; i < IN; ++i) {
+            float x = sX[r][i];
+#pragma unroll
+            for (int q = 0; q < HALF; ++q) {
+                int o = h * HALF + q;
+                if (o < OUT) acc[q] += sW[i][o] * x;
+            }
+        }
+        if (item < n) {
+#pragma unroll
+            for (int q = 0; q < HALF; ++q) {
+                int o = h * HALF + q;
+                if (o < OUT) emit(item, o, acc[q]);
+            }
+        }
     }
 }
 
-// diagonal head: G_ii lower triangle, diagonal softplus
-__global__ void headDiagKernel(int nv, const float* hL, const bf16* w, const int* diagSlot, const int* btype, float* gS, float* headD) {
+// flat list of the lower edges of a row-ranged pattern
+__global__ void lowerCountKernel(int nv, const int* rowS, const int* rowE, const int* col, int* cnt) {
     CIPC_KERNEL_LOOP(v, nv) {
-        float o[6];
-        for (int q = 0; q < 6; ++q) {
-            float s = W(w + MP_BD, q);
-            for (int t = 0; t < MPNN_H; ++t) s += W(w + MP_WD, q * MPNN_H + t) * hL[(size_t)MPNN_H * v + t];
-            o[q] = s;
-            headD[6 * v + q] = s;
-        }
+        int k = 0;
+        for (int s = rowS[v]; s < rowE[v]; ++s) k += col[s] < v;
+        cnt[v] = k;
+    }
+}
+__global__ void lowerFillKernel(int nv, const int* rowS, const int* rowE, const int* col, const int* off, int* eSlot, int* eI, int* eJ) {
+    CIPC_KERNEL_LOOP(v, nv) {
+        int o = off[v];
+        for (int s = rowS[v]; s < rowE[v]; ++s)
+            if (col[s] < v) { eSlot[o] = s; eI[o] = v; eJ[o] = col[s]; ++o; }
+    }
+}
+
+struct NodeFeatGather {
+    const float* f;
+    __device__ float operator()(int v, int i) const { return f[MPNN_NF * v + i]; }
+};
+struct EdgeFeatGather {
+    const int* slot;
+    const float* g;
+    __device__ float operator()(int e, int i) const { return g[(size_t)9 * slot[e] + i]; }
+};
+struct EdgeLayerGather {  // [e_l ; h_i + h_j]
+    const int *slot, *ei, *ej;
+    const float *e, *h;
+    __device__ float operator()(int k, int i) const {
+        if (i < MPNN_H) return e[(size_t)MPNN_H * slot[k] + i];
+        i -= MPNN_H;
+        return h[(size_t)MPNN_H * ei[k] + i] + h[(size_t)MPNN_H * ej[k] + i];
+    }
+};
+struct NodeLayerGather {  // [h ; agg]
+    const float *h, *agg;
+    __device__ float operator()(int v, int i) const {
+        return i < MPNN_H ? h[(size_t)MPNN_H * v + i] : agg[(size_t)MPNN_H * v + i - MPNN_H];
+    }
+};
+struct HeadEdgeGather {  // [e_L ; g]
+    const int* slot;
+    const float *e, *g;
+    __device__ float operator()(int k, int i) const {
+        return i < MPNN_H ? e[(size_t)MPNN_H * slot[k] + i] : g[(size_t)9 * slot[k] + i - MPNN_H];
+    }
+};
+struct NodeHiddenGather {
+    const float* h;
+    __device__ float operator()(int v, int i) const { return h[(size_t)MPNN_H * v + i]; }
+};
+
+struct ReluEmitNode {
+    float* out;
+    __device__ void operator()(int v, int o, float a) const { out[(size_t)MPNN_H * v + o] = relu(a); }
+};
+struct ReluEmitEdge {
+    const int* slot;
+    float* out;
+    __device__ void operator()(int k, int o, float a) const { out[(size_t)MPNN_H * slot[k] + o] = relu(a); }
+};
+// G_ij into the lower slot and G_ij^T into its mirror; no block touches a
+// Dirichlet vertex
+struct HeadEdgeEmit {
+    const int *slot, *ei, *ej, *mirror, *btype;
+    float* gOut;
+    __device__ void operator()(int k, int o, float a) const {
+        const int s = slot[k];
+        const float v = (btype[ei[k]] == 0 && btype[ej[k]] == 0) ? a : 0.f;
+        gOut[(size_t)9 * s + o] = v;
+        const int m = mirror[s];
+        if (m >= 0) gOut[(size_t)9 * m + 3 * (o % 3) + o / 3] = v;
+    }
+};
+// G_ii: lower triangle, softplus diagonal; Dirichlet vertices keep I
+struct HeadDiagEmit {
+    const int *diagSlot, *btype;
+    float *gS, *headD;
+    __device__ void operator()(int v, int o, float a) const {
+        headD[6 * v + o] = a;
         float* G = gS + (size_t)9 * diagSlot[v];
-        if (btype[v] != 0) {
-            // Dirichlet vertex: its rows of the matrix are decoupled, G_ii = I
-            for (int k = 0; k < 9; ++k) G[k] = (k % 4 == 0) ? 1.f : 0.f;
-            continue;
-        }
-        G[0] = softplus(o[0]); G[1] = 0.f; G[2] = 0.f;
-        G[3] = o[3]; G[4] = softplus(o[1]); G[5] = 0.f;
-        G[6] = o[4]; G[7] = o[5]; G[8] = softplus(o[2]);
+        const bool fixedV = btype[v] != 0;
+        const int pos[6] = {0, 4, 8, 3, 6, 7};
+        float val = o < 3 ? softplus(a) : a;
+        if (fixedV) val = o < 3 ? 1.f : 0.f;
+        G[pos[o]] = val;
+        if (o == 0) { G[1] = 0.f; G[2] = 0.f; G[5] = 0.f; }
     }
-}
-
-// off-diagonal head: G_ij = Wo [e_L ; g] + bo for lower slots, transposed
-// into the mirror slot; contact diagonal slots carry no factor part
-__global__ void headEdgeKernel(int nv, const int* rowS, const int* rowE, const int* col, const int* mirror, const float* eL, const float* g,
-                               const bf16* w, const int* btype, float* gOut, int zeroDiag) {
-    CIPC_KERNEL_LOOP(v, nv) {
-        for (int k = rowS[v]; k < rowE[v]; ++k) {
-            int c = col[k];
-            if (c == v) {
-                if (zeroDiag) for (int q = 0; q < 9; ++q) gOut[(size_t)9 * k + q] = 0.f;
-                continue;
-            }
-            if (c > v) continue;
-            float o[9];
-            bool coupled = btype[v] == 0 && btype[c] == 0;  // no factor block touches a Dirichlet vertex
-            for (int q = 0; q < 9; ++q) {
-                const bf16* Wr = w + MP_WO + q * (MPNN_H + MPNN_EF);
-                float s = W(w + MP_BO, q);
-                for (int t = 0; t < MPNN_H; ++t) s += W(Wr, t) * eL[(size_t)MPNN_H * k + t];
-                for (int t = 0; t < MPNN_EF; ++t) s += W(Wr, MPNN_H + t) * g[(size_t)9 * k + t];
-                o[q] = coupled ? s : 0.f;
-            }
-            for (int q = 0; q < 9; ++q) gOut[(size_t)9 * k + q] = o[q];
-            int m = mirror[k];
-            if (m >= 0)
-                for (int a = 0; a < 3; ++a)
-                    for (int b = 0; b < 3; ++b) gOut[(size_t)9 * m + 3 * a + b] = o[3 * b + a];
-        }
-    }
-}
+};
 
 // ---------------------------------------------------------------------------
 // factor and scaled operator products (FP32 vectors, one thread per row)
@@ -752,6 +790,27 @@ void mpnnGetGrad(Ctx& c, float* g) {
     CIPC_CUDA(cudaStreamSynchronize(c.s));
 }
 
+// Flat list of the lower edges of a row-ranged pattern: three arrays of
+// `count` ints (slot, row, column) packed in `out`.  Returns the count.
+static int buildLowerList(Ctx& c, const int* rowS, const int* rowE, const int* col, DBuf<int>& out) {
+    int nv = c.nv;
+    c.mpScanTmpI.reserve(2 * (size_t)nv + 2);
+    int* cnt = c.mpScanTmpI.p;
+    int* off = cnt + nv + 1;
+    launch(lowerCountKernel, blocksFor(nv), TB, 0, c.s, nv, rowS, rowE, col, cnt);
+    CIPC_CUDA(cudaMemsetAsync(cnt + nv, 0, sizeof(int), c.s));
+    size_t bytes = 0;
+    CIPC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt, off, nv + 1, c.s));
+    c.mpScanTmp.reserve(bytes + 16);
+    CIPC_CUDA(cub::DeviceScan::ExclusiveSum(c.mpScanTmp.p, bytes, cnt, off, nv + 1, c.s));
+    int n = 0;
+    CIPC_CUDA(cudaMemcpyAsync(&n, off + nv, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    out.reserve(3 * (size_t)std::max(n, 1));
+    if (n > 0) launch(lowerFillKernel, blocksFor(nv), TB, 0, c.s, nv, rowS, rowE, col, (const int*)off, out.p, out.p + n, out.p + 2 * (size_t)n);
+    return n;
+}
+
 template <class MT>
 static void prepareT(Ctx& c, const MT* val, const MT* dval, bool features) {
     int nv = c.nv;
@@ -786,6 +845,10 @@ static void prepareT(Ctx& c, const MT* val, const MT* dval, bool features) {
         launch(lowerMaskKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, c.mpLowD.p);
         if (features) launch(edgeFeatKernel<MT>, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, dval, (const double*)c.mpS.p, c.mpEdgeFD.p);
     }
+    if (features) {  // the network's flat edge lists
+        if (c.nFlatS < 0) c.nFlatS = buildLowerList(c, (const int*)c.mpRowS.p, (const int*)c.mpRowE.p, (const int*)c.colIdx.p, c.mpFlatS);
+        c.nFlatD = d.on ? buildLowerList(c, d.rs, d.re, d.col, c.mpFlatD) : 0;
+    }
     c.mpDeg.reserve(nv);
     launch(degreeKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, (const int*)c.colIdx.p, (const int*)c.mpMirS.p, d.rs, d.re, d.col,
            (const int*)c.mpMirD.p, c.mpDeg.p);
@@ -814,27 +877,36 @@ void mpnnForward(Ctx& c) {
     auto H = [&](int l) { return c.mpH.p + (size_t)l * MPNN_H * nv; };
     auto ES = [&](int l) { return c.mpES.p + (size_t)l * MPNN_H * es; };
     auto ED = [&](int l) { return c.mpED.p + (size_t)l * MPNN_H * ed; };
-    const int *rs = c.mpRowS.p, *re = c.mpRowE.p, *col = c.colIdx.p;
-    launch(embedNodeKernel, blocksFor(nv), TB, 0, c.s, nv, (const float*)c.mpNodeF.p, w, H(0));
-    launch(embedEdgeKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const float*)c.mpEdgeF.p, w, ES(0));
-    if (d.on) launch(embedEdgeKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const float*)c.mpEdgeFD.p, w, ED(0));
+    const int nS = c.nFlatS, nD = d.on ? c.nFlatD : 0;
+    const int *sSlot = c.mpFlatS.p, *sI = sSlot + nS, *sJ = sSlot + 2 * (size_t)nS;
+    const int *dSlot = c.mpFlatD.p, *dI = dSlot + nD, *dJ = dSlot + 2 * (size_t)nD;
+    auto grid = [](int n) { return std::max(1, std::min((n + DT_ITEMS - 1) / DT_ITEMS, 148 * 16)); };
+    // embeddings
+    launch(denseTiledKernel<MPNN_NF, MPNN_H, NodeFeatGather, ReluEmitNode>, grid(nv), DT_THREADS, 0, c.s, nv, NodeFeatGather{c.mpNodeF.p},
+           ReluEmitNode{H(0)}, w + MP_WN0, w + MP_BN0);
+    if (nS) launch(denseTiledKernel<MPNN_EF, MPNN_H, EdgeFeatGather, ReluEmitEdge>, grid(nS), DT_THREADS, 0, c.s, nS,
+                   EdgeFeatGather{sSlot, c.mpEdgeF.p}, ReluEmitEdge{sSlot, ES(0)}, w + MP_WE0, w + MP_BE0);
+    if (nD) launch(denseTiledKernel<MPNN_EF, MPNN_H, EdgeFeatGather, ReluEmitEdge>, grid(nD), DT_THREADS, 0, c.s, nD,
+                   EdgeFeatGather{dSlot, c.mpEdgeFD.p}, ReluEmitEdge{dSlot, ED(0)}, w + MP_WE0, w + MP_BE0);
     for (int l = 0; l < MPNN_L; ++l) {
-        launch(edgeLayerKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const float*)ES(l), (const float*)H(l), w + mpWe(l), w + mpBe(l), ES(l + 1));
-        if (d.on)
-            launch(edgeLayerKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const float*)ED(l), (const float*)H(l), w + mpWe(l), w + mpBe(l),
-                   ED(l + 1));
+        if (nS) launch(denseTiledKernel<2 * MPNN_H, MPNN_H, EdgeLayerGather, ReluEmitEdge>, grid(nS), DT_THREADS, 0, c.s, nS,
+                       EdgeLayerGather{sSlot, sI, sJ, ES(l), H(l)}, ReluEmitEdge{sSlot, ES(l + 1)}, w + mpWe(l), w + mpBe(l));
+        if (nD) launch(denseTiledKernel<2 * MPNN_H, MPNN_H, EdgeLayerGather, ReluEmitEdge>, grid(nD), DT_THREADS, 0, c.s, nD,
+                       EdgeLayerGather{dSlot, dI, dJ, ED(l), H(l)}, ReluEmitEdge{dSlot, ED(l + 1)}, w + mpWe(l), w + mpBe(l));
         float* agg = c.mpAgg.p + (size_t)l * MPNN_H * nv;
-        launch(aggregateKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, col, (const int*)c.mpMirS.p, (const float*)ES(l + 1), d.rs,
-               d.re, d.col, (const int*)c.mpMirD.p, (const float*)ED(l + 1), (const int*)c.mpDeg.p, agg);
-        launch(nodeLayerKernel, blocksFor(nv), TB, 0, c.s, nv, (const float*)H(l), (const float*)agg, w + mpWh(l), w + mpBh(l), H(l + 1));
+        launch(aggregateKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, (const int*)c.colIdx.p, (const int*)c.mpMirS.p,
+               (const float*)ES(l + 1), d.rs, d.re, d.col, (const int*)c.mpMirD.p, (const float*)ED(l + 1), (const int*)c.mpDeg.p, agg);
+        launch(denseTiledKernel<2 * MPNN_H, MPNN_H, NodeLayerGather, ReluEmitNode>, grid(nv), DT_THREADS, 0, c.s, nv,
+               NodeLayerGather{H(l), agg}, ReluEmitNode{H(l + 1)}, w + mpWh(l), w + mpBh(l));
     }
-    launch(headEdgeKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const int*)c.mpMirS.p, (const float*)ES(MPNN_L), (const float*)c.mpEdgeF.p,
-           w, (const int*)c.btype.p, c.mpGS.p, 0);
-    launch(headDiagKernel, blocksFor(nv), TB, 0, c.s, nv, (const float*)H(MPNN_L), w, (const int*)c.diagSlot.p, (const int*)c.btype.p, c.mpGS.p,
-           c.mpHeadD.p);
-    if (d.on)
-        launch(headEdgeKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const int*)c.mpMirD.p, (const float*)ED(MPNN_L),
-               (const float*)c.mpEdgeFD.p, w, (const int*)c.btype.p, c.mpGD.p, 1);
+    // heads: contact diagonal slots carry no factor part
+    if (d.on) CIPC_CUDA(cudaMemsetAsync(c.mpGD.p, 0, sizeof(float) * 9 * (size_t)c.nDynB, c.s));
+    if (nS) launch(denseTiledKernel<MPNN_H + MPNN_EF, 9, HeadEdgeGather, HeadEdgeEmit>, grid(nS), DT_THREADS, 0, c.s, nS,
+                   HeadEdgeGather{sSlot, ES(MPNN_L), c.mpEdgeF.p}, HeadEdgeEmit{sSlot, sI, sJ, c.mpMirS.p, c.btype.p, c.mpGS.p}, w + MP_WO, w + MP_BO);
+    if (nD) launch(denseTiledKernel<MPNN_H + MPNN_EF, 9, HeadEdgeGather, HeadEdgeEmit>, grid(nD), DT_THREADS, 0, c.s, nD,
+                   HeadEdgeGather{dSlot, ED(MPNN_L), c.mpEdgeFD.p}, HeadEdgeEmit{dSlot, dI, dJ, c.mpMirD.p, c.btype.p, c.mpGD.p}, w + MP_WO, w + MP_BO);
+    launch(denseTiledKernel<MPNN_H, 6, NodeHiddenGather, HeadDiagEmit>, grid(nv), DT_THREADS, 0, c.s, nv, NodeHiddenGather{H(MPNN_L)},
+           HeadDiagEmit{c.diagSlot.p, c.btype.p, c.mpGS.p, c.mpHeadD.p}, w + MP_WD, w + MP_BD);
     CIPC_CUDA(cudaGetLastError());
     c.mpFactorReady = true;
 }
