@@ -314,7 +314,9 @@ def main():
     sampler.start()
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStart()
+    fb0 = sim.precond_stats()["fallbacks"]
     r = device_timed(sim, args.steps, flush, args.roofline_kernel, cipc, torch)
+    fb_timed = sim.precond_stats()["fallbacks"] - fb0
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStop()
     clocks = sampler.stop()
@@ -372,7 +374,8 @@ def main():
         if train:
             cfg["training"] = train
         if args.precond != "jacobi":
-            cfg["factor_fallbacks"] = sim.precond_stats()["fallbacks"]
+            cfg["factor_fallbacks_timed"] = fb_timed
+            cfg["factor_fallbacks_total"] = sim.precond_stats()["fallbacks"]
         if rp is not None:
             plain_v = args.steps / (rp["ms"] / 1000.0)
             cfg["plain_fp64_gpu"] = {"steps_per_s": plain_v, "ms_per_newton_iteration": rp["ms"] / max(1, rp["newton"]),
