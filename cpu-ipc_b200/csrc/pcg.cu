@@ -663,6 +663,12 @@ __host__ __device__ constexpr size_t rowCacheBytes(int sliceMax) {
            (ROWS_PER_BLOCK + 1) * sizeof(int);
 }
 
+// offset (16-byte aligned) of the per-row recurrence state after the cache
+template <class MT>
+__host__ __device__ constexpr size_t rowStateOffset(int sliceMax) {
+    return (rowCacheBytes<MT>(sliceMax) + 15) / 16 * 16;
+}
+
 template <class MT, class VT>
 __device__ RowCache<MT> loadRowCache(const PcgArgs<MT, VT>& a, unsigned char* smem) {
     RowCache<MT> rc;
@@ -781,27 +787,34 @@ __device__ __forceinline__ void jacobiRow(const double* Dinv, const VT* in, VT* 
 template <class MT, class VT, bool LEARNED, bool CACHED>
 __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     extern __shared__ __align__(16) unsigned char pipeSmem[];
+    // with block-Jacobi in a single-pass launch, the per-row recurrence
+    // vectors live in shared memory too: only m (gathered by neighbours), u
+    // at the start and x at the end touch global memory
+    constexpr bool SH = CACHED && !LEARNED;
     const unsigned nb = gridDim.x;
     unsigned ep = 0;
     const int nv = a.nv;
     const RowIter it;
     RowCache<MT> rc{};
     if (CACHED) rc = loadRowCache(a, pipeSmem);
+    VT* sv = SH ? reinterpret_cast<VT*>(pipeSmem + rowStateOffset<MT>(a.sliceMax)) : nullptr;
+    // own-row vector k (0 x, 1 r, 2 u, 3 w, 4 z, 5 q, 6 s, 7 p), component q
+    auto V = [&](int k, int row, int q) -> VT& {
+        if (SH) return sv[(k * ROWS_PER_BLOCK + (row - rc.row0)) * 3 + q];
+        VT* g = k == 0 ? a.x : k == 1 ? a.r : k == 2 ? a.u : k == 3 ? a.w : k == 4 ? a.z : k == 5 ? a.q : k == 6 ? a.s : a.p;
+        return g[3 * row + q];
+    };
     auto Ax = [&](int row, const VT* u, VT acc[3]) {
         if (CACHED) rowAxCached(a, rc, it, row, u, acc);
         else rowAx(a, it, row, u, acc);
     };
-    auto jac = [&](const VT* in, VT* out, int row) {
-        if (CACHED) {
-            // block-Jacobi inverse from the cache
-            const double* D = rc.dinv + 9 * (row - rc.row0);
-            double r0 = in[3 * row], r1 = in[3 * row + 1], r2 = in[3 * row + 2];
-            out[3 * row] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
-            out[3 * row + 1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
-            out[3 * row + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
-        } else {
-            jacobiRow(a.Dinv, in, out, row);
-        }
+    // out = Dinv_row in (block-Jacobi), in and out given per component
+    auto jac3 = [&](int row, const VT in[3], VT out[3]) {
+        const double* D = CACHED ? rc.dinv + 9 * (row - rc.row0) : a.Dinv + 9 * (size_t)row;
+        double r0 = in[0], r1 = in[1], r2 = in[2];
+        out[0] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
+        out[1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
+        out[2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
     };
     VT* sw = a.Ap;  // S w for the factor passes
     auto part = [&](int set, int k) { return a.pp + (size_t)(3 * set + k) * PIPE_PMAX; };
@@ -810,13 +823,18 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     for (int base = it.first; base < nv; base += it.stride) {
         int row = base + it.grp;
         if (row < nv && it.lane == 0) {
+            VT rv[3];
             for (int q = 0; q < 3; ++q) {
-                int i = 3 * row + q;
-                a.x[i] = VT(0); a.z[i] = VT(0); a.q[i] = VT(0); a.s[i] = VT(0); a.p[i] = VT(0);
-                a.r[i] = a.b[i];
-                rr += (double)a.r[i] * (double)a.r[i];
+                V(0, row, q) = VT(0); V(4, row, q) = VT(0); V(5, row, q) = VT(0); V(6, row, q) = VT(0); V(7, row, q) = VT(0);
+                rv[q] = a.b[3 * row + q];
+                V(1, row, q) = rv[q];
+                rr += (double)rv[q] * (double)rv[q];
             }
-            if (!LEARNED) jac((const VT*)a.r, a.u, row);
+            if (!LEARNED) {
+                VT uv[3];
+                jac3(row, rv, uv);
+                for (int q = 0; q < 3; ++q) { V(2, row, q) = uv[q]; a.u[3 * row + q] = uv[q]; }
+            }
         }
     }
     if (LEARNED && !factorPasses(a, it, (const VT*)a.r, sw, a.u, ep)) return;
@@ -829,12 +847,15 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         Ax(row, (const VT*)a.u, acc);
         if (row < nv && it.lane == 0) {
             for (int q = 0; q < 3; ++q) {
-                int i = 3 * row + q;
-                a.w[i] = acc[q];
-                g += (double)a.r[i] * (double)a.u[i];
-                dl += (double)acc[q] * (double)a.u[i];
+                V(3, row, q) = acc[q];
+                g += (double)V(1, row, q) * (double)V(2, row, q);
+                dl += (double)acc[q] * (double)V(2, row, q);
             }
-            if (!LEARNED) jac((const VT*)a.w, a.mA, row);
+            if (!LEARNED) {
+                VT mv[3];
+                jac3(row, acc, mv);
+                for (int q = 0; q < 3; ++q) a.mA[3 * row + q] = mv[q];
+            }
         }
     }
     blockReduce3(rr, g, dl);
@@ -862,22 +883,26 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
             Ax(row, mCur, acc);
             if (row < nv && it.lane == 0) {
                 for (int q = 0; q < 3; ++q) {
-                    int i = 3 * row + q;
-                    VT zv = acc[q] + bt * a.z[i];
-                    VT qv = __ldcg(mCur + i) + bt * a.q[i];
-                    VT sv = a.w[i] + bt * a.s[i];
-                    VT pv = a.u[i] + bt * a.p[i];
-                    a.z[i] = zv; a.q[i] = qv; a.s[i] = sv; a.p[i] = pv;
-                    a.x[i] += al * pv;
-                    VT rv = a.r[i] - al * sv;
-                    VT uv = a.u[i] - al * qv;
-                    VT wv = a.w[i] - al * zv;
-                    a.r[i] = rv; a.u[i] = uv; a.w[i] = wv;
+                    VT zv = acc[q] + bt * V(4, row, q);
+                    VT qv = __ldcg(mCur + 3 * row + q) + bt * V(5, row, q);
+                    VT sv2 = V(3, row, q) + bt * V(6, row, q);
+                    VT pv = V(2, row, q) + bt * V(7, row, q);
+                    V(4, row, q) = zv; V(5, row, q) = qv; V(6, row, q) = sv2; V(7, row, q) = pv;
+                    V(0, row, q) += al * pv;
+                    VT rv = V(1, row, q) - al * sv2;
+                    VT uv = V(2, row, q) - al * qv;
+                    VT wv = V(3, row, q) - al * zv;
+                    V(1, row, q) = rv; V(2, row, q) = uv; V(3, row, q) = wv;
                     lrr += (double)rv * (double)rv;
                     lg += (double)rv * (double)uv;
                     ld += (double)wv * (double)uv;
                 }
-                if (!LEARNED) jac((const VT*)a.w, mNext, row);
+                if (!LEARNED) {
+                    const VT wn[3] = {V(3, row, 0), V(3, row, 1), V(3, row, 2)};
+                    VT mv[3];
+                    jac3(row, wn, mv);
+                    for (int q = 0; q < 3; ++q) mNext[3 * row + q] = mv[q];
+                }
             }
         }
         const int set = (iter + 1) & 1;
@@ -893,6 +918,14 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         ++iter;
         if (rr < thr) { status = 1; break; }
         if (iter >= a.maxIter || !isfinite(rr)) { status = 2; break; }
+    }
+    if (SH) {
+        // the solution leaves shared memory
+        for (int base = it.first; base < nv; base += it.stride) {
+            int row = base + it.grp;
+            if (row < nv && it.lane == 0)
+                for (int q = 0; q < 3; ++q) a.x[3 * row + q] = V(0, row, q);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.scal[3] = rr;
@@ -1035,7 +1068,7 @@ static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool class
         // single-pass launch: each block owns ROWS_PER_BLOCK rows for the whole
         // solve and stages them in shared memory
         a.sliceMax = pcgSliceMax(c);
-        size_t smem = rowCacheBytes<MT>(a.sliceMax);
+        size_t smem = LEARNED ? rowCacheBytes<MT>(a.sliceMax) : rowStateOffset<MT>(a.sliceMax) + (size_t)8 * ROWS_PER_BLOCK * 3 * sizeof(VT);
         const void* fn = (const void*)pcgPipelinedKernel<MT, VT, LEARNED, true>;
         int maxOptin = 0, dev = 0;
         CIPC_CUDA(cudaGetDevice(&dev));
