@@ -253,7 +253,10 @@ __global__ void accumulateKernel(int n3, const float* d, double* x) {
 // splits in three (r and S r | t = G S r | z = S^T G^T t), four barriers per
 // iteration.  A group of GROUP lanes owns one block row in every phase, so a
 // row's x, r, p, Ap are only touched by their owner; z, S r and t are read by
-// neighbours through L2 (__ldcg) after a barrier.  Every block sums the
+// neighbours after a barrier.  Those reads are plain loads: the barrier's
+// acquire (then __syncthreads) orders them after the other blocks' writes
+// under the PTX memory model, and they may hit in L1, where the vertices
+// that neighbouring rows of one SM share are fetched from L2 once.  Every block sums the
 // per-block partials in the same order, so all blocks take the same branch and
 // results are reproducible.  The barrier spin is bounded: on timeout it sets
 // an error flag and the kernel returns.
@@ -441,13 +444,13 @@ template <class MT, class VT>
 __device__ __forceinline__ void rowSpmv(const PcgArgs<MT, VT>& a, int row, int lane, const VT* u, VT acc[3]) {
     for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
         int c = a.col[k];
-        VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+        VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
         blockMulAdd(a.val + (size_t)9 * k, xv, acc);
     }
     if (a.dRowS) {
         for (int k = a.dRowS[row] + lane; k < a.dRowE[row]; k += GROUP) {
             int c = a.dCol[k];
-            VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+            VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
             blockMulAdd(a.dVal + (size_t)9 * k, xv, acc);
         }
     }
@@ -460,7 +463,7 @@ __device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int
     for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
         int c = a.col[k];
         if (TR ? c < row : c > row) continue;
-        VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+        VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
         const float* B = a.gS + (size_t)9 * k;
         if (TR && c == row) {
             for (int q = 0; q < 3; ++q) acc[q] += (VT)B[q] * xv[0] + (VT)B[3 + q] * xv[1] + (VT)B[6 + q] * xv[2];
@@ -472,7 +475,7 @@ __device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int
         for (int k = a.dRowS[row] + lane; k < a.dRowE[row]; k += GROUP) {
             int c = a.dCol[k];
             if (TR ? c <= row : c >= row) continue;
-            VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+            VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
             blockMulAdd(a.gD + (size_t)9 * k, xv, acc);
         }
     }
@@ -775,7 +778,7 @@ __device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowC
         const int kb = rc.rp[lr] - rc.s0, ke = rc.rp[lr + 1] - rc.s0;
         for (int kk = kb + it.lane; kk < ke; kk += GROUP) {
             int c = rc.col[kk];
-            VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+            VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
             blockMulAdd(rc.val + (size_t)9 * kk, xv, acc);
         }
         const int ds = rc.drs[2 * lr], de = rc.drs[2 * lr + 1];
@@ -783,13 +786,13 @@ __device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowC
             for (int k = ds + it.lane; k < de; k += GROUP) {
                 int kk = k - rc.d0;
                 int c = rc.dcol[kk];
-                VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+                VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
                 blockMulAdd(rc.dval + (size_t)9 * kk, xv, acc);
             }
         } else {
             for (int k = ds + it.lane; k < de; k += GROUP) {
                 int c = a.dCol[k];
-                VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+                VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
                 blockMulAdd(a.dVal + (size_t)9 * k, xv, acc);
             }
         }
@@ -810,7 +813,7 @@ __device__ __forceinline__ void rowFactorCached(const PcgArgs<MT, VT>& a, const 
     for (int kk = kb + it.lane; kk < ke; kk += GROUP) {
         int c = rc.col[kk];
         if (TR ? c < row : c > row) continue;
-        VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+        VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
         const float* B = rc.gval ? rc.gval + (size_t)9 * kk : a.gS + (size_t)9 * (kk + rc.s0);
         if (TR && c == row) {
             for (int q = 0; q < 3; ++q) acc[q] += (VT)B[q] * xv[0] + (VT)B[3 + q] * xv[1] + (VT)B[6 + q] * xv[2];
@@ -823,7 +826,7 @@ __device__ __forceinline__ void rowFactorCached(const PcgArgs<MT, VT>& a, const 
         const bool cached = rc.d0 >= 0;
         int c = cached ? rc.dcol[k - rc.d0] : a.dCol[k];
         if (TR ? c <= row : c >= row) continue;
-        VT xv[3] = {__ldcg(u + 3 * c), __ldcg(u + 3 * c + 1), __ldcg(u + 3 * c + 2)};
+        VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
         blockMulAdd((cached && rc.dgval) ? rc.dgval + (size_t)9 * (k - rc.d0) : a.gD + (size_t)9 * k, xv, acc);
     }
 }
@@ -873,7 +876,7 @@ __device__ __forceinline__ void rowAx(const PcgArgs<MT, VT>& a, const RowIter& i
     groupReduce3(acc);
     if (row < a.nv && it.lane == 0) {
         const double* D = a.diagExtra + 9 * row;
-        VT uv[3] = {__ldcg(u + 3 * row), __ldcg(u + 3 * row + 1), __ldcg(u + 3 * row + 2)};
+        VT uv[3] = {u[3 * row], u[3 * row + 1], u[3 * row + 2]};
         for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)uv[0] + D[3 * q + 1] * (double)uv[1] + D[3 * q + 2] * (double)uv[2]);
     }
 }
@@ -1067,7 +1070,7 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
             VT acc[3] = {VT(0), VT(0), VT(0)};
             VT mo[3] = {VT(0), VT(0), VT(0)};  // m at the row itself
             if (row < nv && it.lane == 0)
-                for (int q = 0; q < 3; ++q) mo[q] = CACHED ? ownM[3 * (row - rc.row0) + q] : __ldcg(mCur + 3 * row + q);
+                for (int q = 0; q < 3; ++q) mo[q] = CACHED ? ownM[3 * (row - rc.row0) + q] : mCur[3 * row + q];
             Ax(row, mCur, mo, acc);
             if (row < nv && it.lane == 0) {
                 for (int q = 0; q < 3; ++q) {
