@@ -25,6 +25,10 @@ cube), so the timed steps are in contact like most of the configuration's
 the same frames.
 Multi-GPU: replicas only (one independent simulation per rank, weak scaling).
 
+--scene pile measures the pile configuration instead: 64 cubes of 0.2 m
+(12^3 cells, 6 tets per cell: 663,552 tets, 140,608 vertices) at seeded
+random rotations, dropped into a static open box, dt = 0.01 s.
+
 --impl reference times the reference's CPU path on the host cores.  The
 reference itself cannot be compiled here (Eigen, oneTBB, oneMKL and
 SuiteSparse are absent), so its FP64 restatement (oracle/) stands in.
@@ -51,7 +55,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scene", default="cloth_drape", choices=["cloth_drape", "pile"])
     ap.add_argument("--cloth", type=int, default=128)
+    ap.add_argument("--pile-cubes", type=int, default=64)
+    ap.add_argument("--pile-cells", type=int, default=12)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--precond", default="learned", choices=["jacobi", "learned", "fsai"])
     ap.add_argument("--settle-steps", type=int, default=40, help="untimed steps before warm-up: the cloth reaches the cube")
@@ -64,6 +71,31 @@ def parse():
                     help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
+
+
+def make_scene(args, cipc):
+    if args.scene == "pile":
+        return cipc.scene_pile(args.pile_cubes, args.pile_cells)
+    return cipc.scene_cloth_drape(args.cloth, 10)
+
+
+def workload(args, detail=False):
+    """Name (and with detail the description) of the measured workload."""
+    if args.scene == "pile":
+        n, c = args.pile_cubes, args.pile_cells
+        name = f"pile_{n}x{c}"
+        if detail:
+            name += (f": {n} cubes of 0.2 m ({c}^3 cells x 6 tets each, {n * 6 * c ** 3} tets, {n * (c + 1) ** 3} vertices) "
+                     "at seeded random rotations and positions in a 1.5 m box, dropped into a static open box; "
+                     "Neo-Hookean E ~ U[5e4, 5e5], nu=0.4, mu=0.2, dt=0.01, dhat=1e-3")
+        return name
+    name = f"cloth_drape_{args.cloth}"
+    if detail:
+        name += (f": {args.cloth}x{args.cloth}-vertex 1 m cloth ({2 * (args.cloth - 1) ** 2} tris, BW membrane E=1e4, "
+                 "quadratic bending k_b=1e-3, mu=0.3) 0.1 m above a fixed 0.5 m tet cube (10^3 cells x 6 tets), dt=0.005, dhat=1e-3")
+    else:
+        name += f" (cloth {args.cloth}x{args.cloth} + 10^3-cell tet cube)"
+    return name
 
 
 def dist_setup():
@@ -184,7 +216,7 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     import cipc
-    scene = cipc.scene_cloth_drape(args.cloth, 10)
+    scene = make_scene(args, cipc)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
@@ -202,7 +234,7 @@ def run_reference(args, world, rank):
     v = n / dt
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": n, "warmup": w,
             "ms_per_step": 1000 * dt / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": f"cloth_drape_{args.cloth} (cloth {args.cloth}x{args.cloth} + 10^3-cell tet cube)",
+            "data": "synthetic", "config": {"workload": workload(args),
                                             "solver": "FP64 CPU restatement of the reference pipeline, block-Jacobi PCG 1e-6"},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
                              "sample": f"{n} steps after {w} warm-up steps; the reference itself does not compile here"},
@@ -275,7 +307,7 @@ def main():
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
-    scene = cipc.scene_cloth_drape(args.cloth, 10)
+    scene = make_scene(args, cipc)
     learned = args.precond == "learned"
     sim = cipc.Simulator(scene, precision=args.precision, precond=args.precond)
     is_plain = args.precision == "fp64" and args.precond == "jacobi"
@@ -361,9 +393,7 @@ def main():
                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic("pcg"),
                     "algorithmic_bytes_per_launch": bytes_, "bytes_per_iteration": per_it, "launches": r["nprof"],
                     "mean_launch_us": 1000 * avg_ms, "share_of_step_time": r["prof_ms"] / r["ms"]}
-        cfg = {"workload": f"cloth_drape_{args.cloth}: {args.cloth}x{args.cloth}-vertex 1 m cloth "
-                           f"({2 * (args.cloth - 1) ** 2} tris, BW membrane E=1e4, quadratic bending k_b=1e-3, mu=0.3) "
-                           "0.1 m above a fixed 0.5 m tet cube (10^3 cells x 6 tets), dt=0.005, dhat=1e-3",
+        cfg = {"workload": workload(args, detail=True),
                "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
                "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
                "ms_per_newton_iteration": max_ms / max(1, r["newton"]),

@@ -495,14 +495,28 @@ def _rand_rot(rng):
 
 
 def scene_pile(n_cubes=64, cells=12, seed=0, box=1.5, newton_thr=1e-2):
-    """Cubes of 0.2 m at seeded random rotations/positions in a box, dropped into a static open box (5 quads)."""
+    """Cubes of 0.2 m at seeded random rotations, dropped into a static open
+    box (5 quads).  Positions are seeded uniform jitters of the points of a
+    k x k x k lattice that fills the box (k = ceil(n_cubes^(1/3)); n_cubes of
+    its cells, chosen at random): every cube's bounding sphere stays inside
+    its own cell, so no two cubes touch whatever their rotations.  (Rejection
+    sampling of free positions cannot place 64 such spheres in a 1.5 m box:
+    that packing is past the random-sequential-addition limit.)"""
     rng = np.random.default_rng(seed)
     r = 0.1 * math.sqrt(3) + 1e-3
+    k = 1
+    while k ** 3 < n_cubes:
+        k += 1
+    cell = box / k
+    slack = 0.5 * cell - r
+    if slack < 0:
+        raise ValueError(f"{n_cubes} cubes of 0.2 m do not fit a {box} m box")
+    base = np.array([-0.5 * box, -1.0 + 0.05, -0.5 * box])
+    slots = rng.permutation(k ** 3)[:n_cubes]
     centers = []
-    while len(centers) < n_cubes:
-        c = rng.uniform([-0.5 * box + r, -1.0 + 0.05 + r, -0.5 * box + r], [0.5 * box - r, -1.0 + 0.05 + box - r, 0.5 * box - r])
-        if all(np.linalg.norm(c - o) > 2 * r for o in centers):
-            centers.append(c)
+    for sl in slots:
+        ijk = np.array([sl % k, (sl // k) % k, sl // (k * k)], float)
+        centers.append(base + (ijk + 0.5) * cell + rng.uniform(-slack, slack, 3))
     xs, ts, te = [], [], []
     off = 0
     Es = rng.uniform(5e4, 5e5, n_cubes)
