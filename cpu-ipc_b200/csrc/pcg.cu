@@ -769,10 +769,11 @@ __device__ RowCache<MT> loadRowCache(const PcgArgs<MT, VT>& a, unsigned char* sm
     return rc;
 }
 
-// acc = (A u)_row from the cache; own holds u at the row itself (lane 0)
+// acc = (A u)_row without the diagonal extras, from the cache; every lane of
+// the row's group gets the sum
 template <class MT, class VT>
 __device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowCache<MT>& rc, const RowIter& it, int row, const VT* u,
-                                            const VT own[3], VT acc[3]) {
+                                            VT acc[3]) {
     const int lr = row - rc.row0;
     if (row < a.nv) {
         const int kb = rc.rp[lr] - rc.s0, ke = rc.rp[lr + 1] - rc.s0;
@@ -798,10 +799,6 @@ __device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowC
         }
     }
     groupReduce3(acc);
-    if (row < a.nv && it.lane == 0) {
-        const double* D = rc.dex + 9 * lr;
-        for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)own[0] + D[3 * q + 1] * (double)own[1] + D[3 * q + 2] * (double)own[2]);
-    }
 }
 
 // (G u)_row (TR false) or (G^T u)_row (TR true) from the cache, as rowFactor
@@ -846,8 +843,9 @@ __device__ bool factorCachedPasses(const PcgArgs<MT, VT>& a, const RowCache<MT>&
         VT acc[3] = {VT(0), VT(0), VT(0)};
         if (active) rowFactorCached<false>(a, rc, it, row, tmp, acc);
         groupReduce3(acc);
-        if (active && it.lane == 0)
-            for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
+        // lanes 0, 1, 2 of the group store components 0, 1, 2
+        const int q = it.lane;
+        if (active && q < 3) a.t[3 * row + q] = q == 0 ? acc[0] : (q == 1 ? acc[1] : acc[2]);
     }
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
@@ -856,29 +854,25 @@ __device__ bool factorCachedPasses(const PcgArgs<MT, VT>& a, const RowCache<MT>&
         VT acc[3] = {VT(0), VT(0), VT(0)};
         if (active) rowFactorCached<true>(a, rc, it, row, (const VT*)a.t, acc);
         groupReduce3(acc);
-        if (active && it.lane == 0) {
+        const int q = it.lane;
+        if (active && q < 3) {
+            // component q of S^T y (S lower triangular)
             const int lr = row - rc.row0;
             const double* S = rc.blk + 9 * lr;
-            double y0 = acc[0], y1 = acc[1], y2 = acc[2];
-            VT o[3] = {(VT)(S[0] * y0 + S[3] * y1 + S[6] * y2), (VT)(S[4] * y1 + S[7] * y2), (VT)(S[8] * y2)};
-            for (int q = 0; q < 3; ++q) {
-                outG[3 * row + q] = o[q];
-                own[3 * lr + q] = o[q];
-            }
+            const double y0 = acc[0], y1 = acc[1], y2 = acc[2];
+            const VT o = (VT)(q == 0 ? S[0] * y0 + S[3] * y1 + S[6] * y2 : (q == 1 ? S[4] * y1 + S[7] * y2 : S[8] * y2));
+            outG[3 * row + q] = o;
+            own[3 * lr + q] = o;
         }
     }
     return true;
 }
 
+// acc = (A u)_row without the diagonal extras; every lane of the group gets the sum
 template <class MT, class VT>
 __device__ __forceinline__ void rowAx(const PcgArgs<MT, VT>& a, const RowIter& it, int row, const VT* u, VT acc[3]) {
     if (row < a.nv) rowSpmv(a, row, it.lane, u, acc);
     groupReduce3(acc);
-    if (row < a.nv && it.lane == 0) {
-        const double* D = a.diagExtra + 9 * row;
-        VT uv[3] = {u[3 * row], u[3 * row + 1], u[3 * row + 2]};
-        for (int q = 0; q < 3; ++q) acc[q] += (VT)(D[3 * q] * (double)uv[0] + D[3 * q + 1] * (double)uv[1] + D[3 * q + 2] * (double)uv[2]);
-    }
 }
 
 // out = M^-1 in for the factor: S in -> tmp (own rows), barrier, t = G tmp,
@@ -939,11 +933,13 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     // In a single-pass launch (CACHED) the block's matrix rows and its rows'
     // recurrence vectors live in shared memory: only the gathered vectors
     // (u once; m, and with a factor S w and t, every iteration), the partial
-    // sums and the solution at the end touch global memory.
+    // sums and the solution at the end touch global memory.  Lanes 0, 1, 2
+    // of a row's group update components 0, 1, 2 of the row's vectors.
     const unsigned nb = gridDim.x;
     unsigned ep = 0;
     const int nv = a.nv;
     const RowIter it;
+    const int q = it.lane;  // the component this lane updates (q < 3)
     RowCache<MT> rc{};
     VT* sv = nullptr;
     if (CACHED) {
@@ -951,55 +947,70 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         const bool cacheG = LEARNED && a.cacheG != 0;
         sv = reinterpret_cast<VT*>(pipeSmem + smemLayout(a.sliceMax, a.dynCap, cacheG, (int)sizeof(MT), (int)sizeof(VT)).state);
     }
-    // own-row vector k (0 x, 1 r, 2 u, 3 w, 4 z, 5 q, 6 s, 7 p), component q
-    auto V = [&](int k, int row, int q) -> VT& {
+    // component q of own-row vector k (0 x, 1 r, 2 u, 3 w, 4 z, 5 q, 6 s, 7 p)
+    auto V = [&](int k, int row) -> VT& {
         if (CACHED) return sv[(k * ROWS_PER_BLOCK + (row - rc.row0)) * 3 + q];
         VT* g = k == 0 ? a.x : k == 1 ? a.r : k == 2 ? a.u : k == 3 ? a.w : k == 4 ? a.z : k == 5 ? a.q : k == 6 ? a.s : a.p;
         return g[3 * row + q];
     };
     VT* const ownM = CACHED ? sv + 8 * ROWS_PER_BLOCK * 3 : nullptr;  // the rows' own m (shared copy)
     VT* const ownU = CACHED ? sv + 2 * ROWS_PER_BLOCK * 3 : nullptr;
-    auto Ax = [&](int row, const VT* u, const VT own[3], VT acc[3]) {
-        if (CACHED) rowAxCached(a, rc, it, row, u, own, acc);
+    auto Ax = [&](int row, const VT* u, VT acc[3]) {
+        if (CACHED) rowAxCached(a, rc, it, row, u, acc);
         else rowAx(a, it, row, u, acc);
     };
-    // out = Dinv_row in (block-Jacobi)
-    auto jac3 = [&](int row, const VT in[3], VT out[3]) {
-        const double* D = CACHED ? rc.blk + 9 * (row - rc.row0) : a.Dinv + 9 * (size_t)row;
-        double r0 = in[0], r1 = in[1], r2 = in[2];
-        out[0] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
-        out[1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
-        out[2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
+    auto pick = [&](const VT v[3]) { return q == 0 ? v[0] : (q == 1 ? v[1] : v[2]); };
+    // component q of D v for a row's 3x3 block D (row-major), v given whole
+    auto rowDot = [&](const double* D, const VT v[3]) {
+        return (VT)(D[3 * q] * (double)v[0] + D[3 * q + 1] * (double)v[1] + D[3 * q + 2] * (double)v[2]);
+    };
+    auto dexRow = [&](int row) { return CACHED ? rc.dex + 9 * (row - rc.row0) : a.diagExtra + 9 * (size_t)row; };
+    auto blkRow = [&](int row) { return CACHED ? rc.blk + 9 * (row - rc.row0) : a.Dinv + 9 * (size_t)row; };
+    // the group's three components of v (held by lanes 0, 1, 2); every lane calls
+    auto share3 = [&](VT v, VT out[3]) {
+        out[0] = __shfl_sync(0xffffffffu, v, 0, GROUP);
+        out[1] = __shfl_sync(0xffffffffu, v, 1, GROUP);
+        out[2] = __shfl_sync(0xffffffffu, v, 2, GROUP);
     };
     VT* sw = a.Ap;  // S w, gathered by the factor's first pass
-    // sw_row = S_row in (the factor's scaling, lower triangular; cached path)
-    auto scale3 = [&](int row, const VT in[3]) {
-        const double* S = rc.blk + 9 * (row - rc.row0);
-        double r0 = in[0], r1 = in[1], r2 = in[2];
-        sw[3 * row] = (VT)(S[0] * r0);
-        sw[3 * row + 1] = (VT)(S[3] * r0 + S[4] * r1);
-        sw[3 * row + 2] = (VT)(S[6] * r0 + S[7] * r1 + S[8] * r2);
+    // the row's M-related output from the group's three components of v:
+    // block-Jacobi m = Dinv v into mOut (and the shared copy), or with a
+    // factor (cached path) S v into sw; lanes q < 3 of active rows store
+    auto precondRow = [&](int row, bool active, const VT v[3], VT* mOut) {
+        if (!active || q >= 3) return;
+        if (!LEARNED) {
+            const VT mq = rowDot(blkRow(row), v);
+            mOut[3 * row + q] = mq;
+            if (CACHED) ownM[3 * (row - rc.row0) + q] = mq;
+        } else if (CACHED) {
+            const double* S = rc.blk + 9 * (row - rc.row0);  // lower triangular
+            const double v0 = v[0], v1 = v[1], v2 = v[2];
+            sw[3 * row + q] = (VT)(q == 0 ? S[0] * v0 : (q == 1 ? S[3] * v0 + S[4] * v1 : S[6] * v0 + S[7] * v1 + S[8] * v2));
+        }
     };
     auto part = [&](int set, int k) { return a.pp + (size_t)(3 * set + k) * PIPE_PMAX; };
     // x = 0, r = b, u = M r; the recurrence vectors start at 0
     double rr = 0;
     for (int base = it.first; base < nv; base += it.stride) {
-        int row = base + it.grp;
-        if (row < nv && it.lane == 0) {
-            VT rv[3];
-            for (int q = 0; q < 3; ++q) {
-                V(0, row, q) = VT(0); V(4, row, q) = VT(0); V(5, row, q) = VT(0); V(6, row, q) = VT(0); V(7, row, q) = VT(0);
-                rv[q] = a.b[3 * row + q];
-                V(1, row, q) = rv[q];
-                rr += (double)rv[q] * (double)rv[q];
+        const int row = base + it.grp;
+        const bool active = row < nv;
+        VT rq = VT(0);
+        if (active && q < 3) {
+            V(0, row) = VT(0); V(4, row) = VT(0); V(5, row) = VT(0); V(6, row) = VT(0); V(7, row) = VT(0);
+            rq = a.b[3 * row + q];
+            V(1, row) = rq;
+            rr += (double)rq * (double)rq;
+        }
+        VT rv[3];
+        share3(rq, rv);
+        if (!LEARNED) {
+            if (active && q < 3) {
+                const VT uq = rowDot(blkRow(row), rv);
+                V(2, row) = uq;
+                a.u[3 * row + q] = uq;
             }
-            if (!LEARNED) {
-                VT uv[3];
-                jac3(row, rv, uv);
-                for (int q = 0; q < 3; ++q) { V(2, row, q) = uv[q]; a.u[3 * row + q] = uv[q]; }
-            } else if (CACHED) {
-                scale3(row, rv);
-            }
+        } else {
+            precondRow(row, active, rv, nullptr);
         }
     }
     if (LEARNED) {
@@ -1013,29 +1024,23 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     // w = A u, m = M w, gamma = (r,u), delta = (w,u)
     double g = 0, dl = 0;
     for (int base = it.first; base < nv; base += it.stride) {
-        int row = base + it.grp;
+        const int row = base + it.grp;
+        const bool active = row < nv;
         VT acc[3] = {VT(0), VT(0), VT(0)};
-        VT own[3] = {VT(0), VT(0), VT(0)};
-        if (CACHED && row < nv && it.lane == 0)
-            for (int q = 0; q < 3; ++q) own[q] = V(2, row, q);
-        Ax(row, (const VT*)a.u, own, acc);
-        if (row < nv && it.lane == 0) {
-            for (int q = 0; q < 3; ++q) {
-                V(3, row, q) = acc[q];
-                g += (double)V(1, row, q) * (double)V(2, row, q);
-                dl += (double)acc[q] * (double)V(2, row, q);
-            }
-            if (!LEARNED) {
-                VT mv[3];
-                jac3(row, acc, mv);
-                for (int q = 0; q < 3; ++q) {
-                    a.mA[3 * row + q] = mv[q];
-                    if (CACHED) ownM[3 * (row - rc.row0) + q] = mv[q];
-                }
-            } else if (CACHED) {
-                scale3(row, acc);
-            }
+        Ax(row, (const VT*)a.u, acc);
+        VT wq = VT(0);
+        if (active && q < 3) {
+            const VT* uOwn = CACHED ? ownU + 3 * (row - rc.row0) : a.u + 3 * row;
+            const VT uo[3] = {uOwn[0], uOwn[1], uOwn[2]};
+            wq = pick(acc) + rowDot(dexRow(row), uo);
+            V(3, row) = wq;
+            const VT uq = V(2, row);
+            g += (double)V(1, row) * (double)uq;
+            dl += (double)wq * (double)uq;
         }
+        VT wv[3];
+        share3(wq, wv);
+        precondRow(row, active, wv, a.mA);
     }
     blockReduce3(rr, g, dl);
     if (threadIdx.x == 0) { part(0, 0)[blockIdx.x] = rr; part(0, 1)[blockIdx.x] = g; part(0, 2)[blockIdx.x] = dl; }
@@ -1066,40 +1071,31 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         const VT bt = (VT)beta, al = (VT)alpha;
         double lrr = 0, lg = 0, ld = 0;
         for (int base = it.first; base < nv; base += it.stride) {
-            int row = base + it.grp;
+            const int row = base + it.grp;
+            const bool active = row < nv;
             VT acc[3] = {VT(0), VT(0), VT(0)};
-            VT mo[3] = {VT(0), VT(0), VT(0)};  // m at the row itself
-            if (row < nv && it.lane == 0)
-                for (int q = 0; q < 3; ++q) mo[q] = CACHED ? ownM[3 * (row - rc.row0) + q] : mCur[3 * row + q];
-            Ax(row, mCur, mo, acc);
-            if (row < nv && it.lane == 0) {
-                for (int q = 0; q < 3; ++q) {
-                    VT zv = acc[q] + bt * V(4, row, q);
-                    VT qv = mo[q] + bt * V(5, row, q);
-                    VT sv2 = V(3, row, q) + bt * V(6, row, q);
-                    VT pv = V(2, row, q) + bt * V(7, row, q);
-                    V(4, row, q) = zv; V(5, row, q) = qv; V(6, row, q) = sv2; V(7, row, q) = pv;
-                    V(0, row, q) += al * pv;
-                    VT rv = V(1, row, q) - al * sv2;
-                    VT uv = V(2, row, q) - al * qv;
-                    VT wv = V(3, row, q) - al * zv;
-                    V(1, row, q) = rv; V(2, row, q) = uv; V(3, row, q) = wv;
-                    lrr += (double)rv * (double)rv;
-                    lg += (double)rv * (double)uv;
-                    ld += (double)wv * (double)uv;
-                }
-                const VT wn[3] = {V(3, row, 0), V(3, row, 1), V(3, row, 2)};
-                if (!LEARNED) {
-                    VT mv[3];
-                    jac3(row, wn, mv);
-                    for (int q = 0; q < 3; ++q) {
-                        mNext[3 * row + q] = mv[q];
-                        if (CACHED) ownM[3 * (row - rc.row0) + q] = mv[q];
-                    }
-                } else if (CACHED) {
-                    scale3(row, wn);
-                }
+            Ax(row, mCur, acc);
+            VT wq = VT(0);
+            if (active && q < 3) {
+                const VT* mOwn = CACHED ? ownM + 3 * (row - rc.row0) : mCur + 3 * row;
+                const VT mo[3] = {mOwn[0], mOwn[1], mOwn[2]};
+                const VT zv = pick(acc) + rowDot(dexRow(row), mo) + bt * V(4, row);
+                const VT qv = pick(mo) + bt * V(5, row);
+                const VT sq = V(3, row) + bt * V(6, row);
+                const VT pv = V(2, row) + bt * V(7, row);
+                V(4, row) = zv; V(5, row) = qv; V(6, row) = sq; V(7, row) = pv;
+                V(0, row) += al * pv;
+                const VT rv = V(1, row) - al * sq;
+                const VT uv = V(2, row) - al * qv;
+                wq = V(3, row) - al * zv;
+                V(1, row) = rv; V(2, row) = uv; V(3, row) = wq;
+                lrr += (double)rv * (double)rv;
+                lg += (double)rv * (double)uv;
+                ld += (double)wq * (double)uv;
             }
+            VT wv[3];
+            share3(wq, wv);
+            precondRow(row, active, wv, mNext);
         }
         const int set = (iter + 1) & 1;
         blockReduce3(lrr, lg, ld);
@@ -1125,9 +1121,8 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     if (CACHED) {
         // the solution leaves shared memory
         for (int base = it.first; base < nv; base += it.stride) {
-            int row = base + it.grp;
-            if (row < nv && it.lane == 0)
-                for (int q = 0; q < 3; ++q) a.x[3 * row + q] = V(0, row, q);
+            const int row = base + it.grp;
+            if (row < nv && q < 3) a.x[3 * row + q] = V(0, row);
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
