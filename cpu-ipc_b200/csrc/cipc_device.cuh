@@ -15,6 +15,7 @@ enum CipcStatusBits {
     CIPC_ST_CAPACITY = 4,
     CIPC_ST_CCD_CAP = 8,
     CIPC_ST_JACOBI_CAP = 16,
+    CIPC_ST_TC_TIMEOUT = 32,
 };
 
 template <class T>

@@ -27,6 +27,7 @@
 #include "cipc_device.cuh"
 #include "cipc_internal.h"
 #include "mpnn.h"
+#include "dense_tc.cuh"
 
 #include <cuda_bf16.h>
 #include <cub/cub.cuh>
@@ -299,12 +300,17 @@ struct EdgeLayerGather {  // [e_l ; h_i + h_j]
         i -= MPNN_H;
         return h[(size_t)MPNN_H * ei[k] + i] + h[(size_t)MPNN_H * ej[k] + i];
     }
+    // inputs lane and MPNN_H + lane (tensor-core layer)
+    __device__ float2 pair(int k, int lane) const {
+        return make_float2(e[(size_t)MPNN_H * slot[k] + lane], h[(size_t)MPNN_H * ei[k] + lane] + h[(size_t)MPNN_H * ej[k] + lane]);
+    }
 };
 struct NodeLayerGather {  // [h ; agg]
     const float *h, *agg;
     __device__ float operator()(int v, int i) const {
         return i < MPNN_H ? h[(size_t)MPNN_H * v + i] : agg[(size_t)MPNN_H * v + i - MPNN_H];
     }
+    __device__ float2 pair(int v, int lane) const { return make_float2(h[(size_t)MPNN_H * v + lane], agg[(size_t)MPNN_H * v + lane]); }
 };
 struct HeadEdgeGather {  // [e_L ; g]
     const int* slot;
@@ -318,14 +324,21 @@ struct NodeHiddenGather {
     __device__ float operator()(int v, int i) const { return h[(size_t)MPNN_H * v + i]; }
 };
 
+__device__ __forceinline__ void reluStore32(float* dst, const float v[32]) {
+    float4* p = reinterpret_cast<float4*>(dst);
+#pragma unroll
+    for (int o = 0; o < 8; ++o) p[o] = make_float4(relu(v[4 * o]), relu(v[4 * o + 1]), relu(v[4 * o + 2]), relu(v[4 * o + 3]));
+}
 struct ReluEmitNode {
     float* out;
     __device__ void operator()(int v, int o, float a) const { out[(size_t)MPNN_H * v + o] = relu(a); }
+    __device__ void emit32(int v, const float a[32]) const { reluStore32(out + (size_t)MPNN_H * v, a); }
 };
 struct ReluEmitEdge {
     const int* slot;
     float* out;
     __device__ void operator()(int k, int o, float a) const { out[(size_t)MPNN_H * slot[k] + o] = relu(a); }
+    __device__ void emit32(int k, const float a[32]) const { reluStore32(out + (size_t)MPNN_H * slot[k], a); }
 };
 // G_ij into the lower slot and G_ij^T into its mirror; no block touches a
 // Dirichlet vertex
@@ -510,8 +523,10 @@ constexpr int WG_THREADS = 256;
 constexpr int WG_GRID = 296;     // CTAs of the split-K reduction (2 per SM)
 
 // X = [X1 (ld1, IN1 columns) ; X2 (ld2, IN2 columns)] per item; mask may be
-// null (all items active).  partial[cta][OUT*(IN1+IN2) + OUT].
-template <int OUT, int IN1, int IN2>
+// null (all items active).  partial[cta][OUT*(IN1+IN2) + OUT].  RX: the
+// layer's forward multiplies BF16-rounded inputs (tensor-core layers), so
+// the weight gradient uses the same rounded X.
+template <int OUT, int IN1, int IN2, bool RX = false>
 __global__ void __launch_bounds__(WG_THREADS) weightGradKernel(int items, const float* D, const float* X1, const float* X2, const unsigned char* mask,
                                                                float* partial) {
     constexpr int IN = IN1 + IN2;
@@ -533,7 +548,7 @@ __global__ void __launch_bounds__(WG_THREADS) weightGradKernel(int items, const 
             bool on = it < items && (!mask || mask[it]);
             float v = 0.f;
             if (on) v = i < IN1 ? X1[(size_t)it * IN1 + i] : X2[(size_t)it * IN2 + (i - IN1)];
-            sX[r][i] = v;
+            sX[r][i] = RX ? __bfloat162float(__float2bfloat16_rn(v)) : v;
         }
         __syncthreads();
         for (int q = 0; q < PER; ++q) {
@@ -861,6 +876,9 @@ void mpnnPrepare(Ctx& c, bool features) {
     else prepareT<double>(c, c.valD.p, c.dynBD.p, features);
 }
 
+static_assert(mpWe(0) % 8 == 0 && mpWh(0) % 8 == 0 && MP_LAYER % 8 == 0,
+              "tensor-core layer weights start on 16-byte boundaries");
+
 void mpnnForward(Ctx& c) {
     if (!c.mpReady) throw InvalidArgument("no network weights set");
     int nv = c.nv;
@@ -888,16 +906,18 @@ void mpnnForward(Ctx& c) {
                    EdgeFeatGather{sSlot, c.mpEdgeF.p}, ReluEmitEdge{sSlot, ES(0)}, w + MP_WE0, w + MP_BE0);
     if (nD) launch(denseTiledKernel<MPNN_EF, MPNN_H, EdgeFeatGather, ReluEmitEdge>, grid(nD), DT_THREADS, 0, c.s, nD,
                    EdgeFeatGather{dSlot, c.mpEdgeFD.p}, ReluEmitEdge{dSlot, ED(0)}, w + MP_WE0, w + MP_BE0);
+    // the 64 -> 32 message-passing layers run on the tensor cores
+    auto tcGrid = [](int n) { return std::max(1, std::min((n + tc::M - 1) / tc::M, 148 * 4)); };
     for (int l = 0; l < MPNN_L; ++l) {
-        if (nS) launch(denseTiledKernel<2 * MPNN_H, MPNN_H, EdgeLayerGather, ReluEmitEdge>, grid(nS), DT_THREADS, 0, c.s, nS,
-                       EdgeLayerGather{sSlot, sI, sJ, ES(l), H(l)}, ReluEmitEdge{sSlot, ES(l + 1)}, w + mpWe(l), w + mpBe(l));
-        if (nD) launch(denseTiledKernel<2 * MPNN_H, MPNN_H, EdgeLayerGather, ReluEmitEdge>, grid(nD), DT_THREADS, 0, c.s, nD,
-                       EdgeLayerGather{dSlot, dI, dJ, ED(l), H(l)}, ReluEmitEdge{dSlot, ED(l + 1)}, w + mpWe(l), w + mpBe(l));
+        if (nS) launch(tc::denseTcKernel<EdgeLayerGather, ReluEmitEdge>, tcGrid(nS), tc::THREADS, 0, c.s, nS, EdgeLayerGather{sSlot, sI, sJ, ES(l), H(l)},
+                       ReluEmitEdge{sSlot, ES(l + 1)}, w + mpWe(l), w + mpBe(l), c.status.p, (int)CIPC_ST_TC_TIMEOUT);
+        if (nD) launch(tc::denseTcKernel<EdgeLayerGather, ReluEmitEdge>, tcGrid(nD), tc::THREADS, 0, c.s, nD, EdgeLayerGather{dSlot, dI, dJ, ED(l), H(l)},
+                       ReluEmitEdge{dSlot, ED(l + 1)}, w + mpWe(l), w + mpBe(l), c.status.p, (int)CIPC_ST_TC_TIMEOUT);
         float* agg = c.mpAgg.p + (size_t)l * MPNN_H * nv;
         launch(aggregateKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, (const int*)c.colIdx.p, (const int*)c.mpMirS.p,
                (const float*)ES(l + 1), d.rs, d.re, d.col, (const int*)c.mpMirD.p, (const float*)ED(l + 1), (const int*)c.mpDeg.p, agg);
-        launch(denseTiledKernel<2 * MPNN_H, MPNN_H, NodeLayerGather, ReluEmitNode>, grid(nv), DT_THREADS, 0, c.s, nv,
-               NodeLayerGather{H(l), agg}, ReluEmitNode{H(l + 1)}, w + mpWh(l), w + mpBh(l));
+        launch(tc::denseTcKernel<NodeLayerGather, ReluEmitNode>, tcGrid(nv), tc::THREADS, 0, c.s, nv, NodeLayerGather{H(l), agg}, ReluEmitNode{H(l + 1)},
+               w + mpWh(l), w + mpBh(l), c.status.p, (int)CIPC_ST_TC_TIMEOUT);
     }
     // heads: contact diagonal slots carry no factor part
     if (d.on) CIPC_CUDA(cudaMemsetAsync(c.mpGD.p, 0, sizeof(float) * 9 * (size_t)c.nDynB, c.s));
@@ -1019,17 +1039,17 @@ static double lossT(Ctx& c, const MT* val, const MT* dval, int nprobes, const fl
     for (int l = MPNN_L - 1; l >= 0; --l) {
         const float* agg = c.mpAgg.p + (size_t)l * MPNN_H * nv;
         launch(nodeLayerBackKernel, blocksFor(nv), TB, 0, c.s, nv, (const float*)H(l + 1), (const float*)DH(l + 1), wb + mpWh(l), BD, DH(l), c.mpDAgg.p);
-        wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H>, MPNN_H, 2 * MPNN_H, nv, (const float*)H(l), agg, (const unsigned char*)nullptr, mpWh(l), mpBh(l));
+        wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H, true>, MPNN_H, 2 * MPNN_H, nv, (const float*)H(l), agg, (const unsigned char*)nullptr, mpWh(l), mpBh(l));
         launch(aggBackKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const float*)c.mpDAgg.p, (const int*)c.mpDeg.p, DES(l + 1));
         if (d.on) launch(aggBackKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const float*)c.mpDAgg.p, (const int*)c.mpDeg.p, DED(l + 1));
         launch(edgeLayerBackKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const float*)H(l), (const float*)ES(l + 1), (const float*)DES(l + 1),
                wb + mpWe(l), BD, BX, DES(l), c.mpDS.p);
-        wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H>, MPNN_H, 2 * MPNN_H, c.nnzb, (const float*)ES(l), (const float*)BX,
+        wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H, true>, MPNN_H, 2 * MPNN_H, c.nnzb, (const float*)ES(l), (const float*)BX,
               (const unsigned char*)c.mpLowS.p, mpWe(l), mpBe(l));
         if (d.on) {
             launch(edgeLayerBackKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const float*)H(l), (const float*)ED(l + 1),
                    (const float*)DED(l + 1), wb + mpWe(l), BD, BX, DED(l), c.mpDSD.p);
-            wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H>, MPNN_H, 2 * MPNN_H, nd, (const float*)ED(l), (const float*)BX,
+            wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H, true>, MPNN_H, 2 * MPNN_H, nd, (const float*)ED(l), (const float*)BX,
                   (const unsigned char*)c.mpLowD.p, mpWe(l), mpBe(l));
         }
         launch(dsGatherKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, col, (const int*)c.mpMirS.p, (const float*)c.mpDS.p, d.rs, d.re,

@@ -89,6 +89,7 @@ void checkStatus(Ctx& c, const char* stage) {
         if (st & CIPC_ST_CAPACITY) msg += " candidate buffer capacity exceeded;";
         if (st & CIPC_ST_CCD_CAP) msg += " CCD iteration cap;";
         if (st & CIPC_ST_JACOBI_CAP) msg += " eigen-solver sweep cap;";
+        if (st & CIPC_ST_TC_TIMEOUT) msg += " tensor-core completion wait timed out;";
         throw std::runtime_error(msg);
     }
 }

@@ -19,9 +19,11 @@ of the static and of the contact pattern (a pair present in both gives two
 edges).  Network (width H=32, 3 layers):
     h0 = relu(Wn0 f + bn0)            f: 6 node features
     e0 = relu(We0 g + be0)            g: the 9 entries of Â_ij
-    e_{l+1} = relu(We_l [e_l ; h_l[i] + h_l[j]] + be_l)
+    e_{l+1} = relu(We_l bf16([e_l ; h_l[i] + h_l[j]]) + be_l)
     a_i = mean of e_{l+1} over edges incident to i
-    h_{l+1} = relu(Wh_l [h_l ; a] + bh_l)
+    h_{l+1} = relu(Wh_l bf16([h_l ; a]) + bh_l)
+(the message-passing layers run on the GPU's tensor cores with BF16 operands;
+bf16() rounds to nearest even, and the backward treats it as the identity)
 Heads:
     G_ii = lower triangle, diagonal softplus(o[0:3]), o = Wd h_L + bd,
            entries (1,0),(2,0),(2,1) = o[3],o[4],o[5]
@@ -275,13 +277,13 @@ def forward(sysm, w):
     e = _relu(g @ P["We0"].T + P["be0"])
     hs, es, aggs = [h], [e], []
     for l in range(NL):
-        x = np.concatenate([e, h[ei] + h[ej]], axis=1)
+        x = bf16(np.concatenate([e, h[ei] + h[ej]], axis=1))  # tensor-core layer: BF16 inputs
         e = _relu(x @ P["We", l].T + P["be", l])
         a = np.zeros((sysm.nv, H))
         np.add.at(a, ei, e)
         np.add.at(a, ej, e)
         a = a / np.maximum(sysm.deg, 1)[:, None] * (sysm.deg > 0)[:, None]
-        h = _relu(np.concatenate([h, a], axis=1) @ P["Wh", l].T + P["bh", l])
+        h = _relu(bf16(np.concatenate([h, a], axis=1)) @ P["Wh", l].T + P["bh", l])
         hs.append(h); es.append(e); aggs.append(a)
     od = h @ P["Wd"].T + P["bd"]
     oe = np.concatenate([e, g], axis=1) @ P["Wo"].T + P["bo"]
@@ -382,7 +384,7 @@ def loss_and_grad(sysm, w, probes, backward=True, kind="kaporin"):
     de = doe @ P["Wo"][:, :H]
     for l in range(NL - 1, -1, -1):
         # node layer
-        xin = np.concatenate([hs[l], aggs[l]], axis=1)
+        xin = bf16(np.concatenate([hs[l], aggs[l]], axis=1))
         dpre = dh * (hs[l + 1] > 0)
         grad[Wh(l):Bh(l)] = (dpre.T @ xin).reshape(-1)
         grad[Bh(l):Bh(l) + H] = dpre.sum(0)
@@ -391,7 +393,7 @@ def loss_and_grad(sysm, w, probes, backward=True, kind="kaporin"):
         dagg = dx[:, H:] / np.maximum(sysm.deg, 1)[:, None] * (sysm.deg > 0)[:, None]
         de = de + dagg[ei] + dagg[ej]
         # edge layer
-        xe = np.concatenate([es[l], hs[l][ei] + hs[l][ej]], axis=1)
+        xe = bf16(np.concatenate([es[l], hs[l][ei] + hs[l][ej]], axis=1))
         dpe = de * (es[l + 1] > 0)
         grad[We(l):Be(l)] = (dpe.T @ xe).reshape(-1)
         grad[Be(l):Wh(l)] = dpe.sum(0)

@@ -4,7 +4,8 @@
   (oracle/mpnn_ref.py) on a Newton system the simulator produced, with the
   same weights and probe vectors: loss within 1e-4 relative, gradient within
   1e-3 relative in norm (FP32 accumulation in different orders; the weights
-  are BF16 on both sides).
+  are BF16 on both sides, and so are the inputs of the message-passing
+  layers, which run on the tensor cores).
 * Training on systems the simulator produces lowers the loss, and the trained
   network cuts PCG iterations against block-Jacobi at the same 1e-6 residual
   while the trajectory stays within 1e-6 of the bounding-box diagonal.
@@ -136,16 +137,23 @@ def test_factors_match_oracle(scene_name):
     assert np.abs(gs - es).max() <= 1e-5 * scale
     if len(ed):
         assert np.abs(gd - ed).max() <= 1e-5 * scale
-    # the network forward (trained-looking weights)
+    # the network forward (trained-looking weights).  The message-passing
+    # layers round their inputs to BF16 on both sides, but the GPU forms
+    # those inputs in FP32 and the oracle in FP64, so an input that lies
+    # within rounding distance of a BF16 tie can round to the neighbouring
+    # BF16 value: that input moves by 2^-8 of itself, and the entries
+    # downstream of it by up to about 1e-3 of the factor's scale.  The bulk
+    # of the entries agrees to FP32 accumulation order.
     w = _weights()
     sim.set_precond_weights(w)
     gs, gd = sim.precond_factor("learned")
     Gd, Ge, _ = M.forward(s, w)
     es, ed = _to_slots(d, s, Gd, Ge)
     scale = np.abs(es).max()
-    assert np.abs(gs - es).max() <= 1e-4 * scale
-    if len(ed):
-        assert np.abs(gd - ed).max() <= 1e-4 * scale
+    diff = np.abs(np.concatenate([(gs - es).ravel(), (gd - ed).ravel()]))
+    assert diff.max() <= 2e-3 * scale, (diff.max() / scale, np.median(diff) / scale)
+    assert np.median(diff) <= 1e-6 * scale, (diff.max() / scale, np.median(diff) / scale)
+    assert np.mean(diff <= 1e-4 * scale) >= 0.95, np.mean(diff <= 1e-4 * scale)
 
 
 def test_fsai_pcg_cuts_iterations():
