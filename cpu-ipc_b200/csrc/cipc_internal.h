@@ -77,6 +77,8 @@ struct DevBvh {
     DBuf<double> primLo, primHi;  // 3 per primitive
     DBuf<unsigned char> sortTmp;
     DBuf<double> sceneBox;     // 6
+    DBuf<double> boxPart;      // 6 per block of the scene-box reduction
+    DBuf<float> rec;           // 16 per internal node: both children's boxes (rounded outward) and indices
 };
 
 struct Ctx {

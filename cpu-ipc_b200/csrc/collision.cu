@@ -73,11 +73,28 @@ __global__ void edgeBoxKernel(int n, const int* edges, const double* x, const do
     }
 }
 
+// Scene box in two passes: each block reduces a strided share of the
+// primitive boxes into 6 partials, one block reduces the partials (min and
+// max do not depend on the order).  n lo/hi triples, stride 3.
 __global__ void sceneBoxKernel(int n, const double* lo, const double* hi, double* out) {
     double l[3], h[3];
     boxInit(l, h);
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x)
         for (int k = 0; k < 3; ++k) { l[k] = fmin(l[k], lo[3 * i + k]); h[k] = fmax(h[k], hi[3 * i + k]); }
+    for (int k = 0; k < 3; ++k) {
+        l[k] = blockReduce(l[k], MinOp(), 1.7976931348623157e308);
+        __syncthreads();
+        h[k] = blockReduce(h[k], MaxOp(), -1.7976931348623157e308);
+        __syncthreads();
+        if (threadIdx.x == 0) { out[6 * blockIdx.x + k] = l[k]; out[6 * blockIdx.x + 3 + k] = h[k]; }
+    }
+}
+// partials (6 per block, lo then hi) of nb blocks -> box
+__global__ void sceneBoxFinalKernel(int nb, const double* part, double* out) {
+    double l[3], h[3];
+    boxInit(l, h);
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        for (int k = 0; k < 3; ++k) { l[k] = fmin(l[k], part[6 * i + k]); h[k] = fmax(h[k], part[6 * i + 3 + k]); }
     for (int k = 0; k < 3; ++k) {
         l[k] = blockReduce(l[k], MinOp(), 1.7976931348623157e308);
         __syncthreads();
@@ -194,28 +211,68 @@ __global__ void refitKernel(int n, const int* left, const int* right, const int*
     }
 }
 
+// Traversal record of internal node i (64 bytes, one cache sector pair):
+// the boxes of both children rounded outward to FP32 (lo down, hi up) and
+// the children's node indices, so one load tests both children.
+__global__ void nodeRecordKernel(int n, const int* left, const int* right, const double* lo, const double* hi, float* rec) {
+    CIPC_KERNEL_LOOP(i, n - 1) {
+        const int ch[2] = {left[i], right[i]};
+        float r[16];
+        for (int s = 0; s < 2; ++s)
+            for (int k = 0; k < 3; ++k) {
+                r[6 * s + k] = __double2float_rd(lo[3 * ch[s] + k]);
+                r[6 * s + 3 + k] = __double2float_ru(hi[3 * ch[s] + k]);
+            }
+        r[12] = __int_as_float(ch[0]);
+        r[13] = __int_as_float(ch[1]);
+        r[14] = r[15] = 0.f;
+        float4* o = reinterpret_cast<float4*>(rec) + 4 * (size_t)i;
+        for (int q = 0; q < 4; ++q) o[q] = make_float4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+    }
+}
+
 struct BvhView {
     int n;
     const int *left, *right, *leafPrim;
     const double *lo, *hi;
+    const float4* rec;
 };
-BvhView view(const DevBvh& t) { return BvhView{t.n, t.left, t.right, t.leafPrim, t.lo, t.hi}; }
+BvhView view(const DevBvh& t) { return BvhView{t.n, t.left, t.right, t.leafPrim, t.lo, t.hi, reinterpret_cast<const float4*>(t.rec.p)}; }
 
-// Depth-first traversal (right pushed before left, as the reference); calls
-// f(prim) for every leaf whose box overlaps the query box with the gap.
+// Depth-first traversal; calls f(prim) for every leaf whose box overlaps the
+// query box with the gap (inclusive test, in FP64).  Internal nodes are
+// culled on their children's outward-rounded FP32 boxes, which contain the
+// FP64 boxes, so no leaf the FP64 test accepts is lost; each leaf is then
+// tested on its FP64 box.  The set of leaves reported is exactly that of a
+// walk on the FP64 boxes (the order of the calls differs, and every caller
+// sorts or reduces what it collects).
 template <class F>
 __device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, const double* qhi, double gap, int* status, F f) {
     if (t.n <= 0) return;
+    if (!overlaps(qlo, qhi, t.lo, t.hi, gap)) return;  // the root (node 0)
+    if (t.n == 1) { f(t.leafPrim[0]); return; }
     int stack[64];
     int sp = 0;
     stack[sp++] = 0;
     while (sp > 0) {
-        int node = stack[--sp];
-        if (!overlaps(qlo, qhi, t.lo + 3 * node, t.hi + 3 * node, gap)) continue;
-        if (node >= t.n - 1) { f(t.leafPrim[node - (t.n - 1)]); continue; }
-        if (sp + 2 > 64) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
-        stack[sp++] = t.right[node];
-        stack[sp++] = t.left[node];
+        const int node = stack[--sp];
+        const float4* r = t.rec + 4 * (size_t)node;
+        const float4 a = r[0], b = r[1], cc = r[2], d = r[3];
+        const double lo0[3] = {a.x, a.y, a.z}, hi0[3] = {a.w, b.x, b.y};
+        const double lo1[3] = {b.z, b.w, cc.x}, hi1[3] = {cc.y, cc.z, cc.w};
+        const int ch[2] = {__float_as_int(d.x), __float_as_int(d.y)};
+        const bool hit[2] = {overlaps(qlo, qhi, lo0, hi0, gap), overlaps(qlo, qhi, lo1, hi1, gap)};
+        // the right child goes on the stack first: the left subtree is walked first
+        for (int s = 1; s >= 0; --s) {
+            if (!hit[s]) continue;
+            const int cn = ch[s];
+            if (cn >= t.n - 1) {
+                if (overlaps(qlo, qhi, t.lo + 3 * cn, t.hi + 3 * cn, gap)) f(t.leafPrim[cn - (t.n - 1)]);
+            } else {
+                if (sp >= 64) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
+                stack[sp++] = cn;
+            }
+        }
     }
 }
 
@@ -475,13 +532,22 @@ __global__ void groundIntersectKernel(int n, const int* ground, const double* x,
     }
 }
 
-void sortKeys(Ctx& c, uint64_t* in, uint64_t* tmp, int n, int endBit) {
+// Stable radix sort of 64-bit keys on bits [beginBit, endBit): the bits
+// outside the range are either zero for every key or already in order.
+void sortKeys(Ctx& c, uint64_t* in, uint64_t* tmp, int n, int endBit, int beginBit = 0) {
     if (n <= 1) return;
     size_t bytes = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, in, tmp, n, 0, endBit, c.s);
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, in, tmp, n, beginBit, endBit, c.s);
     c.sortTmp.reserve(bytes + 16);
-    CIPC_CUDA(cub::DeviceRadixSort::SortKeys(c.sortTmp.p, bytes, in, tmp, n, 0, endBit, c.s));
+    CIPC_CUDA(cub::DeviceRadixSort::SortKeys(c.sortTmp.p, bytes, in, tmp, n, beginBit, endBit, c.s));
     CIPC_CUDA(cudaMemcpyAsync(in, tmp, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, c.s));
+}
+
+// bits needed for the values 0 .. m - 1
+int bitsFor(int m) {
+    int b = 1;
+    while (b < 31 && (1 << b) < m) ++b;
+    return b;
 }
 
 }  // namespace
@@ -504,12 +570,19 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     t.keys.reserve(n); t.keysAlt.reserve(n);
     t.left.reserve(nn); t.right.reserve(nn); t.parent.reserve(nn); t.leafPrim.reserve(n); t.flags.reserve(n);
     t.lo.reserve(3 * nn); t.hi.reserve(3 * nn); t.sceneBox.reserve(6);
-    launch(sceneBoxKernel, 1, 1024, 0, c.s, n, t.primLo, t.primHi, t.sceneBox);
+    const int nbBox = std::max(1, std::min(148, (n + 255) / 256));
+    t.boxPart.reserve(6 * (size_t)nbBox);
+    launch(sceneBoxKernel, nbBox, 256, 0, c.s, n, t.primLo, t.primHi, t.boxPart);
+    launch(sceneBoxFinalKernel, 1, 256, 0, c.s, nbBox, (const double*)t.boxPart, t.sceneBox);
     launch(mortonKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, t.sceneBox, t.keys);
-    sortKeys(c, t.keys, t.keysAlt, n, 64);
+    // keys are (30-bit code << 32) | index, written in index order: a stable
+    // sort on the code bits gives the order of a sort on the whole key
+    sortKeys(c, t.keys, t.keysAlt, n, 62, 32);
     if (n > 1) launch(karrasKernel, blocksFor(n - 1), TB, 0, c.s, n, t.keys, t.left, t.right, t.parent);
     launch(leafKernel, blocksFor(n), TB, 0, c.s, n, t.keys, t.primLo, t.primHi, t.leafPrim, t.lo, t.hi, t.flags, t.parent);
     if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, t.left, t.right, t.parent, t.lo, t.hi, t.flags);
+    t.rec.reserve(16 * (size_t)std::max(1, n - 1));
+    if (n > 1) launch(nodeRecordKernel, blocksFor(n - 1), TB, 0, c.s, n, t.left, t.right, (const double*)t.lo, (const double*)t.hi, t.rec.p);
     CIPC_CUDA(cudaGetLastError());
 }
 
@@ -575,12 +648,14 @@ void buildCollisionSets(Ctx& c, bool rehash) {
         c.nCcdPT = cnt[0]; c.nPT = cnt[1]; c.nPPERaw = cnt[2]; c.nCcdEE = cnt[3]; c.nEE = cnt[4]; c.nMoll = cnt[5];
         int mx = std::max(std::max(std::max(cnt[0], cnt[1]), std::max(cnt[2], cnt[3])), std::max(cnt[4], cnt[5]));
         c.kTmp.reserve(std::max(mx, 1));
-        sortKeys(c, c.ccdPT, c.kTmp, cnt[0], 64);
-        sortKeys(c, c.kPT, c.kTmp, cnt[1], 64);
+        // pair keys (query << 32 | primitive), mollified (eI << 34 | eJ << 4 | type)
+        const int ptBits = 32 + bitsFor(c.nsv), eeBits = 32 + bitsFor(c.nse), mollBits = std::min(64, 34 + bitsFor(c.nse));
+        sortKeys(c, c.ccdPT, c.kTmp, cnt[0], ptBits);
+        sortKeys(c, c.kPT, c.kTmp, cnt[1], ptBits);
         sortKeys(c, c.kPPE, c.kTmp, cnt[2], 63);
-        sortKeys(c, c.ccdEE, c.kTmp, cnt[3], 64);
-        sortKeys(c, c.kEE, c.kTmp, cnt[4], 64);
-        sortKeys(c, c.kMoll, c.kTmp, cnt[5], 64);
+        sortKeys(c, c.ccdEE, c.kTmp, cnt[3], eeBits);
+        sortKeys(c, c.kEE, c.kTmp, cnt[4], eeBits);
+        sortKeys(c, c.kMoll, c.kTmp, cnt[5], mollBits);
         // merge PP/PE duplicates (multiplicity)
         int nu = 0;
         c.uniq.reserve(std::max(cnt[2], 1));

@@ -541,12 +541,12 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                               &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.corrX, &c.corrR, &c.sweptPt, &c.scratch,
                               &c.scal, &c.energyBuf, &c.mpS, &c.mpT, &c.pcgPipe, &c.pcgParts,
                               &c.faceTree.lo, &c.faceTree.hi, &c.faceTree.primLo, &c.faceTree.primHi, &c.faceTree.sceneBox, &c.edgeTree.lo,
-                              &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox};
+                              &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox, &c.faceTree.boxPart, &c.edgeTree.boxPart};
         for (auto* d : ds) d->free();
         DBuf<float>* fs[] = {&c.valF, &c.elemHF, &c.dynHValF, &c.dynBF, &c.rF, &c.zF, &c.pF, &c.ApF, &c.xF, &c.DinvF, &c.mpW, &c.mpG, &c.mpM, &c.mpV,
                              &c.mpNodeF, &c.mpEdgeF, &c.mpEdgeFD, &c.mpH, &c.mpAgg, &c.mpES, &c.mpED, &c.mpHeadD, &c.mpGS, &c.mpGD,
                              &c.mpVec, &c.mpDGS, &c.mpDGD, &c.mpDH, &c.mpDES, &c.mpDED, &c.mpDAgg, &c.mpDS, &c.mpDSD,
-                             &c.mpBD, &c.mpBX, &c.mpPart};
+                             &c.mpBD, &c.mpBX, &c.mpPart, &c.faceTree.rec, &c.edgeTree.rec};
         for (auto* d : fs) d->free();
         DBuf<int>* is[] = {&c.btype, &c.softIdx, &c.dirIdx, &c.tets, &c.tris, &c.bendV, &c.faces, &c.surfVerts, &c.edges, &c.rowPtr, &c.colIdx,
                            &c.diagSlot, &c.hcPtr, &c.hcIdx, &c.gcPtr, &c.gcIdx, &c.selfActive, &c.selfEE, &c.eeIe, &c.ground, &c.counts, &c.runs,
