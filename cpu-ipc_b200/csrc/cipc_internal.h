@@ -193,6 +193,7 @@ struct Ctx {
     DevBvh faceTree, edgeTree;
     DBuf<double> sweptPt;     // 6 per surface vertex
     DBuf<double> scratch;     // reduction scratch
+    DBuf<double> sums;         // SUM_SLOTS device sums read back together
     DBuf<int> status;
     DBuf<double> scal;        // device scalars
     DBuf<double> energyBuf;
@@ -250,6 +251,9 @@ void buildRhs(Ctx& c);
 
 // ---- reductions (util.cu) ----
 double deviceSum(Ctx& c, const double* v, int n);
+constexpr int SUM_SLOTS = 16;
+void deviceSumTo(Ctx& c, const double* v, int n, int slot);  // no host sync
+void fetchSums(Ctx& c, double* h, int nslots);
 double deviceMax(Ctx& c, const double* v, int n);
 double deviceMin(Ctx& c, const double* v, int n, double init);
 double deviceDot(Ctx& c, const double* a, const double* b, int n);

@@ -185,49 +185,54 @@ __global__ void leafKernel(int n, const uint64_t* keys, const double* plo, const
     if (blockIdx.x == 0 && threadIdx.x == 0) parent[0] = -1;
 }
 
+__device__ __forceinline__ int atomAddAcqRel(int* p, int v) {
+    int old;
+    asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Bottom-up box merge: the second child to arrive at a node combines both
 // child boxes (left first, then right, as the reference's post-order merge).
-__global__ void refitKernel(int n, const int* left, const int* right, const int* parent, double* lo, double* hi, int* flags) {
+// The arrival is an acquire-release atomic: it publishes the box this thread
+// wrote for the child it came from and, for the second arrival, makes the
+// sibling's box visible.  The same thread writes the node's traversal
+// record: the boxes of both children rounded outward to FP32 (lo down, hi
+// up) and the children's node indices, 64 bytes, so that one load tests
+// both children.
+__global__ void refitKernel(int n, const int* left, const int* right, const int* parent, double* lo, double* hi, int* flags, float* rec) {
     CIPC_KERNEL_LOOP(s, n) {
         int node = s + n - 1;
         int p = parent[node];
         for (int guard = 0; guard < 64 && p >= 0; ++guard) {
-            __threadfence();
-            if (atomicAdd(&flags[p], 1) == 0) break;
-            __threadfence();
-            int l = left[p], r = right[p];
+            if (atomAddAcqRel(&flags[p], 1) == 0) break;
+            const int ch[2] = {left[p], right[p]};
+            double cb[2][6];
+            for (int q = 0; q < 2; ++q)
+                for (int k = 0; k < 3; ++k) {
+                    cb[q][k] = __ldcg(&lo[3 * ch[q] + k]);
+                    cb[q][3 + k] = __ldcg(&hi[3 * ch[q] + k]);
+                }
             for (int k = 0; k < 3; ++k) {
-                // L2 loads (__ldcg): a child box written by another SM must
-                // not be served from a stale L1 line.
-                double a = fmin(1.7976931348623157e308, __ldcg(&lo[3 * l + k]));
-                a = fmin(a, __ldcg(&lo[3 * r + k]));
-                double b = fmax(-1.7976931348623157e308, __ldcg(&hi[3 * l + k]));
-                b = fmax(b, __ldcg(&hi[3 * r + k]));
+                double a = fmin(1.7976931348623157e308, cb[0][k]);
+                a = fmin(a, cb[1][k]);
+                double b = fmax(-1.7976931348623157e308, cb[0][3 + k]);
+                b = fmax(b, cb[1][3 + k]);
                 lo[3 * p + k] = a; hi[3 * p + k] = b;
             }
+            float r[16];
+            for (int q = 0; q < 2; ++q)
+                for (int k = 0; k < 3; ++k) {
+                    r[6 * q + k] = __double2float_rd(cb[q][k]);
+                    r[6 * q + 3 + k] = __double2float_ru(cb[q][3 + k]);
+                }
+            r[12] = __int_as_float(ch[0]);
+            r[13] = __int_as_float(ch[1]);
+            r[14] = r[15] = 0.f;
+            float4* o = reinterpret_cast<float4*>(rec) + 4 * (size_t)p;
+            for (int q = 0; q < 4; ++q) o[q] = make_float4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
             node = p;
             p = parent[node];
         }
-    }
-}
-
-// Traversal record of internal node i (64 bytes, one cache sector pair):
-// the boxes of both children rounded outward to FP32 (lo down, hi up) and
-// the children's node indices, so one load tests both children.
-__global__ void nodeRecordKernel(int n, const int* left, const int* right, const double* lo, const double* hi, float* rec) {
-    CIPC_KERNEL_LOOP(i, n - 1) {
-        const int ch[2] = {left[i], right[i]};
-        float r[16];
-        for (int s = 0; s < 2; ++s)
-            for (int k = 0; k < 3; ++k) {
-                r[6 * s + k] = __double2float_rd(lo[3 * ch[s] + k]);
-                r[6 * s + 3 + k] = __double2float_ru(hi[3 * ch[s] + k]);
-            }
-        r[12] = __int_as_float(ch[0]);
-        r[13] = __int_as_float(ch[1]);
-        r[14] = r[15] = 0.f;
-        float4* o = reinterpret_cast<float4*>(rec) + 4 * (size_t)i;
-        for (int q = 0; q < 4; ++q) o[q] = make_float4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
     }
 }
 
@@ -580,9 +585,8 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     sortKeys(c, t.keys, t.keysAlt, n, 62, 32);
     if (n > 1) launch(karrasKernel, blocksFor(n - 1), TB, 0, c.s, n, t.keys, t.left, t.right, t.parent);
     launch(leafKernel, blocksFor(n), TB, 0, c.s, n, t.keys, t.primLo, t.primHi, t.leafPrim, t.lo, t.hi, t.flags, t.parent);
-    if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, t.left, t.right, t.parent, t.lo, t.hi, t.flags);
     t.rec.reserve(16 * (size_t)std::max(1, n - 1));
-    if (n > 1) launch(nodeRecordKernel, blocksFor(n - 1), TB, 0, c.s, n, t.left, t.right, (const double*)t.lo, (const double*)t.hi, t.rec.p);
+    if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, t.left, t.right, t.parent, t.lo, t.hi, t.flags, t.rec.p);
     CIPC_CUDA(cudaGetLastError());
 }
 

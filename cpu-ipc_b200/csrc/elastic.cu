@@ -480,27 +480,36 @@ double elasticEnergy(Ctx& c) {
     const SimParams& P = c.P;
     int n = std::max(std::max(c.nt, c.nf), std::max(c.nb, c.nv));
     c.energyBuf.reserve(std::max(n, 1));
-    double E = 0;
+    // every term's sum stays on the device until one read-back; the terms
+    // combine on the host in the fixed order below
+    const int ns = (int)c.hSoftIdx.size();
     if (c.nt) {
         launch(tetEnergyKernel, blocksFor(c.nt), TB, 0, c.s, c.nt, c.tets, c.x, c.DmInv, c.vol, c.tetMu, c.tetLam, c.energyBuf);
-        E += deviceSum(c, c.energyBuf, c.nt);
+        deviceSumTo(c, c.energyBuf, c.nt, 0);
     }
     if (c.nf) {
         launch(triEnergyKernel, blocksFor(c.nf), TB, 0, c.s, c.nf, c.tris, c.x, c.DmInv2, c.area, P.stretchS, P.shearS, P.strainRate, c.energyBuf);
-        E += deviceSum(c, c.energyBuf, c.nf);
+        deviceSumTo(c, c.energyBuf, c.nf, 1);
     }
     if (c.nb) {
         launch(bendEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.energyBuf);
-        E += 0.5 * P.plateRigidity * deviceSum(c, c.energyBuf, c.nb);
+        deviceSumTo(c, c.energyBuf, c.nb, 2);
     }
-    E *= P.dt * P.dt;
     launch(inertiaEnergyKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.vp, c.mass, P.drag, c.energyBuf);
-    E += deviceSum(c, c.energyBuf, c.nv);
-    int ns = (int)c.hSoftIdx.size();
+    deviceSumTo(c, c.energyBuf, c.nv, 3);
     if (ns) {
         launch(softEnergyKernel, blocksFor(ns), TB, 0, c.s, ns, c.softIdx, c.softTarget, P.softW, c.x, c.energyBuf);
-        E += deviceSum(c, c.energyBuf, ns);
+        deviceSumTo(c, c.energyBuf, ns, 4);
     }
+    double h[5];
+    fetchSums(c, h, 5);
+    double E = 0;
+    if (c.nt) E += h[0];
+    if (c.nf) E += h[1];
+    if (c.nb) E += 0.5 * P.plateRigidity * h[2];
+    E *= P.dt * P.dt;
+    E += h[3];
+    if (ns) E += h[4];
     return E;
 }
 

@@ -118,8 +118,19 @@ struct Stats {
     cipc_step_stats s;
 };
 
-bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st) {
-    double E0 = totalEnergy(c, kappa);
+// Energy of the point a line search accepted, kept for the next line search
+// of the same barrier subproblem: x, the active sets and the lagged friction
+// are unchanged in between (assembly, the linear solve and the step bounds
+// do not touch them), so the next search starts from the same value it
+// would recompute, as long as kappa has not changed.
+struct EnergyCache {
+    bool valid = false;
+    double kappa = 0, E = 0;
+};
+
+bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st, EnergyCache& ec) {
+    const double E0 = (ec.valid && ec.kappa == kappa) ? ec.E : totalEnergy(c, kappa);
+    ec.valid = false;
     double gTp = deviceDot(c, c.grad, c.dir, 3 * c.nv);
     if (!std::isfinite(E0) || !std::isfinite(gTp)) throw std::runtime_error("line search received a non-finite energy or direction");
     CIPC_CUDA(cudaMemcpyAsync(c.x0.p, c.x.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToDevice, c.s));
@@ -162,6 +173,7 @@ bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st) {
         buildCollisionSets(c, true);
         E = totalEnergy(c, kappa);
     }
+    bool recomputeAfterE = false;
     if (alpha < LF) {
         bool recompute = false;
         if (c.P.useBarrier) {
@@ -176,6 +188,7 @@ bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st) {
             }
         }
         if (recompute) buildCollisionSets(c, false);
+        recomputeAfterE = recompute;
     }
     st.energyBacktracks += nLS;
     st.intersectionBacktracks += nInter;
@@ -185,6 +198,13 @@ bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st) {
     st.acceptedStepSum += alpha;
     st.minimumAcceptedStep = std::min(st.minimumAcceptedStep, alpha);
     st.maximumAcceptedStep = std::max(st.maximumAcceptedStep, alpha);
+    // E was evaluated at the accepted x with the active sets now in place,
+    // unless the intersection check moved x afterwards
+    if (!recomputeAfterE) {
+        ec.valid = true;
+        ec.kappa = kappa;
+        ec.E = E;
+    }
     return true;
 }
 
@@ -209,6 +229,7 @@ void linearSolve(Ctx& c) {
 }
 
 int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
+    EnergyCache ec;
     int k = 0;
     double beta = 1;
     const int kmin = 6;
@@ -244,7 +265,7 @@ int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
         }
         sync(c);
         auto t3 = Clock::now();
-        bool accepted = lineSearch(c, alpha, kappa, st);
+        bool accepted = lineSearch(c, alpha, kappa, st, ec);
         sync(c);
         auto t4 = Clock::now();
         if (!accepted) {
@@ -539,7 +560,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                               &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
                               &c.fricLambda, &c.fricCoord, &c.fricBasis, &c.fricGLambda, &c.closeGVal, &c.closeSVal, &c.dynGVal, &c.dynHValD,
                               &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.corrX, &c.corrR, &c.sweptPt, &c.scratch,
-                              &c.scal, &c.energyBuf, &c.mpS, &c.mpT, &c.pcgPipe, &c.pcgParts,
+                              &c.scal, &c.energyBuf, &c.sums, &c.mpS, &c.mpT, &c.pcgPipe, &c.pcgParts,
                               &c.faceTree.lo, &c.faceTree.hi, &c.faceTree.primLo, &c.faceTree.primHi, &c.faceTree.sceneBox, &c.edgeTree.lo,
                               &c.edgeTree.hi, &c.edgeTree.primLo, &c.edgeTree.primHi, &c.edgeTree.sceneBox, &c.faceTree.boxPart, &c.edgeTree.boxPart};
         for (auto* d : ds) d->free();

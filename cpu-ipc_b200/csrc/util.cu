@@ -72,6 +72,25 @@ double reduce(Ctx& c, const double* a, const double* b, int n) {
 }  // namespace
 
 double deviceSum(Ctx& c, const double* v, int n) { return reduce<0>(c, v, nullptr, n); }
+
+// The same two-pass sum as deviceSum, left on the device in slot `slot` of
+// c.sums (no host synchronisation); fetchSums reads the slots back at once.
+void deviceSumTo(Ctx& c, const double* v, int n, int slot) {
+    c.sums.reserve(SUM_SLOTS);
+    if (n <= 0) {
+        CIPC_CUDA(cudaMemsetAsync(c.sums.p + slot, 0, sizeof(double), c.s));
+        return;
+    }
+    int nb = std::min(1024, (n + 4 * RB - 1) / (4 * RB));
+    int chunk = (n + nb - 1) / nb;
+    c.scratch.reserve(nb + 8);
+    launch(partialKernel<0>, nb, RB, 0, c.s, v, (const double*)nullptr, n, chunk, c.scratch.p + 8);
+    launch(finalKernel<0>, 1, RB, 0, c.s, (const double*)(c.scratch.p + 8), nb, c.sums.p + slot);
+}
+void fetchSums(Ctx& c, double* h, int nslots) {
+    CIPC_CUDA(cudaMemcpyAsync(h, c.sums.p, sizeof(double) * nslots, cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+}
 double deviceMax(Ctx& c, const double* v, int n) { return reduce<1>(c, v, nullptr, n); }
 double deviceMin(Ctx& c, const double* v, int n, double init) { return std::min(init, reduce<2>(c, v, nullptr, n)); }
 double deviceDot(Ctx& c, const double* a, const double* b, int n) { return reduce<3>(c, a, b, n); }
