@@ -107,3 +107,20 @@ def test_lbvh_candidates_equal_brute_force(oracle_mod):
     # the oracle's gap is sqrt(Hhat); rebuild the brute force with the same gap
     want = _brute_pairs(x, faces, verts, edges, sc["btype"], np.sqrt(o.scalars()["Hhat"]))
     assert got == want
+
+
+def test_pile_scene_places_every_cube_apart():
+    """The pile generator terminates at the configuration's size (64 cubes of
+    0.2 m in a 1.5 m box) and no two cubes' bounding spheres overlap, so the
+    initial state is free of intersections whatever the rotations."""
+    sc = cipc.scene_pile(64, 2)
+    x = sc["x"][sc["btype"] != 2].reshape(64, -1, 3)
+    centers = x.mean(axis=1)
+    radius = np.linalg.norm(x - centers[:, None, :], axis=2).max()
+    d = np.linalg.norm(centers[:, None, :] - centers[None, :, :], axis=2)
+    d[np.arange(64), np.arange(64)] = np.inf
+    assert d.min() > 2 * radius
+    # inside the box walls and above the floor
+    assert x[..., 1].min() > -1.0 + 0.02 and np.abs(x[..., 0]).max() < 0.8 and np.abs(x[..., 2]).max() < 0.8
+    # seeded: the same seed gives the same scene
+    assert np.array_equal(cipc.scene_pile(64, 2)["x"], sc["x"])
