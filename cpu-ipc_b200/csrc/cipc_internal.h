@@ -164,6 +164,7 @@ struct Ctx {
     DBuf<unsigned> pcgBar;              // grid-barrier counters of the persistent PCG
     DBuf<double> pcgPipe, pcgParts;     // pipelined PCG: six recurrence vectors, two sets of partial sums
     int pcgSliceMax = -1;               // cached pipelined PCG: largest static-slot count of a block's rows
+    int pcgSliceRows = 0;               // the block row count pcgSliceMax was computed for
     bool assembled = false;             // a Newton system has been assembled
 
     // learned preconditioner: network weights (FP32 master, BF16 copy, Adam

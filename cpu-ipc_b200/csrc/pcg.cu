@@ -280,6 +280,7 @@ struct PcgArgs {
     double *partA, *partB, *partC;
     double* pp;                   // pipelined variant: two sets of three partial arrays, PIPE_PMAX each
     int sliceMax;                 // cached variant: static slots of the largest block row range
+    int rowsPerBlock;             // cached variant: rows each block owns (<= ROWS_PER_BLOCK)
     int dynCap;                   // cached variant: contact slots a block's window may hold
     int cacheG;                   // cached variant with a factor: G blocks staged in shared memory
     double* scal;  // out: [3] rr, [4] iterations, [6] rhs2
@@ -423,13 +424,23 @@ __device__ __forceinline__ bool gridBarrierSum(unsigned* bar, int* flag, unsigne
 // Row-group iteration shared by every phase: the same (block, lane group)
 // owns the same rows in all phases.
 struct RowIter {
-    int lane, grp, first, stride;
+    int lane, grp, first, stride, limit;
     __device__ RowIter() {
         int gid = blockIdx.x * blockDim.x + threadIdx.x;
         lane = threadIdx.x & (GROUP - 1);
         grp = (threadIdx.x & 31) / GROUP;
         first = (gid / 32) * (32 / GROUP);
         stride = gridDim.x * blockDim.x / 32 * (32 / GROUP);
+        limit = 0x7fffffff;
+    }
+    // single pass over this block's own rows [blockIdx.x * rows, + rows) of nv
+    __device__ RowIter(int nv, int rows) {
+        lane = threadIdx.x & (GROUP - 1);
+        grp = (threadIdx.x & 31) / GROUP;
+        const int row0 = blockIdx.x * rows;
+        first = row0 + (threadIdx.x / 32) * (32 / GROUP);
+        stride = nv;
+        limit = min(nv, row0 + rows);
     }
 };
 
@@ -729,8 +740,8 @@ __device__ RowCache<MT> loadRowCache(const PcgArgs<MT, VT>& a, unsigned char* sm
     int* dcol = reinterpret_cast<int*>(smem + L.dcol);
     __shared__ int dlo, dhi;
     RowCache<MT> rc;
-    rc.row0 = blockIdx.x * ROWS_PER_BLOCK;
-    const int nrows = min(ROWS_PER_BLOCK, a.nv - rc.row0);
+    rc.row0 = blockIdx.x * a.rowsPerBlock;
+    const int nrows = min(a.rowsPerBlock, a.nv - rc.row0);  // >= 1: the grid is ceil(nv / rowsPerBlock)
     if (threadIdx.x == 0) { dlo = 0x7fffffff; dhi = 0; }
     for (int i = threadIdx.x; i <= nrows; i += blockDim.x) rp[i] = a.rowPtr[rc.row0 + i];
     __syncthreads();
@@ -775,7 +786,7 @@ template <class MT, class VT>
 __device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowCache<MT>& rc, const RowIter& it, int row, const VT* u,
                                             VT acc[3]) {
     const int lr = row - rc.row0;
-    if (row < a.nv) {
+    if (row < it.limit) {
         const int kb = rc.rp[lr] - rc.s0, ke = rc.rp[lr + 1] - rc.s0;
         for (int kk = kb + it.lane; kk < ke; kk += GROUP) {
             int c = rc.col[kk];
@@ -837,9 +848,9 @@ __device__ bool factorCachedPasses(const PcgArgs<MT, VT>& a, const RowCache<MT>&
                                    unsigned& ep) {
     const unsigned nb = gridDim.x;
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
-    for (int base = it.first; base < a.nv; base += it.stride) {
+    for (int base = it.first; base < it.limit; base += it.stride) {
         int row = base + it.grp;
-        bool active = row < a.nv;
+        bool active = row < it.limit;
         VT acc[3] = {VT(0), VT(0), VT(0)};
         if (active) rowFactorCached<false>(a, rc, it, row, tmp, acc);
         groupReduce3(acc);
@@ -848,9 +859,9 @@ __device__ bool factorCachedPasses(const PcgArgs<MT, VT>& a, const RowCache<MT>&
         if (active && q < 3) a.t[3 * row + q] = q == 0 ? acc[0] : (q == 1 ? acc[1] : acc[2]);
     }
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
-    for (int base = it.first; base < a.nv; base += it.stride) {
+    for (int base = it.first; base < it.limit; base += it.stride) {
         int row = base + it.grp;
-        bool active = row < a.nv;
+        bool active = row < it.limit;
         VT acc[3] = {VT(0), VT(0), VT(0)};
         if (active) rowFactorCached<true>(a, rc, it, row, (const VT*)a.t, acc);
         groupReduce3(acc);
@@ -938,7 +949,8 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     const unsigned nb = gridDim.x;
     unsigned ep = 0;
     const int nv = a.nv;
-    const RowIter it;
+    const RowIter it = CACHED ? RowIter(a.nv, a.rowsPerBlock) : RowIter();
+    const int rEnd = CACHED ? it.limit : a.nv;  // rows this thread's loops cover end here
     const int q = it.lane;  // the component this lane updates (q < 3)
     RowCache<MT> rc{};
     VT* sv = nullptr;
@@ -991,9 +1003,9 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     auto part = [&](int set, int k) { return a.pp + (size_t)(3 * set + k) * PIPE_PMAX; };
     // x = 0, r = b, u = M r; the recurrence vectors start at 0
     double rr = 0;
-    for (int base = it.first; base < nv; base += it.stride) {
+    for (int base = it.first; base < rEnd; base += it.stride) {
         const int row = base + it.grp;
-        const bool active = row < nv;
+        const bool active = row < rEnd;
         VT rq = VT(0);
         if (active && q < 3) {
             V(0, row) = VT(0); V(4, row) = VT(0); V(5, row) = VT(0); V(6, row) = VT(0); V(7, row) = VT(0);
@@ -1023,9 +1035,9 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return;
     // w = A u, m = M w, gamma = (r,u), delta = (w,u)
     double g = 0, dl = 0;
-    for (int base = it.first; base < nv; base += it.stride) {
+    for (int base = it.first; base < rEnd; base += it.stride) {
         const int row = base + it.grp;
-        const bool active = row < nv;
+        const bool active = row < rEnd;
         VT acc[3] = {VT(0), VT(0), VT(0)};
         Ax(row, (const VT*)a.u, acc);
         VT wq = VT(0);
@@ -1070,9 +1082,9 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
         VT* mNext = LEARNED ? a.mA : ((iter & 1) == 0 ? a.mB : a.mA);
         const VT bt = (VT)beta, al = (VT)alpha;
         double lrr = 0, lg = 0, ld = 0;
-        for (int base = it.first; base < nv; base += it.stride) {
+        for (int base = it.first; base < rEnd; base += it.stride) {
             const int row = base + it.grp;
-            const bool active = row < nv;
+            const bool active = row < rEnd;
             VT acc[3] = {VT(0), VT(0), VT(0)};
             Ax(row, mCur, acc);
             VT wq = VT(0);
@@ -1120,9 +1132,9 @@ __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     }
     if (CACHED) {
         // the solution leaves shared memory
-        for (int base = it.first; base < nv; base += it.stride) {
+        for (int base = it.first; base < rEnd; base += it.stride) {
             const int row = base + it.grp;
-            if (row < nv && q < 3) a.x[3 * row + q] = V(0, row);
+            if (row < rEnd && q < 3) a.x[3 * row + q] = V(0, row);
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1252,14 +1264,16 @@ static bool debugPcg() {
     return v == 1;
 }
 
-static int pcgSliceMax(Ctx& c) {
-    if (c.pcgSliceMax < 0) {
+// largest static-slot count of `rows` consecutive rows starting at a multiple of rows
+static int pcgSliceMax(Ctx& c, int rows) {
+    if (c.pcgSliceMax < 0 || c.pcgSliceRows != rows) {
         int m = 0;
-        for (int r0 = 0; r0 < c.nv; r0 += ROWS_PER_BLOCK) {
-            int r1 = std::min(c.nv, r0 + ROWS_PER_BLOCK);
+        for (int r0 = 0; r0 < c.nv; r0 += rows) {
+            int r1 = std::min(c.nv, r0 + rows);
             m = std::max(m, c.hRowPtr[r1] - c.hRowPtr[r0]);
         }
         c.pcgSliceMax = m;
+        c.pcgSliceRows = rows;
     }
     return c.pcgSliceMax;
 }
@@ -1276,7 +1290,11 @@ static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool class
         // solve and stages them in shared memory.  The largest configuration
         // that keeps every block resident is taken: the factor's blocks
         // cached or not, a contact window of 512 down to 0 slots.
-        a.sliceMax = pcgSliceMax(c);
+        // rows spread evenly over at least one block per SM
+        const int rows = (c.nv + std::max(needed, smCount) - 1) / std::max(needed, smCount);
+        const int nbRows = (c.nv + rows - 1) / rows;
+        a.rowsPerBlock = rows;
+        a.sliceMax = pcgSliceMax(c, rows);
         const void* fn = (const void*)pcgPipelinedKernel<MT, VT, LEARNED, true>;
         int maxOptin = 0, dev = 0;
         CIPC_CUDA(cudaGetDevice(&dev));
@@ -1291,20 +1309,21 @@ static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool class
                 CIPC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 int perSM = 0;
                 CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, smem));
-                if (perSM >= 1 && needed <= perSM * smCount) {
+                if (perSM >= 1 && nbRows <= perSM * smCount && nbRows <= cap) {
                     a.dynCap = dc;
                     a.cacheG = cg;
                     if (debugPcg())
-                        std::fprintf(stderr, "[pcg] single-pass launch: %d blocks, slice %d, contact window %d, factor cached %d, %zu B shared\n", needed,
-                                     a.sliceMax, dc, cg, smem);
+                        std::fprintf(stderr, "[pcg] single-pass launch: %d blocks of %d rows, slice %d, contact window %d, factor cached %d, %zu B shared\n",
+                                     nbRows, rows, a.sliceMax, dc, cg, smem);
                     ++g_kernelLaunches;
-                    CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(needed), dim3(PB), args, smem, c.s));
+                    CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(nbRows), dim3(PB), args, smem, c.s));
                     return;
                 }
             }
         }
     }
     a.sliceMax = 0;
+    a.rowsPerBlock = 0;
     const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false>;
     int perSM = 0;
     CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, 0));
