@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(PB) pcgPersistentKernel(PcgArgs<MT, VT> a) {
 // neighbours read the current one in the same pass; the partial sums also
 // alternate between two sets, so a set is rewritten only two barriers after
 // its last read.  The recurrences drift from the true residual in finite
-// precision; the callers judge every solve by the true FP64 residual.
+// precision; the callers decide every solve on the true FP64 residual.
 // ---------------------------------------------------------------------------
 // Rows a block owns in a single-pass launch (PB / GROUP consecutive rows),
 // staged once per solve in shared memory: the static slots (column and
@@ -1450,7 +1450,7 @@ static int pcgSolve64(Ctx& c) {
     int it = runPcgPersistent<double, double>(c, c.valD, c.dynBD, c.rhs.p, c.sol.p, c.r.p, c.z.p, c.p.p, c.Ap.p,
                                               pcgClassic() ? c.pcgTol : std::max(c.pcgTol, 1e-8),
                                               learned ? std::min(c.pcgMaxIter, factorCap()) : c.pcgMaxIter, flag, rel, learned);
-    // the true FP64 residual judges every solve; corrections restart from
+    // the true FP64 residual decides every solve; corrections restart from
     // the current iterate (residual replacement) with the textbook
     // recurrences, block-Jacobi taking over from a rejected factor
     double rhs2 = deviceDot(c, c.rhs, c.rhs, n3);
