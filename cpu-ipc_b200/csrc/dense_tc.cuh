@@ -114,11 +114,12 @@ __device__ __forceinline__ uint32_t packBf16(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&p);
 }
 
-// Layers of IN = 64 inputs made of two 32-wide halves: G::pair(item, lane)
-// gives inputs lane and 32 + lane of an item, so that a warp gathers one
-// item with coalesced 128-byte loads; E::emit32(item, const float v[32])
-// stores one item's OUT = 32 pre-activation outputs.  Shared memory:
-// 128 x 64 + 32 x 64 BF16 operands.
+// Layers of IN = 64 inputs made of two 32-wide halves.  G::Idx holds what
+// locates an item's inputs (G::index(item)); G::pair(idx, lane) gives inputs
+// lane and 32 + lane, so that a warp gathers one item with coalesced 128-byte
+// loads; G::shfl(idx, src) broadcasts lane src's Idx.  E::emit32(item, const
+// float v[32]) stores one item's OUT = 32 pre-activation outputs.  Shared
+// memory: 128 x 64 + 32 x 64 BF16 operands.
 template <class G, class E>
 __global__ void __launch_bounds__(THREADS) denseTcKernel(int n, G gather, E emit, const __nv_bfloat16* W, const __nv_bfloat16* bias, int* status,
                                                          int timeoutBit) {
@@ -150,12 +151,16 @@ __global__ void __launch_bounds__(THREADS) denseTcKernel(int n, G gather, E emit
     constexpr uint32_t lboA = (M / 8) * 128, lboB = (OUT / 8) * 128, sbo = 128;
     unsigned phase = 0;
     for (int base = blockIdx.x * M; base < n; base += gridDim.x * M) {
-        // warp w gathers the 32 items of its accumulator lanes, one item per
-        // step, inputs lane and 32 + lane from each lane (zeros past the end)
+        // warp w gathers the 32 items of its accumulator lanes: each lane
+        // reads one item's index (coalesced), then the warp walks the items,
+        // inputs lane and 32 + lane from each lane (zeros past the end)
+        const int mine = base + warp * 32 + lane;
+        const typename G::Idx myIdx = gather.index(mine < n ? mine : n - 1);
 #pragma unroll 8
         for (int j = 0; j < 32; ++j) {
             const int row = warp * 32 + j, item = base + row;
-            const float2 v = item < n ? gather.pair(item, lane) : make_float2(0.f, 0.f);
+            const typename G::Idx idx = G::shfl(myIdx, j);
+            const float2 v = item < n ? gather.pair(idx, lane) : make_float2(0.f, 0.f);
             *reinterpret_cast<__nv_bfloat16*>(sA + coreOffset(row, lane, M)) = __float2bfloat16_rn(v.x);
             *reinterpret_cast<__nv_bfloat16*>(sA + coreOffset(row, 32 + lane, M)) = __float2bfloat16_rn(v.y);
         }

@@ -300,9 +300,17 @@ struct EdgeLayerGather {  // [e_l ; h_i + h_j]
         i -= MPNN_H;
         return h[(size_t)MPNN_H * ei[k] + i] + h[(size_t)MPNN_H * ej[k] + i];
     }
-    // inputs lane and MPNN_H + lane (tensor-core layer)
-    __device__ float2 pair(int k, int lane) const {
-        return make_float2(e[(size_t)MPNN_H * slot[k] + lane], h[(size_t)MPNN_H * ei[k] + lane] + h[(size_t)MPNN_H * ej[k] + lane]);
+    // tensor-core layer: an edge's slot and end vertices, and its inputs
+    // lane and MPNN_H + lane
+    struct Idx {
+        int s, i, j;
+    };
+    __device__ Idx index(int k) const { return Idx{slot[k], ei[k], ej[k]}; }
+    __device__ static Idx shfl(const Idx& x, int src) {
+        return Idx{__shfl_sync(0xffffffffu, x.s, src), __shfl_sync(0xffffffffu, x.i, src), __shfl_sync(0xffffffffu, x.j, src)};
+    }
+    __device__ float2 pair(const Idx& x, int lane) const {
+        return make_float2(e[(size_t)MPNN_H * x.s + lane], h[(size_t)MPNN_H * x.i + lane] + h[(size_t)MPNN_H * x.j + lane]);
     }
 };
 struct NodeLayerGather {  // [h ; agg]
@@ -310,7 +318,14 @@ struct NodeLayerGather {  // [h ; agg]
     __device__ float operator()(int v, int i) const {
         return i < MPNN_H ? h[(size_t)MPNN_H * v + i] : agg[(size_t)MPNN_H * v + i - MPNN_H];
     }
-    __device__ float2 pair(int v, int lane) const { return make_float2(h[(size_t)MPNN_H * v + lane], agg[(size_t)MPNN_H * v + lane]); }
+    struct Idx {
+        int v;
+    };
+    __device__ Idx index(int v) const { return Idx{v}; }
+    __device__ static Idx shfl(const Idx& x, int src) { return Idx{__shfl_sync(0xffffffffu, x.v, src)}; }
+    __device__ float2 pair(const Idx& x, int lane) const {
+        return make_float2(h[(size_t)MPNN_H * x.v + lane], agg[(size_t)MPNN_H * x.v + lane]);
+    }
 };
 struct HeadEdgeGather {  // [e_L ; g]
     const int* slot;
