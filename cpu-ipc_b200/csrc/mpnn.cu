@@ -192,28 +192,37 @@ __global__ void degreeKernel(int nv, const int* rowPtr, const int* col, const in
 }
 
 // mean of incident edge states; an edge is read at its lower slot
+// Mean of the incident edges' features, one warp per vertex: lane t sums
+// feature t over the row's static slots, then its contact slots, in slot
+// order (one coalesced 128-byte row per edge).  Each lane first resolves one
+// slot of the row (its lower-slot index, or -1 for the diagonal and for
+// blocks without an edge), and the warp walks them with shuffles.
+__device__ __forceinline__ float aggregateRange(float a, int v, int k0, int k1, const int* col, const int* mir, const float* e, int lane) {
+    for (int c0 = k0; c0 < k1; c0 += 32) {
+        const int k = c0 + lane;
+        int slot = -1;
+        if (k < k1) {
+            const int c = col[k];
+            slot = c == v ? -1 : (c < v ? k : mir[k]);
+        }
+        const int m = min(32, k1 - c0);
+        for (int j = 0; j < m; ++j) {
+            const int sj = __shfl_sync(0xffffffffu, slot, j);
+            if (sj >= 0) a += e[(size_t)MPNN_H * sj + lane];
+        }
+    }
+    return a;
+}
+
 __global__ void aggregateKernel(int nv, const int* rowPtr, const int* col, const int* mirS, const float* eS, const int* dRowS, const int* dRowE,
                                 const int* dCol, const int* mirD, const float* eD, const int* deg, float* agg) {
-    CIPC_KERNEL_LOOP(v, nv) {
-        float a[MPNN_H];
-        for (int t = 0; t < MPNN_H; ++t) a[t] = 0.f;
-        for (int k = rowPtr[v]; k < rowPtr[v + 1]; ++k) {
-            int c = col[k];
-            if (c == v) continue;
-            int slot = c < v ? k : mirS[k];
-            if (slot < 0) continue;
-            for (int t = 0; t < MPNN_H; ++t) a[t] += eS[(size_t)MPNN_H * slot + t];
-        }
-        if (dRowS)
-            for (int k = dRowS[v]; k < dRowE[v]; ++k) {
-                int c = dCol[k];
-                if (c == v) continue;
-                int slot = c < v ? k : mirD[k];
-                if (slot < 0) continue;
-                for (int t = 0; t < MPNN_H; ++t) a[t] += eD[(size_t)MPNN_H * slot + t];
-            }
-        float inv = deg[v] > 0 ? 1.f / deg[v] : 0.f;
-        for (int t = 0; t < MPNN_H; ++t) agg[(size_t)MPNN_H * v + t] = a[t] * inv;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * blockDim.x / 32;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) / 32; v < nv; v += warps) {
+        float a = aggregateRange(0.f, v, rowPtr[v], rowPtr[v + 1], col, mirS, eS, lane);
+        if (dRowS) a = aggregateRange(a, v, dRowS[v], dRowE[v], dCol, mirD, eD, lane);
+        const float inv = deg[v] > 0 ? 1.f / deg[v] : 0.f;
+        agg[(size_t)MPNN_H * v + lane] = a * inv;
     }
 }
 
@@ -929,7 +938,7 @@ void mpnnForward(Ctx& c) {
         if (nD) launch(tc::denseTcKernel<EdgeLayerGather, ReluEmitEdge>, tcGrid(nD), tc::THREADS, 0, c.s, nD, EdgeLayerGather{dSlot, dI, dJ, ED(l), H(l)},
                        ReluEmitEdge{dSlot, ED(l + 1)}, w + mpWe(l), w + mpBe(l), c.status.p, (int)CIPC_ST_TC_TIMEOUT);
         float* agg = c.mpAgg.p + (size_t)l * MPNN_H * nv;
-        launch(aggregateKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, (const int*)c.colIdx.p, (const int*)c.mpMirS.p,
+        launch(aggregateKernel, blocksFor(32 * nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, (const int*)c.colIdx.p, (const int*)c.mpMirS.p,
                (const float*)ES(l + 1), d.rs, d.re, d.col, (const int*)c.mpMirD.p, (const float*)ED(l + 1), (const int*)c.mpDeg.p, agg);
         launch(tc::denseTcKernel<NodeLayerGather, ReluEmitNode>, tcGrid(nv), tc::THREADS, 0, c.s, nv, NodeLayerGather{H(l), agg}, ReluEmitNode{H(l + 1)},
                w + mpWh(l), w + mpBh(l), c.status.p, (int)CIPC_ST_TC_TIMEOUT);
