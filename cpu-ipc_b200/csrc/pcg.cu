@@ -929,15 +929,6 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
     return true;
 }
 
-template <class VT>
-__device__ __forceinline__ void jacobiRow(const double* Dinv, const VT* in, VT* out, int row) {
-    const double* D = Dinv + 9 * row;
-    double r0 = in[3 * row], r1 = in[3 * row + 1], r2 = in[3 * row + 2];
-    out[3 * row] = (VT)(D[0] * r0 + D[1] * r1 + D[2] * r2);
-    out[3 * row + 1] = (VT)(D[3] * r0 + D[4] * r1 + D[5] * r2);
-    out[3 * row + 2] = (VT)(D[6] * r0 + D[7] * r1 + D[8] * r2);
-}
-
 template <class MT, class VT, bool LEARNED, bool CACHED>
 __global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     extern __shared__ __align__(16) unsigned char pipeSmem[];
