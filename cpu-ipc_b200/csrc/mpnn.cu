@@ -304,11 +304,6 @@ struct EdgeFeatGather {
 struct EdgeLayerGather {  // [e_l ; h_i + h_j]
     const int *slot, *ei, *ej;
     const float *e, *h;
-    __device__ float operator()(int k, int i) const {
-        if (i < MPNN_H) return e[(size_t)MPNN_H * slot[k] + i];
-        i -= MPNN_H;
-        return h[(size_t)MPNN_H * ei[k] + i] + h[(size_t)MPNN_H * ej[k] + i];
-    }
     // tensor-core layer: an edge's slot and end vertices, and its inputs
     // lane and MPNN_H + lane
     struct Idx {
@@ -324,9 +319,6 @@ struct EdgeLayerGather {  // [e_l ; h_i + h_j]
 };
 struct NodeLayerGather {  // [h ; agg]
     const float *h, *agg;
-    __device__ float operator()(int v, int i) const {
-        return i < MPNN_H ? h[(size_t)MPNN_H * v + i] : agg[(size_t)MPNN_H * v + i - MPNN_H];
-    }
     struct Idx {
         int v;
     };
