@@ -389,6 +389,8 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
     if (s->nv >= (1 << 21) - 2) throw InvalidArgument("vertex count exceeds the 2^21 limit of the packed contact keys");
     if (!(s->dt > 0) || !(s->relDhat > 0)) throw InvalidArgument("time step and dHat must be positive");
     if (o && o->backend != CIPC_LINEAR_GPU_PCG) throw InvalidArgument("only the GPU PCG backend is implemented by this library");
+    if (s->quad_bending != 0 && s->quad_bending != 1)
+        throw InvalidArgument("bending model must be 0 (none) or 1 (quadratic); the dihedral-angle hinge model is not built on the GPU");
     if (o && o->precision != CIPC_PRECISION_FP64 && o->precision != CIPC_PRECISION_MIXED) throw InvalidArgument("unknown precision");
     if (o && o->preconditioner != CIPC_PRECOND_BLOCK_JACOBI && o->preconditioner != CIPC_PRECOND_LEARNED && o->preconditioner != CIPC_PRECOND_FSAI)
         throw InvalidArgument("unknown preconditioner");

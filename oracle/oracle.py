@@ -97,6 +97,8 @@ def lib():
         L.cipc_oracle_snh.argtypes = [dp, C.c_double, C.c_double, dp, dp, dp]
         L.cipc_oracle_distance.restype = C.c_double
         L.cipc_oracle_distance.argtypes = [C.c_int, dp, dp, dp]
+        L.cipc_oracle_hinge.restype = C.c_double
+        L.cipc_oracle_hinge.argtypes = [dp, dp, C.c_double, dp, dp]
         L.cipc_oracle_linear_solve.restype = C.c_int
         L.cipc_oracle_linear_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_int, C.c_double, C.c_int, ip, dp]
         _lib = L
@@ -288,6 +290,18 @@ def distance(kind, pts):
     g = np.zeros(n); H = np.zeros(n * n)
     d = lib().cipc_oracle_distance(kind, _dp(pts), _dp(g), _dp(H))
     return d, g, H.reshape(n, n)
+
+
+def hinge(x, rest, k):
+    """One hinge bending element (4 x 3 positions and rest positions: edge
+    start, edge end, first and second opposite vertex): energy, gradient (12)
+    and the PSD-projected Hessian (12 x 12)."""
+    x = np.ascontiguousarray(x, np.float64).reshape(12)
+    r = np.ascontiguousarray(rest, np.float64).reshape(12)
+    g = np.zeros(12)
+    H = np.zeros((12, 12))
+    e = lib().cipc_oracle_hinge(_dp(x), _dp(r), float(k), _dp(g), _dp(H))
+    return e, g, H
 
 
 def linear_solve(nv, rowptr, col, val, rhs, method="pcg", tol=1e-6, max_iter=10000):

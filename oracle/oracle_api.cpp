@@ -55,7 +55,9 @@ void* cipc_oracle_create(const cipc_oracle_scene* s, char* err, int errlen) {
                 m.tetLen[i] = tmp.lengthRate; m.tetVolR[i] = tmp.volumeRate;
             }
         }
-        if (s->quad_bending) prepareQuadraticBending(m);
+        // bending model: 0 none, 1 quadratic (USE_QUADRATIC_BENDING), 2 hinge
+        if (s->quad_bending == 1) prepareQuadraticBending(m);
+        else if (s->quad_bending == 2) prepareHingeBending(m);
         initRestState(m);
         m.rest = m.x;
         m.vprev = m.x;
@@ -262,6 +264,27 @@ void cipc_oracle_snh(const double* Fin, double u, double r, double* P, double* H
     Mat<9, 9> h = snhHessian(F, u, r);
     for (int a = 0; a < 9; ++a) for (int b = 0; b < 9; ++b) H[9 * a + b] = h.a[a][b];
     *psi = snhEnergyDensity(F, u, r);
+}
+
+// One hinge element: positions x12 and rest positions rest12 of (edge start,
+// edge end, first opposite, second opposite); returns 0.5 k w d^2 and fills
+// the gradient (12) and the PSD-projected Hessian (144) when given.
+double cipc_oracle_hinge(const double* x12, const double* rest12, double k, double* g, double* H) {
+    Mesh m;
+    for (int i = 0; i < 4; ++i) m.x.push_back(V3(rest12[3 * i], rest12[3 * i + 1], rest12[3 * i + 2]));
+    m.tris.push_back({0, 1, 2});
+    m.tris.push_back({0, 3, 1});
+    prepareHingeBending(m);
+    if (m.hinges.size() != 1) return std::nan("");
+    std::vector<V3> x;
+    for (int i = 0; i < 4; ++i) x.push_back(V3(x12[3 * i], x12[3 * i + 1], x12[3 * i + 2]));
+    HingeBend hb = m.hinges[0];
+    // keep the caller's vertex order (the hinge list sorts the edge)
+    hb.v[0] = 0; hb.v[1] = 1; hb.v[2] = 2; hb.v[3] = 3;
+    const double l = norm(m.x[1] - m.x[0]);
+    hb.weight = l * l / (norm(cross(m.x[1] - m.x[0], m.x[2] - m.x[0])) + norm(cross(m.x[1] - m.x[0], m.x[3] - m.x[0])));
+    hb.rest = hingeAngle(m.x[0], m.x[1], m.x[2], m.x[3], nullptr, nullptr);
+    return hingeEnergy(hb, x, k, g, H);
 }
 
 double cipc_oracle_distance(int kind, const double* pts, double* g, double* H) {

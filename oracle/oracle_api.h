@@ -20,7 +20,7 @@ typedef struct {
     const double* tetE;   /* nt per-tet Young's modulus, may be NULL (uniform E) */
     double density, cloth_density, thickness, E, nu, clothE, shearE, bendE, strainRate, friction;
     double dt, drag, newtonThr, relDhat;
-    int use_barrier, apply_gravity, quasi_static, quad_bending;
+    int use_barrier, apply_gravity, quasi_static, quad_bending;  /* bending model: 0 none, 1 quadratic, 2 hinge */
     double bboxMin[3], bboxMax[3];
     int nsoft; const int* softIdx; double softW; int softMotion; double softRate;
     int ndir; const int* dirIdx; int dirMotion; double dirRate;
@@ -70,6 +70,8 @@ double cipc_oracle_ee_ccd(const double* p12, const double* d12, double eta);
 void cipc_oracle_snh(const double* F, double u, double r, double* P, double* H, double* psi);
 /* distance kind 0 PP,1 PE,2 PT,3 EE,4 crossSqNorm: value, gradient, Hessian */
 double cipc_oracle_distance(int kind, const double* pts, double* g, double* H);
+/* one hinge bending element (HingeBending.cpp:76-106 + makePD) */
+double cipc_oracle_hinge(const double* x12, const double* rest12, double k, double* g, double* H);
 /* linear solve of a given lower CSR system (n scalar rows) with the oracle PCG or direct solver */
 int cipc_oracle_linear_solve(int nv, const int* rowptr, const int* col, const double* val, const double* rhs,
                              double* sol, int method, double tol, int maxIter, int* iters, double* relres);

@@ -52,6 +52,14 @@ struct QuadBend {
     Mat<4, 4> Q;
 };
 
+// Dihedral-angle (hinge) bending element, CPU IPC/HingeBending.{h,cpp}: the
+// edge (v[0], v[1]) and the opposite vertices of its two triangles, the
+// weight l0^2 / (2 A0 + 2 A1) and the rest angle.
+struct HingeBend {
+    int v[4];
+    double weight, rest;
+};
+
 // Prescribed boundary motions the scenes use.  The reference stores these as
 // std::function callbacks (BoundaryConditions.h:39-69); the oracle keeps the
 // two closed forms its scenes need.
@@ -75,6 +83,7 @@ struct Mesh {
     std::vector<double> vol, area, mass;
     std::vector<double> tetLen, tetVolR;  // per-tet SNH parameters (uniform in the reference)
     std::vector<QuadBend> bend;
+    std::vector<HingeBend> hinges;
     std::vector<I4> surface;  // v0, v1, v2, owning tet (or 0 for cloth)
     std::vector<int> surfVerts;
     std::vector<I2> surfEdges;
@@ -176,6 +185,12 @@ void parallelFor(int n, int threads, const std::function<void(int, int)>& body);
 void updateMaterial(Mesh& m);
 void initRestState(Mesh& m);
 void prepareQuadraticBending(Mesh& m);
+void prepareHingeBending(Mesh& m);
+// hinge angle and, when g / H are given, its gradient and Hessian in the
+// 12 coordinates (x[v0], x[v1], x[v2], x[v3])
+double hingeAngle(const V3& x0, const V3& x1, const V3& x2, const V3& x3, double* g, double* H);
+// 0.5 k w remainder(theta - rest, 2 pi)^2, and its gradient and PSD-projected Hessian
+double hingeEnergy(const HingeBend& hb, const std::vector<V3>& x, double k, double* g, double* H);
 void getSurface(Mesh& m);
 void updateInertialTarget(Mesh& m);
 

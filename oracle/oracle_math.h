@@ -224,6 +224,26 @@ template <int N> inline Jet<N> operator/(const Jet<N>& a, const Jet<N>& b) {
             r.h[i][j] = (a.h[i][j] - r.g[i] * b.g[j] - b.g[i] * r.g[j] - r.v * b.h[i][j]) / b.v;
     return r;
 }
+template <int N> inline Jet<N> jsqrt(const Jet<N>& a) {
+    Jet<N> r; r.v = std::sqrt(a.v);
+    for (int i = 0; i < N; ++i) r.g[i] = a.g[i] / (2.0 * r.v);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) r.h[i][j] = a.h[i][j] / (2.0 * r.v) - a.g[i] * a.g[j] / (4.0 * a.v * r.v);
+    return r;
+}
+// atan2(y, x) with its first and second partial derivatives chained in
+template <int N> inline Jet<N> jatan2(const Jet<N>& y, const Jet<N>& x) {
+    Jet<N> r; r.v = std::atan2(y.v, x.v);
+    const double r2 = x.v * x.v + y.v * y.v, r4 = r2 * r2;
+    const double ty = x.v / r2, tx = -y.v / r2;                       // d/dy, d/dx
+    const double tyy = -2.0 * x.v * y.v / r4, txx = 2.0 * x.v * y.v / r4, txy = (y.v * y.v - x.v * x.v) / r4;
+    for (int i = 0; i < N; ++i) r.g[i] = ty * y.g[i] + tx * x.g[i];
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j)
+            r.h[i][j] = ty * y.h[i][j] + tx * x.h[i][j] + tyy * y.g[i] * y.g[j] + txx * x.g[i] * x.g[j] +
+                        txy * (x.g[i] * y.g[j] + y.g[i] * x.g[j]);
+    return r;
+}
 template <int N> struct JV3 { Jet<N> x, y, z; };
 template <int N> inline JV3<N> jsub(const JV3<N>& a, const JV3<N>& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 template <int N> inline Jet<N> jdot(const JV3<N>& a, const JV3<N>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }

@@ -155,6 +155,79 @@ void prepareQuadraticBending(Mesh& m) {
     }
 }
 
+// Hinge list of prepareHingeBending (CPU IPC/Simulator.cpp:111-125) over the
+// interior triangle edges of mesh3D::getSurface's edge pass
+// (SimulationMesh.cpp:660-705): edges as (min, max) vertex pairs in
+// lexicographic order, each with the opposite vertices of its two triangles
+// in triangle order; edges on one triangle only carry no hinge.  Weight and
+// rest angle follow makeHingeBendingInfo (HingeBending.cpp:45-73).
+void prepareHingeBending(Mesh& m) {
+    m.hinges.clear();
+    std::map<std::pair<int, int>, std::vector<int>> opposite;
+    for (const I3& tri : m.tris)
+        for (int i = 0; i < 3; ++i) {
+            int a = tri[i], b = tri[(i + 1) % 3];
+            opposite[{std::min(a, b), std::max(a, b)}].push_back(tri[(i + 2) % 3]);
+        }
+    for (const auto& kv : opposite) {
+        if (kv.second.size() != 2) continue;
+        HingeBend hb;
+        hb.v[0] = kv.first.first; hb.v[1] = kv.first.second; hb.v[2] = kv.second[0]; hb.v[3] = kv.second[1];
+        // called at creation, while x holds the rest positions
+        const V3 e = m.x[hb.v[1]] - m.x[hb.v[0]];
+        const double l = norm(e);
+        const double twiceAreas = norm(cross(e, m.x[hb.v[2]] - m.x[hb.v[0]])) + norm(cross(e, m.x[hb.v[3]] - m.x[hb.v[0]]));
+        if (!std::isfinite(l) || !std::isfinite(twiceAreas) || l <= 0.0 || twiceAreas <= 0.0)
+            throw std::runtime_error("degenerate rest hinge geometry");
+        hb.weight = l * l / twiceAreas;
+        hb.rest = hingeAngle(m.x[hb.v[0]], m.x[hb.v[1]], m.x[hb.v[2]], m.x[hb.v[3]], nullptr, nullptr);
+        m.hinges.push_back(hb);
+    }
+}
+
+// Signed dihedral angle about the edge x0 -> x1 between the normals
+// n0 = e x (x2 - x0) and n1 = (x3 - x0) x e: zero when the two triangles are
+// coplanar and unfolded.  The reference measures the same angle through
+// LibShell::angle (Elasticity.cpp:29-150); any convention of the form
+// +/- theta + const gives the same hinge energy, since only
+// remainder(theta - rest, 2 pi) squared enters it.  Derivatives come from
+// second-order jets over the 12 coordinates.
+double hingeAngle(const V3& x0, const V3& x1, const V3& x2, const V3& x3, double* g, double* H) {
+    typedef Jet<12> J;
+    const JV3<12> p0 = jvar<12>(x0, 0), p1 = jvar<12>(x1, 3), p2 = jvar<12>(x2, 6), p3 = jvar<12>(x3, 9);
+    const JV3<12> e = jsub(p1, p0);
+    const JV3<12> n0 = jcross(e, jsub(p2, p0)), n1 = jcross(jsub(p3, p0), e);
+    const J el = jsqrt(jdot(e, e));
+    const J th = jatan2(jdot(jcross(n0, n1), e) / el, jdot(n0, n1));
+    if (g)
+        for (int i = 0; i < 12; ++i) g[i] = th.g[i];
+    if (H)
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) H[12 * i + j] = th.h[i][j];
+    return th.v;
+}
+
+// hingeBendingEnergy / hingeBendingGradientAndHessian (HingeBending.cpp:76-106)
+// followed by makePD, as the assembly (IPCSolver.cpp:238-267) applies it.
+double hingeEnergy(const HingeBend& hb, const std::vector<V3>& x, double k, double* g, double* H) {
+    double tg[12], tH[144];
+    const bool deriv = g || H;
+    const double th = hingeAngle(x[hb.v[0]], x[hb.v[1]], x[hb.v[2]], x[hb.v[3]], deriv ? tg : nullptr, deriv ? tH : nullptr);
+    const double d = std::remainder(th - hb.rest, 6.28318530717958647692);
+    const double s = k * hb.weight;
+    if (g)
+        for (int i = 0; i < 12; ++i) g[i] = s * d * tg[i];
+    if (H) {
+        Mat<12, 12> M;
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) M.a[i][j] = s * (tg[i] * tg[j] + d * tH[12 * i + j]);
+        makePD<12>(M);
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) H[12 * i + j] = M.a[i][j];
+    }
+    return 0.5 * s * d * d;
+}
+
 // mesh3D::getSurface, CPU IPC/SimulationMesh.cpp:364-446.  The reference walks
 // an std::unordered_map, so the face order is the standard library's bucket
 // order; the same container, hash and insertion sequence reproduce it.
@@ -1076,6 +1149,17 @@ int computeGradientAndHessian(Mesh& m, std::vector<V3>& grad, BHessian& BH, cons
         BH.H12.push_back(H);
         BH.D4.push_back({qb.v[0], qb.v[1], qb.v[2], qb.v[3]});
     }
+    // hinge bending (IPCSolver.cpp:238-267)
+    for (const HingeBend& hb : m.hinges) {
+        double hg[12], hH[144];
+        hingeEnergy(hb, m.x, m.plateRigidity, hg, hH);
+        for (int a = 0; a < 4; ++a) grad[hb.v[a]] += dt2 * V3(hg[3 * a], hg[3 * a + 1], hg[3 * a + 2]);
+        Mat<12, 12> H;
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) H.a[i][j] = dt2 * hH[12 * i + j];
+        BH.H12.push_back(H);
+        BH.D4.push_back({hb.v[0], hb.v[1], hb.v[2], hb.v[3]});
+    }
     // ground barrier (IPCSolver.cpp:270-293)
     for (size_t cI = 0; cI < m.envActive.size(); ++cI) {
         int v = m.envActive[cI];
@@ -1145,6 +1229,7 @@ double computeEnergy(const Mesh& m, double kappa, const SolverOptions& o) {
     }
     be *= 0.5 * m.plateRigidity;
     E += be;
+    for (const HingeBend& hb : m.hinges) E += hingeEnergy(hb, m.x, m.plateRigidity, nullptr, nullptr);
     E *= m.dt * m.dt;
     double dE = 0;
     for (int i = 0; i < m.nv(); ++i) {

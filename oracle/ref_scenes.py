@@ -108,10 +108,13 @@ def twisting_mat(soft=False):
     return scene
 
 
-def cloth_bunny():
-    """buildClothOverBunnyScene (Simulator.cpp:332-382)."""
+def cloth_bunny(hinge=False):
+    """buildClothOverBunnyScene (Simulator.cpp:332-382); hinge=True selects the
+    dihedral-angle bending the reference builds without USE_QUADRATIC_BENDING."""
     p = parameter_settings()
     p["E"] = 1e4
+    if hinge:
+        p["quad_bending"] = 2
     xc, tris = load_obj(os.path.join(REFERENCE_ASSETS, "triangleMesh/planes/plane1024.obj"))
     a = math.pi / 2
     R = np.array([[1, 0, 0], [0, math.cos(a), -math.sin(a)], [0, math.sin(a), math.cos(a)]])

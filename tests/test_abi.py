@@ -77,3 +77,13 @@ def test_no_cpu_fallback_without_device():
         pass
     rc, h, msg = _create(cipc.scene_two_cubes(1), cipc.linear_options())
     assert rc == 3 and not h.value
+
+
+def test_create_rejects_hinge_bending():
+    """The dihedral-angle hinge bending of the reference's non-quadratic build
+    exists in the oracle only; the library refuses it rather than falling
+    back to the quadratic model."""
+    sc = cipc.scene_cloth_drape(4, 1)
+    sc["params"] = dict(sc["params"], quad_bending=2)
+    rc, h, msg = _create(sc, cipc.linear_options())
+    assert rc == 1 and not h.value and "hinge" in msg

@@ -74,3 +74,20 @@ def test_cloth_bunny_loader_positions():
     k = KAT["cloth_bunny_loader"]
     assert np.allclose(sc["x"][0], k["vertex0"], atol=1e-6)
     assert np.allclose(sc["x"][1024], k["vertex1024"], atol=1e-6)
+
+
+@needs_assets
+def test_cloth_bunny_hinge_bending_one_step(oracle_mod):
+    """The reference built without USE_QUADRATIC_BENDING bends the cloth with
+    dihedral-angle hinges; its documentation quotes the first step of the
+    cloth-bunny scene in that build.  The hinge Hessian blocks are full 3x3
+    blocks, so the matrix has more nonzeros than with quadratic bending."""
+    sc = ref_scenes.cloth_bunny(hinge=True)
+    k = KAT["cloth_bunny_hinge_1_step"]
+    o = oracle_mod.Oracle(sc, linear="direct", threads=8)
+    assert o.nsf == k["surface_faces"]
+    st = o.step()
+    assert st["newton"] == k["newton"]
+    assert st["energyBacktracks"] == k["energy_backtracks"]
+    assert st["intersectionBacktracks"] == k["intersection_backtracks"]
+    assert st["matrixNnz"] == k["matrix_nnz"]

@@ -124,3 +124,56 @@ def test_pile_scene_places_every_cube_apart():
     assert x[..., 1].min() > -1.0 + 0.02 and np.abs(x[..., 0]).max() < 0.8 and np.abs(x[..., 2]).max() < 0.8
     # seeded: the same seed gives the same scene
     assert np.array_equal(cipc.scene_pile(64, 2)["x"], sc["x"])
+
+
+def _rand_hinge(rng):
+    """A hinge (edge start, edge end, two opposite vertices) near the unit
+    square split along its diagonal, and a bent copy of it."""
+    rest = np.array([[0, 0, 0], [1, 1, 0], [1, 0, 0], [0, 1, 0]], float) + 0.05 * rng.standard_normal((4, 3))
+    x = rest + 0.2 * rng.standard_normal((4, 3))
+    return x, rest
+
+
+def test_hinge_gradient_and_hessian_match_finite_differences(oracle_mod):
+    """The oracle's hinge element (energy 0.5 k w remainder(theta - theta0)^2,
+    HingeBending.cpp:76-106): its gradient matches central differences of its
+    energy, and its Hessian matches the PSD projection (clamped eigenvalues,
+    as makePD) of the central-difference Hessian of the energy."""
+    rng = np.random.default_rng(5)
+    k = 3.0
+    for _ in range(6):
+        x, rest = _rand_hinge(rng)
+        e, g, H = oracle_mod.hinge(x, rest, k)
+        h = 1e-6
+        gf = np.zeros(12)
+        Hf = np.zeros((12, 12))
+        for i in range(12):
+            d = np.zeros(12); d[i] = h
+            ep, gp, _ = oracle_mod.hinge(x.reshape(12) + d, rest, k)
+            em, gm, _ = oracle_mod.hinge(x.reshape(12) - d, rest, k)
+            gf[i] = (ep - em) / (2 * h)
+            Hf[:, i] = (gp - gm) / (2 * h)
+        assert np.abs(g - gf).max() <= 1e-6 * max(1.0, np.abs(g).max())
+        # the finite differences of the projected gradient see the unprojected
+        # Hessian; project it the way makePD does and compare
+        w, V = np.linalg.eigh(0.5 * (Hf + Hf.T))
+        Hp = (V * np.maximum(w, 0.0)) @ V.T
+        assert np.abs(H - Hp).max() <= 1e-5 * max(1.0, np.abs(Hp).max())
+        assert np.allclose(H, H.T) and np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+
+
+def test_hinge_energy_invariants(oracle_mod):
+    """Zero at the rest shape, unchanged by a rigid motion of the bent shape,
+    and the same whichever opposite vertex is listed first."""
+    rng = np.random.default_rng(6)
+    x, rest = _rand_hinge(rng)
+    e0, g0, _ = oracle_mod.hinge(rest, rest, 2.0)
+    assert abs(e0) < 1e-20 and np.abs(g0).max() < 1e-12
+    e, _, _ = oracle_mod.hinge(x, rest, 2.0)
+    q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    er, _, _ = oracle_mod.hinge(x @ q.T + np.array([0.3, -1.0, 2.0]), rest, 2.0)
+    assert abs(er - e) <= 1e-12 * abs(e)
+    es, _, _ = oracle_mod.hinge(x[[0, 1, 3, 2]], rest[[0, 1, 3, 2]], 2.0)
+    assert abs(es - e) <= 1e-12 * abs(e)
