@@ -105,6 +105,8 @@ struct Ctx {
     // topology and rest data
     DBuf<int> tets, tris, bendV, faces, surfVerts, edges;
     DBuf<double> DmInv, vol, tetMu, tetLam, DmInv2, area, bendQ;
+    DBuf<double> hingeW, hingeTh0;  // dihedral-angle bending: per hinge weight and rest angle (bendQ unused)
+    int hinge = 0;                  // bending elements are dihedral-angle hinges
 
     // static symmetric BSR pattern (elements), full storage
     int nnzb = 0;

@@ -8,6 +8,7 @@
 // Elasticity.cpp:1144-1205 (PK1), 1337-1544 (Hessians), 695-771 (energies).
 #include "cipc_device.cuh"
 #include "cipc_internal.h"
+#include "hinge_bending.cuh"
 
 #include <algorithm>
 #include <numeric>
@@ -270,6 +271,69 @@ __global__ void bendKernel(int nb, const int* bv, const double* Q, const double*
     }
 }
 
+// Dihedral-angle bending (hingeBendingGradientAndHessian + makePD,
+// HingeBending.cpp:88-106, IPCSolver.cpp:238-267), one warp per hinge as the
+// contact kernels: every lane forms the angle's gradient in closed form,
+// lanes 0-11 one column each of its Hessian, the warp projects the 12 x 12
+// Hessian onto the PSD cone in shared memory, and the 10 lower 3 x 3 blocks
+// go to the hinge's element slots as bendKernel writes them (blocks touching
+// a constrained vertex zeroed).  scale = plateRigidity * dt^2.
+constexpr int HINGE_WPB = 4;
+template <class T>
+__global__ void __launch_bounds__(HINGE_WPB * 32) hingeKernel(int nb, const int* bv, const double* hw, const double* th0, const double* x,
+                                                              const int* btype, double k, double dt2, double* elemG, T* elemH, int blockBase,
+                                                              int gradBase, int* status) {
+    __shared__ JacobiSmem sm[HINGE_WPB];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    JacobiSmem& S = sm[w];
+    for (int i = blockIdx.x * HINGE_WPB + w; i < nb; i += gridDim.x * HINGE_WPB) {
+        int v[4];
+        double xs[12];
+        for (int a = 0; a < 4; ++a) {
+            v[a] = bv[4 * i + a];
+            for (int q = 0; q < 3; ++q) xs[3 * a + q] = x[3 * (size_t)v[a] + q];
+        }
+        const double s = k * hw[i];
+        const double d = remainder(hinge::angle(xs) - th0[i], 6.28318530717958647692);
+        hinge::Vec3<double> gr[4];
+        hinge::angleGrad(hinge::Vec3<double>{xs[0], xs[1], xs[2]}, hinge::Vec3<double>{xs[3], xs[4], xs[5]},
+                         hinge::Vec3<double>{xs[6], xs[7], xs[8]}, hinge::Vec3<double>{xs[9], xs[10], xs[11]}, gr);
+        double tg[12];
+        for (int a = 0; a < 4; ++a) { tg[3 * a] = gr[a].x; tg[3 * a + 1] = gr[a].y; tg[3 * a + 2] = gr[a].z; }
+        if (!isfinite(d) && lane == 0) raiseStatus(status, CIPC_ST_NONFINITE);
+        if (lane < 12) {
+            double col[12];
+            hinge::angleHessColumn(xs, lane, col);
+            double tl = tg[0];
+            for (int r = 1; r < 12; ++r) tl = r == lane ? tg[r] : tl;
+            for (int r = 0; r < 12; ++r) S.A[12 * r + lane] = s * (tg[r] * tl + d * col[r]);
+        }
+        if (lane < 4) st3(elemG, gradBase + 4 * i + lane, mk(dt2 * s * d * tg[3 * lane], dt2 * s * d * tg[3 * lane + 1], dt2 * s * d * tg[3 * lane + 2]));
+        __syncwarp();
+        if (!warpPsdProject(S, 12, lane) && lane == 0) raiseStatus(status, CIPC_ST_JACOBI_CAP);
+        T* out = elemH + (size_t)9 * (blockBase + 10 * i);
+        for (int e = lane; e < 90; e += 32) {
+            const int blk = e / 9, ent = e % 9;
+            const int a = blk >= 6 ? 3 : (blk >= 3 ? 2 : (blk >= 1 ? 1 : 0));
+            const int b = blk - a * (a + 1) / 2;  // lowerIdx(a, b) = blk
+            const bool ok = btype[v[a]] == 0 && btype[v[b]] == 0;
+            out[e] = ok ? T(dt2 * S.A[12 * (3 * a + ent / 3) + 3 * b + ent % 3]) : T(0);
+        }
+        __syncwarp();
+    }
+}
+
+// w * remainder(theta - theta0, 2 pi)^2 per hinge (the energy sums it with 0.5 k)
+__global__ void hingeEnergyKernel(int nb, const int* bv, const double* hw, const double* th0, const double* x, double* out) {
+    CIPC_KERNEL_LOOP(i, nb) {
+        double xs[12];
+        for (int a = 0; a < 4; ++a)
+            for (int q = 0; q < 3; ++q) xs[3 * a + q] = x[3 * (size_t)bv[4 * i + a] + q];
+        const double d = remainder(hinge::angle(xs) - th0[i], 6.28318530717958647692);
+        out[i] = hw[i] * d * d;
+    }
+}
+
 template <class T>
 __global__ void slotReduceKernel(int nnzb, const int* hcPtr, const int* hcIdx, const T* elemH, T* val) {
     CIPC_KERNEL_LOOP(sl, nnzb) {
@@ -453,7 +517,10 @@ static void assembleElasticT(Ctx& c, T* elemH, T* val) {
                                                        c.elemG, elemH, bBase, gBase);
     profEnd(c, PROF_TRI);
     bBase += 6 * c.nf; gBase += 3 * c.nf;
-    if (c.nb)
+    if (c.nb && c.hinge)
+        launch(hingeKernel<T>, std::max(1, std::min((c.nb + HINGE_WPB - 1) / HINGE_WPB, 148 * 64)), HINGE_WPB * 32, 0, c.s, c.nb, c.bendV,
+               (const double*)c.hingeW, (const double*)c.hingeTh0, c.x, c.btype, P.plateRigidity, dt2, c.elemG, elemH, bBase, gBase, c.status.p);
+    else if (c.nb)
         launch(bendKernel<T>, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.btype, P.plateRigidity * dt2, c.elemG, elemH, bBase, gBase);
     profBegin(c, PROF_SLOT);
     launch(slotReduceKernel<T>, blocksFor(c.nnzb), TB, 0, c.s, c.nnzb, c.hcPtr, c.hcIdx, elemH, val);
@@ -492,7 +559,10 @@ double elasticEnergy(Ctx& c) {
         deviceSumTo(c, c.energyBuf, c.nf, 1);
     }
     if (c.nb) {
-        launch(bendEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.energyBuf);
+        if (c.hinge)
+            launch(hingeEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, (const double*)c.hingeW, (const double*)c.hingeTh0, c.x, c.energyBuf);
+        else
+            launch(bendEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.energyBuf);
         deviceSumTo(c, c.energyBuf, c.nb, 2);
     }
     launch(inertiaEnergyKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.vp, c.mass, P.drag, c.energyBuf);

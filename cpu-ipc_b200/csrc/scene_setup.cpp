@@ -8,11 +8,13 @@
 // (CPU IPC/Simulator.cpp:48-109), mesh3D::getSurface
 // (CPU IPC/SimulationMesh.cpp:364-446), buildModels (Simulator.cpp:426-529).
 #include "scene_setup.h"
+#include "hinge_bending.cuh"
 
 #include <cmath>
 #include <cstdint>
 #include <set>
 #include <stdexcept>
+#include <map>
 #include <unordered_map>
 
 namespace cipc {
@@ -141,6 +143,33 @@ void setupScene(const SceneInput& in, SceneRest& out) {
                 out.bendV.insert(out.bendV.end(), {e0, e1, o1, o2});
                 for (int p = 0; p < 4; ++p) for (int q = 0; q < 4; ++q) out.bendQ.push_back(s * K[p] * K[q]);
             }
+        }
+    }
+    // dihedral-angle hinges (prepareHingeBending, Simulator.cpp:111-125): the
+    // interior triangle edges as (min, max) pairs in lexicographic order, each
+    // with the opposite vertices of its two triangles in triangle order
+    out.hingeW.clear();
+    out.hingeTh0.clear();
+    if (in.hingeBending) {
+        std::map<std::pair<int, int>, std::vector<int>> opposite;
+        for (int i = 0; i < in.nf; ++i) {
+            const int* tri = &in.tris[3 * i];
+            for (int e = 0; e < 3; ++e) {
+                const int a = tri[e], b = tri[(e + 1) % 3];
+                opposite[{std::min(a, b), std::max(a, b)}].push_back(tri[(e + 2) % 3]);
+            }
+        }
+        for (const auto& kv : opposite) {
+            if (kv.second.size() != 2) continue;
+            const int hv[4] = {kv.first.first, kv.first.second, kv.second[0], kv.second[1]};
+            double r[12];
+            for (int k = 0; k < 4; ++k)
+                for (int q = 0; q < 3; ++q) r[3 * k + q] = x[3 * (size_t)hv[k] + q];
+            const double w = hinge::restWeight(r);
+            if (!std::isfinite(w) || !(w > 0)) throw std::invalid_argument("degenerate rest hinge geometry");
+            out.bendV.insert(out.bendV.end(), {hv[0], hv[1], hv[2], hv[3]});
+            out.hingeW.push_back(w);
+            out.hingeTh0.push_back(hinge::angle(r));
         }
     }
     // collision surface

@@ -389,8 +389,7 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
     if (s->nv >= (1 << 21) - 2) throw InvalidArgument("vertex count exceeds the 2^21 limit of the packed contact keys");
     if (!(s->dt > 0) || !(s->relDhat > 0)) throw InvalidArgument("time step and dHat must be positive");
     if (o && o->backend != CIPC_LINEAR_GPU_PCG) throw InvalidArgument("only the GPU PCG backend is implemented by this library");
-    if (s->quad_bending != 0 && s->quad_bending != 1)
-        throw InvalidArgument("bending model must be 0 (none) or 1 (quadratic); the dihedral-angle hinge model is not built on the GPU");
+    if (s->quad_bending < 0 || s->quad_bending > 2) throw InvalidArgument("bending model must be 0 (none), 1 (quadratic) or 2 (hinge)");
     if (o && o->precision != CIPC_PRECISION_FP64 && o->precision != CIPC_PRECISION_MIXED) throw InvalidArgument("unknown precision");
     if (o && o->preconditioner != CIPC_PRECOND_BLOCK_JACOBI && o->preconditioner != CIPC_PRECOND_LEARNED && o->preconditioner != CIPC_PRECOND_FSAI)
         throw InvalidArgument("unknown preconditioner");
@@ -429,7 +428,8 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
         if (s->tetE) in.tetE.assign(s->tetE, s->tetE + s->nt);
         in.density = s->density; in.cloth_density = s->cloth_density; in.thickness = s->thickness; in.E = s->E; in.nu = s->nu;
         in.clothE = s->clothE; in.shearE = s->shearE; in.bendE = s->bendE; in.strainRate = s->strainRate; in.relDhat = s->relDhat;
-        in.quadBending = s->quad_bending != 0;
+        in.quadBending = s->quad_bending == 1;
+        in.hingeBending = s->quad_bending == 2;
         for (int k = 0; k < 3; ++k) { in.bboxMin[k] = s->bboxMin[k]; in.bboxMax[k] = s->bboxMax[k]; }
         if (s->surfFaces && s->surfVerts && s->surfEdges) {
             in.hasSurface = true;
@@ -471,6 +471,8 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
         upload(c->DmInv, r.DmInv); upload(c->vol, r.vol); upload(c->tetMu, r.tetMu); upload(c->tetLam, r.tetLam);
         upload(c->DmInv2, r.DmInv2); upload(c->area, r.area);
         upload(c->bendV, r.bendV); upload(c->bendQ, r.bendQ);
+        c->hinge = in.hingeBending ? 1 : 0;
+        if (c->hinge) { upload(c->hingeW, r.hingeW); upload(c->hingeTh0, r.hingeTh0); }
         upload(c->faces, r.faces); upload(c->surfVerts, r.surfVerts); upload(c->edges, r.edges);
         upload(c->softIdx, c->hSoftIdx);
         std::vector<double> tgt;
@@ -559,7 +561,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
         if (h->c->s) cudaStreamSynchronize(h->c->s);
         Ctx& c = *h->c;
         DBuf<double>* ds[] = {&c.x, &c.x0, &c.xt, &c.vp, &c.vel, &c.rest, &c.dir, &c.grad, &c.mass, &c.softTarget, &c.DmInv, &c.vol, &c.tetMu,
-                              &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
+                              &c.tetLam, &c.DmInv2, &c.area, &c.bendQ, &c.hingeW, &c.hingeTh0, &c.valD, &c.constD, &c.elemHD, &c.elemG, &c.vtxGrad, &c.diagExtra,
                               &c.fricLambda, &c.fricCoord, &c.fricBasis, &c.fricGLambda, &c.closeGVal, &c.closeSVal, &c.dynGVal, &c.dynHValD,
                               &c.dynBD, &c.rhs, &c.sol, &c.r, &c.z, &c.p, &c.Ap, &c.Dinv, &c.red, &c.corrX, &c.corrR, &c.sweptPt, &c.scratch,
                               &c.scal, &c.energyBuf, &c.sums, &c.mpS, &c.mpT, &c.pcgPipe, &c.pcgParts,

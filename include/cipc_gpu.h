@@ -68,8 +68,8 @@ typedef struct {
     double density, cloth_density, thickness, E, nu, clothE, shearE, bendE, strainRate, friction;
     double dt, drag, newtonThr, relDhat;
     int use_barrier, apply_gravity, quasi_static;
-    int quad_bending;       /* bending model: 1 quadratic (USE_QUADRATIC_BENDING), 0 none; the
-                               reference's dihedral-angle hinge model is rejected */
+    int quad_bending;       /* bending model: 1 quadratic (USE_QUADRATIC_BENDING), 2 dihedral-angle
+                               hinges (the reference's build without it), 0 none */
     double bboxMin[3], bboxMax[3];
     int nsoft; const int* softIdx; double softW; int softMotion; double softRate;
     int ndir; const int* dirIdx; int dirMotion; double dirRate;

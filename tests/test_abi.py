@@ -79,11 +79,8 @@ def test_no_cpu_fallback_without_device():
     assert rc == 3 and not h.value
 
 
-def test_create_rejects_hinge_bending():
-    """The dihedral-angle hinge bending of the reference's non-quadratic build
-    exists in the oracle only; the library refuses it rather than falling
-    back to the quadratic model."""
+def test_create_rejects_unknown_bending_model():
     sc = cipc.scene_cloth_drape(4, 1)
-    sc["params"] = dict(sc["params"], quad_bending=2)
+    sc["params"] = dict(sc["params"], quad_bending=3)
     rc, h, msg = _create(sc, cipc.linear_options())
-    assert rc == 1 and not h.value and "hinge" in msg
+    assert rc == 1 and not h.value and "bending model" in msg

@@ -57,3 +57,11 @@ def test_cloth_bunny_one_step():
     assert st["energyBacktracks"] == k["energy_backtracks"]
     assert st["intersectionBacktracks"] == k["intersection_backtracks"]
     assert abs(st["minConstraintDistance2"] - k["min_distance2"]) <= 1e-9 * k["min_distance2"]
+
+
+def test_cloth_bunny_hinge_bending_one_step():
+    _, st = _run(ref_scenes.cloth_bunny(hinge=True), 1)
+    k = KAT["cloth_bunny_hinge_1_step"]
+    assert st["newtonIterations"] == k["newton"]
+    assert st["energyBacktracks"] == k["energy_backtracks"]
+    assert st["intersectionBacktracks"] == k["intersection_backtracks"]

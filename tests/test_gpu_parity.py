@@ -60,9 +60,16 @@ def _gpu_full_matrix(g, btype):
     return (D @ A @ D + sp.diags((~free) * A.diagonal())).tocsr()
 
 
+def _hinge(sc):
+    """The scene with dihedral-angle hinge bending in place of quadratic bending."""
+    sc["params"] = dict(sc["params"], quad_bending=2)
+    return sc
+
+
 CONTACT_SCENES = {
     "cubes_touching": lambda: (cipc.scene_two_cubes(3, gap=0.0015), 2e-4),
     "cloth_on_cube": lambda: (cipc.scene_cloth_drape(10, 2), 0.0),
+    "cloth_on_cube_hinge": lambda: (_hinge(cipc.scene_cloth_drape(10, 2)), 0.0),
     "pile": lambda: (cipc.scene_pile(4, 2, seed=3), 0.0),
 }
 
@@ -161,6 +168,7 @@ def test_ccd_and_step_bounds(oracle_mod, contact_states, name):
 @pytest.mark.parametrize("scene_fn,steps", [
     (lambda: cipc.scene_two_cubes(3), 25),
     (lambda: cipc.scene_cloth_drape(10, 2), 25),
+    (lambda: _hinge(cipc.scene_cloth_drape(10, 2)), 25),
     (lambda: cipc.scene_pile(4, 2, seed=3), 15),
     (lambda: cipc.scene_twist(2, 8, 6), 6),
 ])

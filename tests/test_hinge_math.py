@@ -1,8 +1,8 @@
 """The library's hinge bending element math (cpu-ipc_b200/csrc/hinge_bending.cuh:
 closed-form angle gradient, forward-mode Hessian) built for the host and
 compared with the oracle's element (second-order jets, makePD projection), no
-GPU.  The GPU kernel that will call this header is not built yet; the library
-rejects the hinge model at creation."""
+GPU.  The GPU kernel (elastic.cu, hingeKernel) runs this same code; its
+parity with the oracle is in test_gpu_parity.py."""
 import ctypes as C
 import os
 import shutil
