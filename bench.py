@@ -33,7 +33,10 @@ random rotations, dropped into a static open box, dt = 0.01 s.
 
 --impl reference times the reference's CPU path on the host cores.  The
 reference itself cannot be compiled here (Eigen, oneTBB, oneMKL and
-SuiteSparse are absent), so its FP64 restatement (oracle/) stands in.
+SuiteSparse are absent), so its FP64 restatement (oracle/) stands in.  For
+the cloth drape it starts from the oracle's own state after the settle steps
+(oracle/states/), then runs the same warm-up, so it times the same frames as
+the GPU arm; cpu_baseline does the same without the warm-up.
 """
 import argparse
 import json
@@ -196,12 +199,33 @@ def pcg_iteration_bytes(counts, mixed, factor):
     return b
 
 
-def cpu_baseline(scene, seconds, steps_cap=50):
-    """The FP64 oracle on the same scene, all host cores, bounded by time."""
+def oracle_at_settled_frame(args, scene, threads):
+    """The FP64 oracle on the bench scene, at the frame the GPU arm's warm-up
+    starts from when a saved state exists.
+
+    For the cloth drape the oracle's own state after --settle-steps steps
+    (written by oracle/states/make_contact_state.py) is restored, so the CPU
+    legs time the same contact frames as the GPU arm.  Without a saved state
+    for this scene they start at frame 0 (free fall: cheaper steps).
+    Returns (oracle, index of the next step)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    threads = os.cpu_count() or 1
     o = oracle.Oracle(scene, linear="pcg", threads=threads)
+    if args.scene == "cloth_drape":
+        path = os.path.join(ROOT, "oracle", "states", f"cloth_drape_{args.cloth}_frame{args.settle_steps}.npz")
+        if os.path.exists(path):
+            return o, o.restore_state(path)
+    return o, 0
+
+
+def frames(first, n, restored):
+    return f"frames {first}-{first + n - 1}" + (" (from the restored contact-phase state)" if restored else " (from the start of the scene)")
+
+
+def cpu_baseline(args, scene, seconds, steps_cap=50):
+    """The FP64 oracle on the same scene, all host cores, bounded by time."""
+    threads = os.cpu_count() or 1
+    o, f0 = oracle_at_settled_frame(args, scene, threads)
     t0 = time.time()
     n = 0
     while n < steps_cap:
@@ -211,7 +235,7 @@ def cpu_baseline(scene, seconds, steps_cap=50):
             break
     dt = time.time() - t0
     return {"value": n / dt, "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"first {n} steps of the same scene ({dt:.1f} s, block-Jacobi PCG at 1e-6, {threads} threads)"}
+            "sample": f"{frames(f0, n, f0 > 0)} of the same scene ({dt:.1f} s, block-Jacobi PCG at 1e-6, {threads} threads)"}
 
 
 def run_reference(args, world, rank):
@@ -219,14 +243,12 @@ def run_reference(args, world, rank):
         return
     import cipc
     scene = make_scene(args, cipc)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
     threads = os.cpu_count() or 1
-    o = oracle.Oracle(scene, linear="pcg", threads=threads)
+    o, f0 = oracle_at_settled_frame(args, scene, threads)
     budget = 150.0
     t0 = time.time()
     w = 0
-    while w < args.warmup and time.time() - t0 < budget / 4:
+    while w < max(3, args.warmup) and time.time() - t0 < budget / 4:
         o.step(); w += 1
     t1 = time.time()
     n = 0
@@ -237,9 +259,10 @@ def run_reference(args, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": n, "warmup": w,
             "ms_per_step": 1000 * dt / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": workload(args),
-                                            "solver": "FP64 CPU restatement of the reference pipeline, block-Jacobi PCG 1e-6"},
+                                            "solver": "FP64 CPU restatement of the reference pipeline, block-Jacobi PCG 1e-6",
+                                            "timed_frames": f"{f0 + w}-{f0 + w + n - 1}"},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{n} steps after {w} warm-up steps; the reference itself does not compile here"},
+                             "sample": f"{frames(f0 + w, n, f0 > 0)} after {w} warm-up steps; the reference itself does not compile here"},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -435,7 +458,7 @@ def main():
         }
         if not args.no_cpu_baseline and world == 1:
             try:
-                line["cpu_baseline"] = cpu_baseline(scene, args.cpu_seconds)
+                line["cpu_baseline"] = cpu_baseline(args, scene, args.cpu_seconds)
             except Exception as e:
                 line["cpu_baseline"] = {"error": str(e)}
         print(json.dumps(line), flush=True)

@@ -1,11 +1,13 @@
 """Test infrastructure only: ctypes front-end of the FP64 CPU oracle.
 
-Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
-this module; the shipped library never uses it.  It loads ``liboracle.so``
-(built from the sources beside it by ``make``) and exposes the oracle's
-scene set-up, time step and per-stage evaluations.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs (cpu_baseline
+and --impl reference) import this module; the shipped library never uses
+it.  It loads ``liboracle.so`` (built from the sources beside it by
+``make``) and exposes the oracle's scene set-up, time step and per-stage
+evaluations.
 """
 import ctypes as C
+import hashlib
 import os
 import subprocess
 
@@ -212,6 +214,51 @@ class Oracle:
     def set(self, name, arr):
         a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.nv, 3)
         self.L.cipc_oracle_set(self.h, self._FIELDS[name], _dp(a))
+
+    def rest_digest(self):
+        """SHA-256 of the rest positions: names the scene a saved state belongs to."""
+        return hashlib.sha256(self.get("rest").tobytes()).hexdigest()
+
+    def save_state(self, path, frame):
+        """Write what the next step starts from: positions, velocities, kappa.
+
+        After every step V_prev equals x and x_tilde = V_prev + dt v + dt^2 g
+        (updateInertialTarget, IPCSolver.cpp:55-70), so restore_state rebuilds
+        those two; this checks the rebuild against the oracle's own x_tilde.
+        """
+        x, vel = self.get("x"), self.get("vel")
+        if not np.array_equal(self.get("vprev"), x):
+            raise RuntimeError("save_state must follow a completed step (V_prev != x)")
+        xt = self.get("xtilde")
+        g = next((g for g in (-9.8, 0.0) if np.array_equal(xt, self._xtilde(x, vel, g))), None)
+        if g is None:
+            raise RuntimeError("x_tilde does not follow V_prev + dt v + dt^2 g")
+        np.savez_compressed(path, x=x, vel=vel, kappa=self.scalars()["kappa"], gravity=g, frame=frame,
+                            rest_sha256=self.rest_digest())
+
+    def restore_state(self, path):
+        """Load a state written by save_state; returns its frame number.
+
+        The collision sets are rebuilt at the restored positions: a step
+        leaves them built at its final positions, and the next step's lagged
+        friction starts from them (frictionInitialize, Friction.cpp:81-156).
+        Raises ValueError when the state belongs to another scene."""
+        s = np.load(path)
+        if str(s["rest_sha256"]) != self.rest_digest():
+            raise ValueError(f"{path} was saved from another scene")
+        x, vel = s["x"], s["vel"]
+        self.set("x", x)
+        self.set("vprev", x)
+        self.set("vel", vel)
+        self.set("xtilde", self._xtilde(x, vel, float(s["gravity"])))
+        self.set_kappa(float(s["kappa"]))
+        self.collision_sets()
+        return int(s["frame"])
+
+    def _xtilde(self, vprev, vel, g):
+        # componentwise as the oracle: (V_prev + v dt) + (0, g dt dt, 0)
+        dt = self.scalars()["dt"]
+        return vprev + vel * dt + np.array([0.0, g * dt * dt, 0.0])
 
     def surface(self):
         f = np.zeros((self.nsf, 3), np.int32)
