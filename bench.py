@@ -33,7 +33,9 @@ random rotations, dropped into a static open box, dt = 0.01 s.
 
 --impl reference times the reference's CPU path on the host cores.  The
 reference itself cannot be compiled here (Eigen, oneTBB, oneMKL and
-SuiteSparse are absent), so its FP64 restatement (oracle/) stands in.  For
+SuiteSparse are absent), so its FP64 restatement (oracle/) stands in, with
+the reference's default linear solver, PARDISO, restated as a parallel
+multifrontal Cholesky under a nested-dissection ordering.  For
 the cloth drape it starts from the oracle's own state after the settle steps
 (oracle/states/), then runs the same warm-up, so it times the same frames as
 the GPU arm; cpu_baseline does the same without the warm-up.
@@ -210,7 +212,7 @@ def oracle_at_settled_frame(args, scene, threads):
     Returns (oracle, index of the next step)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    o = oracle.Oracle(scene, linear="pcg", threads=threads)
+    o = oracle.Oracle(scene, linear="multifrontal", threads=threads)
     if args.scene == "cloth_drape":
         path = os.path.join(ROOT, "oracle", "states", f"cloth_drape_{args.cloth}_frame{args.settle_steps}.npz")
         if os.path.exists(path):
@@ -235,7 +237,7 @@ def cpu_baseline(args, scene, seconds, steps_cap=50):
             break
     dt = time.time() - t0
     return {"value": n / dt, "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"{frames(f0, n, f0 > 0)} of the same scene ({dt:.1f} s, block-Jacobi PCG at 1e-6, {threads} threads)"}
+            "sample": f"{frames(f0, n, f0 > 0)} of the same scene ({dt:.1f} s, multifrontal Cholesky under nested dissection, {threads} threads)"}
 
 
 def run_reference(args, world, rank):
@@ -259,7 +261,8 @@ def run_reference(args, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": n, "warmup": w,
             "ms_per_step": 1000 * dt / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": workload(args),
-                                            "solver": "FP64 CPU restatement of the reference pipeline, block-Jacobi PCG 1e-6",
+                                            "solver": "FP64 CPU restatement of the reference pipeline; linear solve by a parallel multifrontal "
+                                                      "Cholesky under nested dissection (the PARDISO algorithm class)",
                                             "timed_frames": f"{f0 + w}-{f0 + w + n - 1}"},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
                              "sample": f"{frames(f0 + w, n, f0 > 0)} after {w} warm-up steps; the reference itself does not compile here"},

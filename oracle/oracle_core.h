@@ -172,7 +172,7 @@ struct StepStats {
 };
 
 struct SolverOptions {
-    int linear = 0;           // 0 = direct sparse Cholesky, 1 = block-Jacobi PCG
+    int linear = 0;           // 0 = envelope Cholesky, 1 = block-Jacobi PCG, 2 = multifrontal Cholesky
     double pcgRelTol = 1e-6;  // LinearSolverOptions.h:15
     int pcgMaxIter = 10000;   // LinearSolverOptions.h:16
     int threads = 1;
@@ -246,6 +246,7 @@ struct LinearSystem {
 };
 void assembleSystem(const Mesh& m, const BHessian& BH, const std::vector<V3>& g, LinearSystem& ls);
 void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o);
+void multifrontalSolve(LinearSystem& ls, int nv, int threads);
 int solveIPCStep(Mesh& m, BroadPhase& bp, StepStats& stats, int stepIndex, const SolverOptions& o);
 
 }  // namespace oracle

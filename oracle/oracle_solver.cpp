@@ -239,6 +239,7 @@ static void pcgSolve(LinearSystem& ls, int nv, double tol, int maxIter) {
 
 void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o) {
     if (o.linear == 0) directSolve(ls, nv);
+    else if (o.linear == 2) multifrontalSolve(ls, nv, o.threads);
     else pcgSolve(ls, nv, o.pcgRelTol, o.pcgMaxIter);
     for (double v : ls.sol)
         if (!std::isfinite(v)) throw std::runtime_error("linear solve produced a non-finite direction");

@@ -30,6 +30,19 @@ def test_twisting_mat_one_step(oracle_mod):
 
 
 @needs_assets
+def test_twisting_mat_one_step_multifrontal(oracle_mod):
+    # the documented answer came from the PARDISO backend; the oracle's
+    # PARDISO-class solver (multifrontal Cholesky) reproduces it as well
+    o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=False), linear="multifrontal", threads=8)
+    st = o.step()
+    x = o.get("x")
+    k = KAT["twisting_mat_1_step"]
+    assert st["newton"] == k["newton"]
+    assert st["matrixNnz"] == k["matrix_nnz"]
+    assert abs((x * x).sum() - k["squared_norm_sum"]) / k["squared_norm_sum"] < 1e-12
+
+
+@needs_assets
 def test_twisting_mat_soft_five_steps(oracle_mod):
     o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=True), linear="direct", threads=8)
     for _ in range(5):
