@@ -5,11 +5,15 @@
 // from Assets/scene/parameterSetting.txt and the Gmsh/OBJ meshes), plus the
 // synthetic benchmark scenes (two-cubes, cloth-drape).  Writes metrics.csv
 // with the reference's columns (IPCSolver.cpp:1286-1315; the PARDISO columns
-// are zero, the PCG iteration count and residual are appended) and prints the
-// reference's RESULT line (cipc_headless.cpp:146-175).
+// are zero, the PCG iteration count and residual are appended), the
+// reference's timeCost.txt summary and, with --write-checkpoints, its
+// checkpoint files every tenth step; --resume restarts from such a checkpoint
+// (the reference's or this runner's).  Prints the reference's RESULT line
+// (cipc_headless.cpp:146-175).
 //
 // Links only against libcipc_gpu.so through include/cipc_gpu.h.
 #include "cipc_gpu.h"
+#include "runtime_files.h"
 
 #include <algorithm>
 #include <cmath>
@@ -40,6 +44,9 @@ struct Options {
     bool writeOutput = true;
     bool verbose = false;
     bool disableBarrier = false;
+    bool resume = false;            // cipc_headless --resume
+    bool writeCheckpoints = false;  // cipc_headless --write-checkpoints
+    bool hingeBending = false;      // the reference built without USE_QUADRATIC_BENDING
 };
 
 void usage(const char* exe) {
@@ -53,7 +60,10 @@ void usage(const char* exe) {
               << "  --precision fp64|mixed  (default mixed)\n"
               << "  --precond jacobi|learned|fsai (default jacobi)\n"
               << "  --weights FILE          learned-preconditioner weights (raw float32)\n"
-              << "  --output DIRECTORY      metrics.csv goes here\n"
+              << "  --output DIRECTORY      metrics.csv, timeCost.txt and tempData/ go here\n"
+              << "  --resume                start from the checkpoint in DIRECTORY/tempData\n"
+              << "  --write-checkpoints     write a checkpoint to DIRECTORY/tempData every tenth step\n"
+              << "  --hinge-bending         dihedral-angle bending instead of quadratic bending\n"
               << "  --disable-barrier\n"
               << "  --no-output\n"
               << "  --verbose\n"
@@ -98,6 +108,9 @@ Options parse(int argc, char** argv) {
             else if (v == "fsai") o.precond = CIPC_PRECOND_FSAI;
             else throw std::invalid_argument("unknown preconditioner: " + v);
         } else if (a == "--disable-barrier") o.disableBarrier = true;
+        else if (a == "--resume") o.resume = true;
+        else if (a == "--write-checkpoints") o.writeCheckpoints = true;
+        else if (a == "--hinge-bending") o.hingeBending = true;
         else if (a == "--no-output") o.writeOutput = false;
         else if (a == "--verbose") o.verbose = true;
         else if (a == "--help" || a == "-h") { usage(argv[0]); std::exit(0); }
@@ -379,7 +392,7 @@ int main(int argc, char** argv) {
         d.density = p.density; d.cloth_density = p.cloth_density; d.thickness = p.thickness; d.E = p.E; d.nu = p.nu;
         d.clothE = p.clothE; d.shearE = p.shearE; d.bendE = p.bendE; d.strainRate = p.strainRate; d.friction = p.friction;
         d.dt = p.dt; d.drag = p.drag; d.newtonThr = p.newtonThr; d.relDhat = p.relDhat;
-        d.use_barrier = p.use_barrier; d.apply_gravity = p.apply_gravity; d.quasi_static = p.quasi_static; d.quad_bending = 1;
+        d.use_barrier = p.use_barrier; d.apply_gravity = p.apply_gravity; d.quasi_static = p.quasi_static; d.quad_bending = o.hingeBending ? 2 : 1;
         for (int q = 0; q < 3; ++q) { d.bboxMin[q] = lo[q]; d.bboxMax[q] = hi[q]; }
         d.nsoft = (int)s.softIdx.size(); d.softIdx = s.softIdx.data(); d.softW = s.softW; d.softMotion = s.softMotion; d.softRate = s.motionRate;
         d.ndir = (int)s.dirIdx.size(); d.dirIdx = s.dirIdx.data(); d.dirMotion = s.dirMotion; d.dirRate = s.motionRate;
@@ -401,29 +414,70 @@ int main(int argc, char** argv) {
             check(cipc_gpu_precond_set_weights(ctx, w.data(), n), ctx, "cipc_gpu_precond_set_weights");
         }
 
+        const std::string outDir = o.output.empty() ? "headless_output" : o.output;
+        cipc_io::RunTotals totals;
+        // resume: positions and inertial target from tempData (V_prev = x),
+        // then the collision sets at those positions (Simulator.cpp:510-519);
+        // the running totals, step index and kappa as the first step reads
+        // them (IPCSolver.cpp:1085-1101)
+        bool resumed = false;
+        if (o.resume) {
+            std::vector<double> xr, xt;
+            resumed = cipc_io::loadVertexState(outDir, nv, xr, xt);
+            if (resumed) {
+                check(cipc_gpu_set_state(ctx, 0, xr.data()), ctx, "cipc_gpu_set_state");
+                check(cipc_gpu_set_state(ctx, 2, xr.data()), ctx, "cipc_gpu_set_state");
+                check(cipc_gpu_set_state(ctx, 3, xt.data()), ctx, "cipc_gpu_set_state");
+                long long counts[4];
+                check(cipc_gpu_build_collision_sets(ctx, counts), ctx, "cipc_gpu_build_collision_sets");
+                if (cipc_io::loadCheckpointTotals(outDir, totals))
+                    check(cipc_gpu_set_kappa(ctx, totals.kappa), ctx, "cipc_gpu_set_kappa");
+            }
+            if (o.verbose) std::cout << (resumed ? "load temp data" : "no temp data") << std::endl;
+        }
+
         std::ofstream metrics;
         if (o.writeOutput) {
-            std::string dir = o.output.empty() ? "headless_output" : o.output;
-            mkdir(dir.c_str(), 0755);
-            metrics.open(dir + "/metrics.csv", std::ios::out | std::ios::trunc);
-            if (!metrics) throw std::runtime_error("invalid output directory " + dir);
-            metrics << "frame,step_ms,assembly_ms,linear_ms,ccd_ms,line_search_ms,post_ms,"
-                       "newton,kappa_loops,backtracks,energy_backtracks,intersection_backtracks,"
-                       "max_energy_backtracks_per_newton,newton_steps_over_two_backtracks,"
-                       "mean_alpha,min_alpha,max_alpha,collisions,kappa,min_distance2,"
-                       "ground_contacts,self_contacts,mollified_contacts,matrix_nnz,"
-                       "symbolic_analyses,numeric_factorizations,pardiso_analysis_ms,"
-                       "pardiso_factorization_ms,pardiso_solve_ms,linear_solver_threads,"
-                       "factor_nnz,pcg_iterations,pcg_relative_residual\n";
+            if (!cipc_io::makeDirectories(outDir)) throw std::runtime_error("invalid output directory " + outDir);
+            // a resumed run appends to the metrics it continues (IPCSolver.cpp:1275-1285)
+            bool hasContent = false;
+            if (resumed) {
+                std::ifstream existing(cipc_io::joinPath(outDir, "metrics.csv"));
+                hasContent = existing && existing.peek() != std::ifstream::traits_type::eof();
+            }
+            metrics.open(cipc_io::joinPath(outDir, "metrics.csv"), resumed ? std::ios::out | std::ios::app : std::ios::out | std::ios::trunc);
+            if (!metrics) throw std::runtime_error("invalid output directory " + outDir);
+            if (!hasContent)
+                metrics << "frame,step_ms,assembly_ms,linear_ms,ccd_ms,line_search_ms,post_ms,"
+                           "newton,kappa_loops,backtracks,energy_backtracks,intersection_backtracks,"
+                           "max_energy_backtracks_per_newton,newton_steps_over_two_backtracks,"
+                           "mean_alpha,min_alpha,max_alpha,collisions,kappa,min_distance2,"
+                           "ground_contacts,self_contacts,mollified_contacts,matrix_nnz,"
+                           "symbolic_analyses,numeric_factorizations,pardiso_analysis_ms,"
+                           "pardiso_factorization_ms,pardiso_solve_ms,linear_solver_threads,"
+                           "factor_nnz,pcg_iterations,pcg_relative_residual\n";
         }
         cipc_step_stats st{};
+        std::vector<double> xs(3 * (size_t)nv), xts(3 * (size_t)nv);
         for (int step = 0; step < o.steps; ++step) {
             check(cipc_gpu_step(ctx, &st), ctx, "cipc_gpu_step");
+            const int frame = totals.stepIndex;  // IPCSolver.cpp:1104-1106
+            totals.stageMs[0] += st.assemblyMilliseconds;
+            totals.stageMs[1] += st.linearSolveMilliseconds;
+            totals.stageMs[2] += st.ccdMilliseconds;
+            totals.stageMs[3] += st.lineSearchMilliseconds;
+            totals.stageMs[4] += st.postLineSearchMilliseconds;
+            totals.stepMs += st.stepMilliseconds;
+            totals.newtonIterations += st.newtonIterations;
+            totals.collisions += st.collisions;
+            totals.kappa = st.kappa;
+            ++totals.stepIndex;
             if (o.verbose)
-                std::cout << "step " << step << " newton " << st.newtonIterations << " pcg " << st.pcgIterations << " ms " << st.stepMilliseconds
+                std::cout << "step " << frame << " newton " << st.newtonIterations << " pcg " << st.pcgIterations << " ms " << st.stepMilliseconds
                           << std::endl;
-            if (metrics.is_open()) {
-                metrics << std::setprecision(17) << st.frame << ',' << st.stepMilliseconds << ',' << st.assemblyMilliseconds << ','
+            if (o.writeOutput) {
+                if (!cipc_io::writeTimeSummary(outDir, totals)) throw std::runtime_error("cannot write timeCost.txt in " + outDir);
+                metrics << std::setprecision(17) << frame << ',' << st.stepMilliseconds << ',' << st.assemblyMilliseconds << ','
                         << st.linearSolveMilliseconds << ',' << st.ccdMilliseconds << ',' << st.lineSearchMilliseconds << ','
                         << st.postLineSearchMilliseconds << ',' << st.newtonIterations << ',' << st.kappaIterations << ','
                         << st.lineSearchBacktracks << ',' << st.energyBacktracks << ',' << st.intersectionBacktracks << ','
@@ -432,6 +486,14 @@ int main(int argc, char** argv) {
                         << st.maximumAcceptedStep << ',' << st.collisions << ',' << st.kappa << ',' << st.minConstraintDistance2 << ','
                         << st.groundContacts << ',' << st.selfContacts << ',' << st.mollifiedContacts << ',' << 9 * st.matrixBlocks
                         << ",0,0,0,0,0,0,0," << st.pcgIterations << ',' << st.pcgRelativeResidual << '\n';
+                metrics.flush();
+                // checkpoint every tenth step (IPCSolver.cpp:1318-1332)
+                if (o.writeCheckpoints && totals.stepIndex % 10 == 0) {
+                    check(cipc_gpu_get_state(ctx, 0, xs.data()), ctx, "cipc_gpu_get_state");
+                    check(cipc_gpu_get_state(ctx, 3, xts.data()), ctx, "cipc_gpu_get_state");
+                    if (!cipc_io::writeCheckpointTotals(outDir, totals) || !cipc_io::writeVertexState(outDir, xs, xts, nv))
+                        std::cerr << "Warning: failed to save simulation checkpoint" << std::endl;
+                }
             }
         }
         // RESULT line over the first mesh (cipc_headless.cpp:146-175)

@@ -85,7 +85,8 @@ def build(jobs=8, force=False):
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     # the headless runner links only against the C ABI library
-    if force or _stale(HEADLESS, [HEADLESS_SRC, LIB, os.path.join(HERE, "..", "include", "cipc_gpu.h")]):
+    if force or _stale(HEADLESS, [HEADLESS_SRC, os.path.join(HERE, "apps", "runtime_files.h"), LIB,
+                                  os.path.join(HERE, "..", "include", "cipc_gpu.h")]):
         cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), HEADLESS_SRC, "-o", HEADLESS,
                "-L", HERE, "-lcipc_gpu", "-Wl,-rpath,$ORIGIN"]
         r = subprocess.run(cmd, capture_output=True, text=True)
