@@ -1,7 +1,7 @@
 // cipc_headless_gpu: the reference's headless runner (apps/cipc_headless.cpp)
 // on the GPU pipeline.  Same command-line shape, the same scenes where the
 // reference's assets are supplied (--assets DIR: twisting-mat,
-// twisting-mat-soft, cloth-bunny, built as Simulator.cpp:265-382 builds them
+// twisting-mat-soft, cloth-bunny, bunny2, built as Simulator.cpp:265-399 builds them
 // from Assets/scene/parameterSetting.txt and the Gmsh/OBJ meshes), plus the
 // synthetic benchmark scenes (two-cubes, cloth-drape).  Writes metrics.csv
 // with the reference's columns (IPCSolver.cpp:1286-1315; the PARDISO columns
@@ -51,8 +51,8 @@ struct Options {
 
 void usage(const char* exe) {
     std::cout << "Usage: " << exe << " [options]\n"
-              << "  --scene cloth-drape|two-cubes|twisting-mat|twisting-mat-soft|cloth-bunny (default cloth-drape)\n"
-              << "  --assets DIRECTORY      the reference's Assets/ tree (twisting-mat, cloth-bunny)\n"
+              << "  --scene cloth-drape|two-cubes|twisting-mat|twisting-mat-soft|cloth-bunny|bunny2 (default cloth-drape)\n"
+              << "  --assets DIRECTORY      the reference's Assets/ tree (twisting-mat, cloth-bunny, bunny2)\n"
               << "  --steps N\n"
               << "  --cloth N               cloth-drape: N x N cloth vertices (default 128)\n"
               << "  --cells N               cube cells per side (default 10 cloth-drape, 8 two-cubes)\n"
@@ -317,11 +317,20 @@ Scene buildScene(const Options& o) {
         s.btype.assign(s.x.size() / 3, 0);
         Params& p = s.p;
         p.E = 1e5; p.nu = 0.4; p.density = 1000; p.friction = 0.2; p.dt = 0.01; p.newtonThr = 1e-6; p.relDhat = 1e-3;
-    } else if (o.scene == "twisting-mat" || o.scene == "twisting-mat-soft" || o.scene == "cloth-bunny") {
+    } else if (o.scene == "twisting-mat" || o.scene == "twisting-mat-soft" || o.scene == "cloth-bunny" || o.scene == "bunny2") {
         if (o.assets.empty()) throw std::invalid_argument("--scene " + o.scene + " needs --assets (the reference's Assets directory)");
         s.p = loadSettings(o.assets + "/scene/parameterSetting.txt");
         const double zero[3] = {0, 0, 0};
-        if (o.scene == "cloth-bunny") {
+        if (o.scene == "bunny2") {
+            // buildBunny2Scene (Simulator.cpp:382-399): two copies of bunny2.msh at
+            // scale 0.2, the upper one raised by 0.65
+            s.p.E = 1e5;
+            const double up[3] = {0.0, 0.65, 0.0};
+            loadGmsh(o.assets + "/tetrahedraMesh/bunny2.msh", 0.2, up, s.x, s.tets);
+            s.firstMeshVertices = (int)(s.x.size() / 3);
+            loadGmsh(o.assets + "/tetrahedraMesh/bunny2.msh", 0.2, zero, s.x, s.tets);
+            s.btype.assign(s.x.size() / 3, 0);
+        } else if (o.scene == "cloth-bunny") {
             // buildClothOverBunnyScene (Simulator.cpp:332-382): plane1024 rotated by pi/2
             // about x, bunny.msh scaled 0.5 and lowered by 0.5
             s.p.E = 1e4;

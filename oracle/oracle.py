@@ -102,7 +102,7 @@ def lib():
         L.cipc_oracle_hinge.restype = C.c_double
         L.cipc_oracle_hinge.argtypes = [dp, dp, C.c_double, dp, dp]
         L.cipc_oracle_linear_solve.restype = C.c_int
-        L.cipc_oracle_linear_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_int, C.c_double, C.c_int, ip, dp, C.c_int]
+        L.cipc_oracle_linear_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_int, C.c_double, C.c_int, ip, dp, C.c_int, dp]
         _lib = L
     return _lib
 
@@ -351,14 +351,16 @@ def hinge(x, rest, k):
     return e, g, H
 
 
-def linear_solve(nv, rowptr, col, val, rhs, method="pcg", tol=1e-6, max_iter=10000, threads=1):
+def linear_solve(nv, rowptr, col, val, rhs, method="pcg", tol=1e-6, max_iter=10000, threads=1, xyz=None):
     rowptr = np.ascontiguousarray(rowptr, np.int32); col = np.ascontiguousarray(col, np.int32)
     val = np.ascontiguousarray(val, np.float64); rhs = np.ascontiguousarray(rhs, np.float64)
     sol = np.zeros(3 * nv)
     it = C.c_int(0); rr = C.c_double(0)
+    if xyz is not None:
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(3 * nv)
     rc = lib().cipc_oracle_linear_solve(nv, _ip(rowptr), _ip(col), _dp(val), _dp(rhs), _dp(sol),
                                        {"direct": 0, "pcg": 1, "multifrontal": 2}[method], tol, max_iter, C.byref(it), C.byref(rr),
-                                       threads)
+                                       threads, None if xyz is None else _dp(xyz))
     if rc != 0:
         raise RuntimeError("oracle linear solve failed")
     return sol, it.value, rr.value

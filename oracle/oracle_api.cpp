@@ -302,7 +302,8 @@ double cipc_oracle_distance(int kind, const double* pts, double* g, double* H) {
 }
 
 int cipc_oracle_linear_solve(int nv, const int* rowptr, const int* col, const double* val, const double* rhs, double* sol,
-                             int method, double tol, int maxIter, int* iters, double* relres, int threads) {
+                             int method, double tol, int maxIter, int* iters, double* relres, int threads,
+                             const double* xyz) {
     try {
         LinearSystem ls;
         int n = 3 * nv;
@@ -312,7 +313,7 @@ int cipc_oracle_linear_solve(int nv, const int* rowptr, const int* col, const do
         ls.rhs.assign(rhs, rhs + n);
         SolverOptions o;
         o.linear = method; o.pcgRelTol = tol; o.pcgMaxIter = maxIter; o.threads = threads > 0 ? threads : 1;
-        solveSystem(ls, nv, o);
+        solveSystem(ls, nv, o, xyz);
         std::memcpy(sol, ls.sol.data(), n * sizeof(double));
         if (iters) *iters = ls.pcgIters;
         if (relres) *relres = ls.pcgRelResidual;

@@ -73,9 +73,10 @@ double cipc_oracle_distance(int kind, const double* pts, double* g, double* H);
 /* one hinge bending element (HingeBending.cpp:76-106 + makePD) */
 double cipc_oracle_hinge(const double* x12, const double* rest12, double k, double* g, double* H);
 /* linear solve of a given lower CSR system (n scalar rows): method 0 envelope Cholesky, 1 block-Jacobi
-   PCG, 2 multifrontal Cholesky on `threads` threads */
+   PCG, 2 multifrontal Cholesky on `threads` threads (xyz: vertex positions for its ordering, or null) */
 int cipc_oracle_linear_solve(int nv, const int* rowptr, const int* col, const double* val, const double* rhs,
-                             double* sol, int method, double tol, int maxIter, int* iters, double* relres, int threads);
+                             double* sol, int method, double tol, int maxIter, int* iters, double* relres, int threads,
+                             const double* xyz);
 double cipc_oracle_total_energy(void* h);
 
 #ifdef __cplusplus

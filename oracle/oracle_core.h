@@ -245,8 +245,9 @@ struct LinearSystem {
     double pcgRelResidual = 0;
 };
 void assembleSystem(const Mesh& m, const BHessian& BH, const std::vector<V3>& g, LinearSystem& ls);
-void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o);
-void multifrontalSolve(LinearSystem& ls, int nv, int threads);
+// xyz (3 nv positions, or null) lets the multifrontal ordering cut by coordinates
+void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o, const double* xyz = nullptr);
+void multifrontalSolve(LinearSystem& ls, int nv, int threads, const double* xyz);
 int solveIPCStep(Mesh& m, BroadPhase& bp, StepStats& stats, int stepIndex, const SolverOptions& o);
 
 }  // namespace oracle

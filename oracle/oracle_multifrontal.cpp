@@ -66,12 +66,14 @@ struct Node {
     double work = 0;         // factorisation flops of the subtree (for load balance)
 };
 
-// Recursive bisection by breadth-first level sets: a pseudo-peripheral root,
-// the level holding the median vertex, and of that level only the vertices
-// adjacent to the next level as the separator.
+// Recursive bisection.  Two candidate separators per connected subgraph, the
+// smaller one kept: breadth-first level sets from a pseudo-peripheral root
+// (of one level, the vertices adjacent to the next), and, when vertex
+// positions are given, cuts at the median coordinate along each axis (of one
+// side, the vertices adjacent to the other).
 class Dissection {
 public:
-    explicit Dissection(const Graph& g) : g_(g), in_(g.n(), 0), level_(g.n(), -1) {}
+    Dissection(const Graph& g, const double* xyz) : g_(g), xyz_(xyz), in_(g.n(), 0), level_(g.n(), -1), side_(g.n(), -1) {}
     std::vector<Node> nodes;
 
     std::vector<int> dissect(const std::vector<int>& S) {
@@ -145,6 +147,7 @@ public:
             else if (l > L) B.push_back(v);
             else (touchesNext(v) ? sep : A).push_back(v);
         }
+        if (xyz_) geometricCut(S, tag, A, B, sep);
         if (2 * sep.size() > S.size()) return {leaf(S)};
         std::vector<int> kids;
         if (!A.empty()) { auto r = dissect(A); kids.insert(kids.end(), r.begin(), r.end()); }
@@ -158,8 +161,58 @@ public:
 
 private:
     const Graph& g_;
-    std::vector<int> in_, level_;
+    const double* xyz_;
+    std::vector<int> in_, level_, side_;
     int stamp_ = 0;
+
+    // the coordinate cuts at the median along each axis; the one with the
+    // smallest separator replaces (A, B, sep) when that separator is smaller
+    void geometricCut(const std::vector<int>& S, int tag, std::vector<int>& A, std::vector<int>& B, std::vector<int>& sep) {
+        const size_t half = S.size() / 2;
+        if (half == 0) return;
+        std::vector<int> T = S, bestA, bestB, bestSep;
+        bool found = false;
+        auto touchesOther = [&](int v) {
+            for (int k = g_.ptr[v]; k < g_.ptr[v + 1]; ++k) {
+                int u = g_.adj[k];
+                if (in_[u] == tag && side_[u] != side_[v]) return true;
+            }
+            return false;
+        };
+        for (int ax = 0; ax < 3; ++ax) {
+            std::nth_element(T.begin(), T.begin() + half, T.end(), [&](int a, int b) {
+                const double ka = xyz_[3 * a + ax], kb = xyz_[3 * b + ax];
+                return ka < kb || (ka == kb && a < b);
+            });
+            for (size_t i = 0; i < T.size(); ++i) side_[T[i]] = i < half ? 2 * tag : 2 * tag + 1;
+            std::vector<int> a0, a1, b0, b1;  // inner and boundary vertices of either side
+            for (size_t i = 0; i < T.size(); ++i) {
+                const int v = T[i];
+                const bool edge = touchesOther(v);
+                if (i < half) (edge ? a1 : a0).push_back(v);
+                else (edge ? b1 : b0).push_back(v);
+            }
+            const size_t size = std::min(a1.size(), b1.size());
+            if (size >= (found ? bestSep.size() : sep.size())) continue;
+            found = true;
+            if (a1.size() <= b1.size()) {
+                bestA = std::move(a0);
+                bestSep = std::move(a1);
+                bestB = std::move(b0);
+                bestB.insert(bestB.end(), b1.begin(), b1.end());
+            } else {
+                bestA = std::move(a0);
+                bestA.insert(bestA.end(), a1.begin(), a1.end());
+                bestSep = std::move(b1);
+                bestB = std::move(b0);
+            }
+        }
+        if (found) {
+            A = std::move(bestA);
+            B = std::move(bestB);
+            sep = std::move(bestSep);
+        }
+    }
 
     int leaf(const std::vector<int>& verts) {
         Node n;
@@ -365,10 +418,10 @@ struct Factor {
 
 class Multifrontal {
 public:
-    Multifrontal(const LinearSystem& ls, int nv, int threads) : nv_(nv), threads_(std::max(1, threads)) {
+    Multifrontal(const LinearSystem& ls, int nv, int threads, const double* xyz) : nv_(nv), threads_(std::max(1, threads)) {
         fullSymmetric(ls);
         Graph g = vertexGraph(ls, nv);
-        Dissection d(g);
+        Dissection d(g, xyz);
         std::vector<int> all(nv);
         for (int v = 0; v < nv; ++v) all[v] = v;
         roots_ = d.dissect(all);
@@ -584,8 +637,9 @@ private:
 
 }  // namespace
 
-void multifrontalSolve(LinearSystem& ls, int nv, int threads) {
-    Multifrontal mf(ls, nv, threads);
+void multifrontalSolve(LinearSystem& ls, int nv, int threads, const double* xyz) {
+    if (nv <= 0) { ls.sol.clear(); return; }
+    Multifrontal mf(ls, nv, threads, xyz);
     mf.factor();
     ls.sol = ls.rhs;
     mf.solve(ls.sol);

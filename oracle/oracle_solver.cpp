@@ -237,9 +237,11 @@ static void pcgSolve(LinearSystem& ls, int nv, double tol, int maxIter) {
     ls.sol = x;
 }
 
-void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o) {
+static_assert(sizeof(V3) == 3 * sizeof(double), "positions are passed as packed xyz triples");
+
+void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o, const double* xyz) {
     if (o.linear == 0) directSolve(ls, nv);
-    else if (o.linear == 2) multifrontalSolve(ls, nv, o.threads);
+    else if (o.linear == 2) multifrontalSolve(ls, nv, o.threads, xyz);
     else pcgSolve(ls, nv, o.pcgRelTol, o.pcgMaxIter);
     for (double v : ls.sol)
         if (!std::isfinite(v)) throw std::runtime_error("linear solve produced a non-finite direction");
@@ -348,7 +350,7 @@ int solveBarrierSubproblem(Mesh& m, BroadPhase& bp, double kappa, StepStats& st,
         st.collisions += computeGradientAndHessian(m, grad, BH, o);
         assembleSystem(m, BH, grad, ls);
         st.matrixNnz = std::max(st.matrixNnz, ls.nnz);
-        solveSystem(ls, m.nv(), o);
+        solveSystem(ls, m.nv(), o, &m.x[0].x);
         st.pcgIterations += ls.pcgIters;
         for (int v = 0; v < m.nv(); ++v) dir[v] = V3(ls.sol[3 * v], ls.sol[3 * v + 1], ls.sol[3 * v + 2]);
         double thr = m.newtonThr * std::sqrt(m.bboxDiag2) * m.dt;

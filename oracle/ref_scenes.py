@@ -127,3 +127,19 @@ def cloth_bunny(hinge=False):
     tets = tets + len(xc)
     btype = np.zeros(len(x), np.int32)
     return dict(x=x, tets=tets, tris=tris, btype=btype, params=p, bbox_min=lo.tolist(), bbox_max=hi.tolist())
+
+
+def bunny2():
+    """buildBunny2Scene (Simulator.cpp:382-399): two copies of bunny2.msh at
+    scale 0.2, offset (0, 0.65, 0) and (0, 0, 0), Young's modulus 1e5, the
+    rest from parameterSetting.txt."""
+    p = parameter_settings()
+    p["E"] = 1e5
+    path = os.path.join(REFERENCE_ASSETS, "tetrahedraMesh/bunny2.msh")
+    xa, ta = load_gmsh(path, 0.2, (0.0, 0.65, 0.0))
+    xb, tb = load_gmsh(path, 0.2, (0.0, 0.0, 0.0))
+    x = np.concatenate([xa, xb])
+    tets = np.concatenate([ta, tb + len(xa)]).astype(np.int32)
+    btype = np.zeros(len(x), np.int32)
+    return dict(x=x, tets=tets, tris=np.zeros((0, 3), np.int32), btype=btype, params=p,
+                bbox_min=x.min(axis=0).tolist(), bbox_max=x.max(axis=0).tolist())

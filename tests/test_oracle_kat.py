@@ -104,3 +104,16 @@ def test_cloth_bunny_hinge_bending_one_step(oracle_mod):
     assert st["energyBacktracks"] == k["energy_backtracks"]
     assert st["intersectionBacktracks"] == k["intersection_backtracks"]
     assert st["matrixNnz"] == k["matrix_nnz"]
+
+
+@needs_assets
+def test_bunny2_one_step(oracle_mod):
+    # the two-bunny PARDISO benchmark scene: its documented first step
+    sc = ref_scenes.bunny2()
+    k = KAT["bunny2_1_step"]
+    assert len(sc["x"]) == k["vertices"] and len(sc["tets"]) == k["tets"]
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=os.cpu_count() or 1)
+    assert o.nsf == k["surface_faces"]
+    st = o.step()
+    assert st["newton"] == k["newton"]
+    assert st["matrixNnz"] == k["matrix_nnz"]

@@ -75,13 +75,15 @@ def test_multifrontal_matches_dense_solve(name, graph):
     b = rng.standard_normal(3 * nv)
     rp, col, val = _lower_csr(A)
     x_ref = np.linalg.solve(A, b)
-    sols = []
-    for threads in (1, 3, 8):
-        x, _, _ = oracle.linear_solve(nv, rp, col, val, b, method="multifrontal", threads=threads)
-        assert np.abs(x - x_ref).max() <= 1e-10 * np.abs(x_ref).max(), (name, threads)
-        sols.append(x)
-    # every entry takes its updates in pivot order whatever the thread count
-    assert all(np.array_equal(sols[0], s) for s in sols[1:])
+    # orderings without positions (level sets) and with them (coordinate cuts)
+    for xyz in (None, rng.random((nv, 3))):
+        sols = []
+        for threads in (1, 3, 8):
+            x, _, _ = oracle.linear_solve(nv, rp, col, val, b, method="multifrontal", threads=threads, xyz=xyz)
+            assert np.abs(x - x_ref).max() <= 1e-10 * np.abs(x_ref).max(), (name, threads)
+            sols.append(x)
+        # every entry takes its updates in pivot order whatever the thread count
+        assert all(np.array_equal(sols[0], s) for s in sols[1:])
 
 
 def test_multifrontal_rejects_an_indefinite_matrix():
