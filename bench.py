@@ -201,6 +201,15 @@ def pcg_iteration_bytes(counts, mixed, factor):
     return b
 
 
+def host_threads():
+    """Host cores this process may run on (the affinity mask, which a
+    container's CPU set narrows; the machine's count where there is none)."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def oracle_at_settled_frame(args, scene, threads):
     """The FP64 oracle on the bench scene, at the frame the GPU arm's warm-up
     starts from when a saved state exists.
@@ -226,7 +235,7 @@ def frames(first, n, restored):
 
 def cpu_baseline(args, scene, seconds, steps_cap=50):
     """The FP64 oracle on the same scene, all host cores, bounded by time."""
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     o, f0 = oracle_at_settled_frame(args, scene, threads)
     t0 = time.time()
     n = 0
@@ -245,7 +254,7 @@ def run_reference(args, world, rank):
         return
     import cipc
     scene = make_scene(args, cipc)
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     o, f0 = oracle_at_settled_frame(args, scene, threads)
     budget = 150.0
     t0 = time.time()

@@ -148,7 +148,8 @@ public:
             else (touchesNext(v) ? sep : A).push_back(v);
         }
         if (xyz_) geometricCut(S, tag, A, B, sep);
-        if (2 * sep.size() > S.size()) return {leaf(S)};
+        // no split worth having (a near-clique): one dense front
+        if (2 * sep.size() > S.size() || A.empty() || B.empty()) return {leaf(S)};
         std::vector<int> kids;
         if (!A.empty()) { auto r = dissect(A); kids.insert(kids.end(), r.begin(), r.end()); }
         if (!B.empty()) { auto r = dissect(B); kids.insert(kids.end(), r.begin(), r.end()); }
