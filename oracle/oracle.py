@@ -53,6 +53,7 @@ class Stats(C.Structure):
         ("acceptedStepSum", C.c_double), ("minStep", C.c_double), ("maxStep", C.c_double),
         ("groundContacts", C.c_longlong), ("selfContacts", C.c_longlong),
         ("mollifiedContacts", C.c_longlong), ("matrixNnz", C.c_longlong), ("pcgIterations", C.c_longlong),
+        ("linearSolves", C.c_longlong),
     ]
 
     def as_dict(self):

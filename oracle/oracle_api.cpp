@@ -111,6 +111,7 @@ int cipc_oracle_step(void* h, cipc_oracle_stats* out, char* err, int errlen) {
             out->acceptedStepSum = st.acceptedStepSum; out->minStep = st.minStep; out->maxStep = st.maxStep;
             out->groundContacts = st.groundContacts; out->selfContacts = st.selfContacts;
             out->mollifiedContacts = st.mollifiedContacts; out->matrixNnz = st.matrixNnz; out->pcgIterations = st.pcgIterations;
+            out->linearSolves = st.linearSolves;
         }
         return 0;
     } catch (const std::exception& e) {

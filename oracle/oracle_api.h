@@ -24,7 +24,7 @@ typedef struct {
     double bboxMin[3], bboxMax[3];
     int nsoft; const int* softIdx; double softW; int softMotion; double softRate;
     int ndir; const int* dirIdx; int dirMotion; double dirRate;
-    int linear;           /* 0 direct, 1 block-Jacobi PCG */
+    int linear;           /* 0 envelope Cholesky, 1 block-Jacobi PCG, 2 multifrontal Cholesky */
     double pcgRelTol;
     int threads;
 } cipc_oracle_scene;
@@ -33,7 +33,7 @@ typedef struct {
     int frame, newton, kappaIters, backtracks, energyBacktracks, intersectionBacktracks;
     int maxEnergyBacktracksPerNewton, newtonOverTwo;
     double collisions, kappa, minDist2, acceptedStepSum, minStep, maxStep;
-    long long groundContacts, selfContacts, mollifiedContacts, matrixNnz, pcgIterations;
+    long long groundContacts, selfContacts, mollifiedContacts, matrixNnz, pcgIterations, linearSolves;
 } cipc_oracle_stats;
 
 void* cipc_oracle_create(const cipc_oracle_scene* s, char* err, int errlen);

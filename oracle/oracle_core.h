@@ -169,6 +169,7 @@ struct StepStats {
     double collisions = 0, kappa = 0, minDist2 = -1, acceptedStepSum = 0, minStep = 1, maxStep = 0;
     long long groundContacts = 0, selfContacts = 0, mollifiedContacts = 0, matrixNnz = 0;
     long long pcgIterations = 0;
+    long long linearSolves = 0;  // numericFactorizations of IPCStepStats (IPCSolver.cpp:1042)
 };
 
 struct SolverOptions {

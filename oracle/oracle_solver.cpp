@@ -352,6 +352,7 @@ int solveBarrierSubproblem(Mesh& m, BroadPhase& bp, double kappa, StepStats& st,
         st.matrixNnz = std::max(st.matrixNnz, ls.nnz);
         solveSystem(ls, m.nv(), o, &m.x[0].x);
         st.pcgIterations += ls.pcgIters;
+        ++st.linearSolves;
         for (int v = 0; v < m.nv(); ++v) dir[v] = V3(ls.sol[3 * v], ls.sol[3 * v + 1], ls.sol[3 * v + 2]);
         double thr = m.newtonThr * std::sqrt(m.bboxDiag2) * m.dt;
         if (infNorm(dir) < thr) break;
