@@ -33,7 +33,7 @@ def dd():
     d = tempfile.mkdtemp()
     so = os.path.join(d, "libdd.so")
     subprocess.run([nvcc, "-O2", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-I", SRC, "-o", so,
-                    os.path.join(HERE, "distance_harness.cu")], check=True)
+                    os.path.join(HERE, "device_math_harness.cu")], check=True)
     L = C.CDLL(so)
     L.dd_grad_hess.restype = C.c_int
     L.dd_grad_hess.argtypes = [C.c_int, dp, dp, dp]
