@@ -225,7 +225,10 @@ def oracle_at_settled_frame(args, scene, threads):
     if args.scene == "cloth_drape":
         path = os.path.join(ROOT, "oracle", "states", f"cloth_drape_{args.cloth}_frame{args.settle_steps}.npz")
         if os.path.exists(path):
-            return o, o.restore_state(path)
+            try:
+                return o, o.restore_state(path)
+            except ValueError:  # saved from another version of the scene: time from frame 0
+                pass
     return o, 0
 
 
