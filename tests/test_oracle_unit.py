@@ -177,3 +177,16 @@ def test_hinge_energy_invariants(oracle_mod):
     assert abs(er - e) <= 1e-12 * abs(e)
     es, _, _ = oracle_mod.hinge(x[[0, 1, 3, 2]], rest[[0, 1, 3, 2]], 2.0)
     assert abs(es - e) <= 1e-12 * abs(e)
+
+
+def test_exact_solve_steps_a_pile_of_rotated_cubes(oracle_mod):
+    """With an exact linear solve the first free-fall step is an exact
+    translation, which keeps the faces of the rotated cubes coplanar up to
+    rounding; the intersection test must not report the edges and triangles
+    of one face as intersecting (or the line search gives up at frame 0)."""
+    sc = cipc.scene_pile(8, 12)
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=8)
+    assert not o.intersected()
+    for _ in range(2):
+        st = o.step()
+    assert st["intersectionBacktracks"] == 0
