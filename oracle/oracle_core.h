@@ -11,6 +11,7 @@
 #include <array>
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <string>
 #include <thread>
 #include <utility>
@@ -172,11 +173,15 @@ struct StepStats {
     long long linearSolves = 0;  // numericFactorizations of IPCStepStats (IPCSolver.cpp:1042)
 };
 
+struct MultifrontalCache;  // ordering and symbolic factorisation of the last pattern (oracle_multifrontal.cpp)
 struct SolverOptions {
     int linear = 0;           // 0 = envelope Cholesky, 1 = block-Jacobi PCG, 2 = multifrontal Cholesky
     double pcgRelTol = 1e-6;  // LinearSolverOptions.h:15
     int pcgMaxIter = 10000;   // LinearSolverOptions.h:16
     int threads = 1;
+    // the multifrontal solve keeps its analysis here and reuses it while the
+    // matrix pattern is unchanged, as PARDISO keeps phase 11 (PardisoSolver.cpp:182-248)
+    mutable std::shared_ptr<MultifrontalCache> mfCache;
 };
 
 // ---- simple deterministic parallel-for over index chunks ----
@@ -248,7 +253,8 @@ struct LinearSystem {
 void assembleSystem(const Mesh& m, const BHessian& BH, const std::vector<V3>& g, LinearSystem& ls);
 // xyz (3 nv positions, or null) lets the multifrontal ordering cut by coordinates
 void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o, const double* xyz = nullptr);
-void multifrontalSolve(LinearSystem& ls, int nv, int threads, const double* xyz);
+void multifrontalSolve(LinearSystem& ls, int nv, int threads, const double* xyz, MultifrontalCache* cache = nullptr);
+std::shared_ptr<MultifrontalCache> newMultifrontalCache();
 int solveIPCStep(Mesh& m, BroadPhase& bp, StepStats& stats, int stepIndex, const SolverOptions& o);
 
 }  // namespace oracle

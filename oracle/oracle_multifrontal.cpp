@@ -411,6 +411,17 @@ bool partialCholesky(double* F, int m, int p, Pool* pool) {
     return true;
 }
 
+}  // namespace
+
+// the analysis of the last pattern: its rows and columns, the assembly tree
+struct MultifrontalCache {
+    std::vector<int> rowPtr, col;
+    std::vector<Node> nodes;
+    std::vector<int> roots, post;
+};
+
+namespace {
+
 struct Factor {
     std::vector<int> idx;   // scalar indices of the front's rows
     std::vector<double> L;  // m x p, column-major (rows from the diagonal down used)
@@ -419,8 +430,15 @@ struct Factor {
 
 class Multifrontal {
 public:
-    Multifrontal(const LinearSystem& ls, int nv, int threads, const double* xyz) : nv_(nv), threads_(std::max(1, threads)) {
+    Multifrontal(const LinearSystem& ls, int nv, int threads, const double* xyz, MultifrontalCache* cache)
+        : nv_(nv), threads_(std::max(1, threads)) {
         fullSymmetric(ls);
+        if (cache && cache->rowPtr == ls.rowPtr && cache->col == ls.col) {
+            nodes_ = cache->nodes;
+            roots_ = cache->roots;
+            post_ = cache->post;
+            return;
+        }
         Graph g = vertexGraph(ls, nv);
         Dissection d(g, xyz);
         std::vector<int> all(nv);
@@ -429,6 +447,13 @@ public:
         nodes_ = std::move(d.nodes);
         postorder();
         symbolic(g);
+        if (cache) {
+            cache->rowPtr = ls.rowPtr;
+            cache->col = ls.col;
+            cache->nodes = nodes_;
+            cache->roots = roots_;
+            cache->post = post_;
+        }
     }
 
     void factor() {
@@ -638,9 +663,11 @@ private:
 
 }  // namespace
 
-void multifrontalSolve(LinearSystem& ls, int nv, int threads, const double* xyz) {
+std::shared_ptr<MultifrontalCache> newMultifrontalCache() { return std::make_shared<MultifrontalCache>(); }
+
+void multifrontalSolve(LinearSystem& ls, int nv, int threads, const double* xyz, MultifrontalCache* cache) {
     if (nv <= 0) { ls.sol.clear(); return; }
-    Multifrontal mf(ls, nv, threads, xyz);
+    Multifrontal mf(ls, nv, threads, xyz, cache);
     mf.factor();
     ls.sol = ls.rhs;
     mf.solve(ls.sol);

@@ -241,7 +241,10 @@ static_assert(sizeof(V3) == 3 * sizeof(double), "positions are passed as packed 
 
 void solveSystem(LinearSystem& ls, int nv, const SolverOptions& o, const double* xyz) {
     if (o.linear == 0) directSolve(ls, nv);
-    else if (o.linear == 2) multifrontalSolve(ls, nv, o.threads, xyz);
+    else if (o.linear == 2) {
+        if (!o.mfCache) o.mfCache = newMultifrontalCache();
+        multifrontalSolve(ls, nv, o.threads, xyz, o.mfCache.get());
+    }
     else pcgSolve(ls, nv, o.pcgRelTol, o.pcgMaxIter);
     for (double v : ls.sol)
         if (!std::isfinite(v)) throw std::runtime_error("linear solve produced a non-finite direction");
