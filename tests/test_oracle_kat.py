@@ -43,6 +43,20 @@ def test_twisting_mat_one_step_multifrontal(oracle_mod):
 
 
 @needs_assets
+def test_twisting_mat_five_steps_multifrontal(oracle_mod):
+    # five steps through the multifrontal solve, which reuses its analysis
+    # while the pattern holds (no contact here, so after the first solve)
+    o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=False), linear="multifrontal", threads=8)
+    for _ in range(5):
+        st = o.step()
+    x = o.get("x")
+    k = KAT["twisting_mat_5_steps"]
+    assert st["newton"] == k["newton_last"]
+    assert st["matrixNnz"] == k["matrix_nnz"]
+    assert abs((x * x).sum() - float(k["squared_norm_sum_prefix"])) < 1e-12
+
+
+@needs_assets
 def test_twisting_mat_soft_five_steps(oracle_mod):
     o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=True), linear="direct", threads=8)
     for _ in range(5):
