@@ -85,6 +85,7 @@ def lib():
         L.cipc_gpu_set_state.argtypes = [vp, C.c_int, _dp]
         L.cipc_gpu_get_scalars.argtypes = [vp, _dp]
         L.cipc_gpu_set_kappa.argtypes = [vp, C.c_double]
+        L.cipc_gpu_set_intersection_rule.argtypes = [vp, C.c_int]
         L.cipc_gpu_get_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.cipc_gpu_get_surface.argtypes = [vp, _ip, _ip, _ip]
         L.cipc_gpu_build_collision_sets.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -118,7 +119,7 @@ def lib():
 
 EXPORTED_SYMBOLS = [
     "cipc_gpu_create", "cipc_gpu_destroy", "cipc_gpu_last_error", "cipc_gpu_create_error", "cipc_gpu_step",
-    "cipc_gpu_get_state", "cipc_gpu_set_state", "cipc_gpu_get_scalars", "cipc_gpu_set_kappa", "cipc_gpu_get_counts",
+    "cipc_gpu_get_state", "cipc_gpu_set_state", "cipc_gpu_get_scalars", "cipc_gpu_set_kappa", "cipc_gpu_set_intersection_rule", "cipc_gpu_get_counts",
     "cipc_gpu_get_surface", "cipc_gpu_build_collision_sets", "cipc_gpu_get_active_sets", "cipc_gpu_friction_init",
     "cipc_gpu_assemble", "cipc_gpu_export_matrix", "cipc_gpu_solve", "cipc_gpu_energy", "cipc_gpu_step_bounds",
     "cipc_gpu_intersected", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
@@ -281,6 +282,11 @@ class Simulator:
 
     def set_kappa(self, k):
         self._chk(self.L.cipc_gpu_set_kappa(self.h, float(k)))
+
+    def set_intersection_rule(self, rule):
+        """'tolerant' (default) or 'reference' (the reference's exact
+        segment-triangle coplanarity rule)."""
+        self._chk(self.L.cipc_gpu_set_intersection_rule(self.h, {"tolerant": 0, "reference": 1}[rule]))
 
     def surface(self):
         f = np.zeros((self.nsf, 3), np.int32); v = np.zeros(self.nsv, np.int32); e = np.zeros((self.nse, 2), np.int32)

@@ -92,6 +92,12 @@ struct Ctx {
     cudaStream_t s = nullptr;
     std::string lastError;
     int stepIndex = 0;
+    // relative coplanarity tolerance of the segment-triangle intersection
+    // test (COPLANAR_TOL); 0 selects the reference's exact rule
+    double coplanarTol = 1e-12;
+    // a tensor-core completion wait timed out: the network's forward pass is
+    // refused for the rest of the context's life
+    bool tcFault = false;
 
     // host mirrors needed by the driver
     std::vector<int> hBtype, hSoftIdx, hDirIdx;

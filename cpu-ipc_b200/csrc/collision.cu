@@ -510,7 +510,8 @@ __global__ void fullEEKernel(int ne, const int* edges, const int* btype, const d
     }
 }
 
-__global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, BvhView tree, int* flag, int* status) {
+__global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, BvhView tree, double coplanarTol,
+                                int* flag, int* status) {
     CIPC_KERNEL_LOOP(f, nsf) {
         int f0 = faces[3 * f], f1 = faces[3 * f + 1], f2 = faces[3 * f + 2];
         d3 a = ld3(x, f0), b = ld3(x, f1), c = ld3(x, f2);
@@ -523,7 +524,7 @@ __global__ void intersectKernel(int nsf, const int* faces, const int* edges, con
             int e0 = edges[2 * e], e1 = edges[2 * e + 1];
             if (e0 == f0 || e0 == f1 || e0 == f2 || e1 == f0 || e1 == f1 || e1 == f2) return;
             if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
-            if (segTriIntersect(ld3(x, e0), ld3(x, e1), a, b, c)) hit = true;
+            if (segTriIntersect(ld3(x, e0), ld3(x, e1), a, b, c, coplanarTol)) hit = true;
         });
         if (hit) atomicOr(flag, 1);
     }
@@ -623,6 +624,7 @@ void buildCollisionSets(Ctx& c, bool rehash) {
         int caps[6] = {(int)std::max<size_t>(c.ccdPT.cap, 1024), (int)std::max<size_t>(c.kPT.cap, 1024), (int)std::max<size_t>(c.kPPE.cap, 1024),
                        (int)std::max<size_t>(c.ccdEE.cap, 1024), (int)std::max<size_t>(c.kEE.cap, 1024), (int)std::max<size_t>(c.kMoll.cap, 1024)};
         int cnt[6];
+        bool fits = false;
         for (int attempt = 0; attempt < 4; ++attempt) {
             c.ccdPT.reserve(caps[0]); c.kPT.reserve(caps[1]); c.kPPE.reserve(caps[2]);
             c.ccdEE.reserve(caps[3]); c.kEE.reserve(caps[4]); c.kMoll.reserve(caps[5]);
@@ -641,14 +643,17 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             CIPC_CUDA(cudaGetLastError());
             CIPC_CUDA(cudaMemcpyAsync(cnt, c.counters.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
             CIPC_CUDA(cudaStreamSynchronize(c.s));
-            bool ok = true;
+            fits = true;
             for (int k = 0; k < 6; ++k)
-                if (cnt[k] > caps[k]) { caps[k] = cnt[k] + cnt[k] / 2 + 1024; ok = false; }
-            if (ok) break;
-            int st = 0;  // clear the capacity bit before retrying
+                if (cnt[k] > caps[k]) { caps[k] = cnt[k] + cnt[k] / 2 + 1024; fits = false; }
+            if (fits || attempt == 3) break;
+            int st = 0;  // clear the capacity bit before retrying (only when another attempt follows)
             CIPC_CUDA(cudaMemcpyAsync(c.status.p, &st, sizeof(int), cudaMemcpyHostToDevice, c.s));
         }
         checkStatus(c, "active set");
+        // the counts size the sorts and decodes below: never past what the
+        // last launch could write
+        if (!fits) throw std::runtime_error("active-set candidate counts exceed their buffers after four attempts");
         c.nCcdPT = cnt[0]; c.nPT = cnt[1]; c.nPPERaw = cnt[2]; c.nCcdEE = cnt[3]; c.nEE = cnt[4]; c.nMoll = cnt[5];
         int mx = std::max(std::max(std::max(cnt[0], cnt[1]), std::max(cnt[2], cnt[3])), std::max(cnt[4], cnt[5]));
         c.kTmp.reserve(std::max(mx, 1));
@@ -692,7 +697,8 @@ bool isIntersected(Ctx& c) {
     if (c.nGround)
         launch(groundIntersectKernel, blocksFor(c.nGround), TB, 0, c.s, c.nGround, c.ground, c.x, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2],
                                                                    c.P.groundD, c.counters.p + 7);
-    if (c.nsf) launch(intersectKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, view(c.edgeTree), c.counters.p + 7, c.status);
+    if (c.nsf) launch(intersectKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, view(c.edgeTree), c.coplanarTol, c.counters.p + 7,
+                            c.status);
     int f = 0;
     CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaStreamSynchronize(c.s));

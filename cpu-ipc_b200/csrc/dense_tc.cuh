@@ -178,12 +178,19 @@ __global__ void __launch_bounds__(THREADS) denseTcKernel(int n, G gather, E emit
             mmaCommit(&mbar);
         }
         const bool done = mbarWait(&mbar, phase);
-        phase ^= 1u;
         // one decision for the whole CTA, so that no thread is left at a barrier
         if (!__syncthreads_and(done)) {
-            if (tid == 0) atomicOr(status, timeoutBit);
+            // the committed MMAs may still read sA/sB and write the
+            // accumulator: a second bounded wait lets a late completion drain
+            // before the tensor memory is freed below.  The host treats the
+            // status bit as fatal for the context either way.
+            if (tid == 0) {
+                atomicOr(status, timeoutBit);
+                mbarWait(&mbar, phase);
+            }
             break;
         }
+        phase ^= 1u;
         fenceAfterSync();
         float acc[32];
         tmemLoad32(dTmem + ((uint32_t)(warp * 32) << 16), acc);

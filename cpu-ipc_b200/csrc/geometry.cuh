@@ -174,18 +174,22 @@ __device__ __forceinline__ double det3c(d3 c0, d3 c1, d3 c2) {
     return c0.x * (c1.y * c2.z - c2.y * c1.z) - c1.x * (c0.y * c2.z - c2.y * c0.z) + c2.x * (c0.y * c1.z - c1.y * c0.z);
 }
 
-// Coplanar pairs are skipped as in the reference (IglUtils::segTriIntersect),
-// and so is a segment whose two plane distances are both within COPLANAR_TOL
-// of zero relative to |n| times its reach from t0: rounding on rotated meshes
-// must not report the edges and triangles of one flat face as intersecting.
+// Coplanar pairs are skipped as in the reference (IglUtils::segTriIntersect).
+// With coplanarTol > 0 so is a segment whose two plane distances are both
+// within coplanarTol of zero relative to |n| times its reach from t0:
+// rounding on rotated meshes must not report the edges and triangles of one
+// flat face as intersecting.  coplanarTol = 0 is the reference's exact rule
+// (signs of the plane distances and det == 0 only).
 constexpr double COPLANAR_TOL = 1e-12;
-__device__ __forceinline__ bool segTriIntersect(d3 e0, d3 e1, d3 t0, d3 t1, d3 t2) {
+__device__ __forceinline__ bool segTriIntersect(d3 e0, d3 e1, d3 t0, d3 t1, d3 t2, double coplanarTol) {
     d3 c0 = t1 - t0, c1 = t2 - t0, c2 = e0 - e1;
     d3 n = cross(c0, c1);
     const double d0 = dot(n, e0 - t0), d1 = dot(n, e1 - t0);
     if (d0 * d1 > 0.0) return false;
-    const double tol = COPLANAR_TOL * sqrt(sqn(n)) * fmax(sqrt(sqn(e0 - t0)), sqrt(sqn(e1 - t0)));
-    if (fabs(d0) <= tol && fabs(d1) <= tol) return false;
+    if (coplanarTol > 0.0) {
+        const double tol = coplanarTol * sqrt(sqn(n)) * fmax(sqrt(sqn(e0 - t0)), sqrt(sqn(e1 - t0)));
+        if (fabs(d0) <= tol && fabs(d1) <= tol) return false;
+    }
     double det = det3c(c0, c1, c2);
     if (det == 0.0) return false;
     d3 rhs = e0 - t0;

@@ -897,6 +897,7 @@ static_assert(mpWe(0) % 8 == 0 && mpWh(0) % 8 == 0 && MP_LAYER % 8 == 0,
 
 void mpnnForward(Ctx& c) {
     if (!c.mpReady) throw InvalidArgument("no network weights set");
+    if (c.tcFault) throw std::runtime_error("a tensor-core wait timed out earlier on this context; recreate it to use the learned preconditioner");
     int nv = c.nv;
     DynView d = dynView(c);
     size_t es = (size_t)std::max(c.nnzb, 1), ed = (size_t)std::max(c.nDynB, 1);

@@ -1577,18 +1577,20 @@ int pcgSolve(Ctx& c) { return c.mixed ? pcgSolveMixed(c) : pcgSolve64(c); }
 // arena) or a loop that must not pay allocation latency.  The caller passes
 // device pointers for the matrix, right-hand side and solution; every scratch
 // vector lives in the file-scope array below.  The array is sized for at
-// most CIPC_NOALLOC_MAX_ROWS block rows (8.2 MB) and every GPU that loads
-// this library keeps it until the process exits.  All calls share it and it
-// keeps the last call's contents, so calls that overlap on the GPU (two
-// streams, two host threads) race; serialise them.
+// most CIPC_NOALLOC_MAX_ROWS block rows (NOALLOC_DOUBLES doubles: 8,008,064
+// bytes, 7.6 MiB) and every GPU that loads this library keeps it until the
+// process exits.  All calls share it and it keeps the last call's contents,
+// so calls that overlap on the GPU (two streams, two host threads) race;
+// serialise them.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int NOALLOC_MAX_ROWS = 32768;
 constexpr int NOALLOC_PARTS = 3 * 512;
 // r, z, p, Ap (3 per row each), Dinv and a zero diagonal term (9 per row
-// each), partial sums, scalars, then int storage (diagonal slots, flag).
+// each), partial sums, scalars, then int storage (flag words, diagonal slots).
 constexpr size_t NOALLOC_VEC = 3 * (size_t)NOALLOC_MAX_ROWS;
 constexpr size_t NOALLOC_DOUBLES = 4 * NOALLOC_VEC + 18 * (size_t)NOALLOC_MAX_ROWS + NOALLOC_PARTS + 16 + (NOALLOC_MAX_ROWS + 64) / 2;
+static_assert(NOALLOC_DOUBLES * sizeof(double) == 8008064, "the documented scratch size");
 }  // namespace
 
 static __device__ __align__(256) double g_noallocScratch[NOALLOC_DOUBLES];
@@ -1596,11 +1598,25 @@ static __device__ __align__(256) double g_noallocScratch[NOALLOC_DOUBLES];
 namespace {
 double* g_noallocAddr[256] = {nullptr};  // device address of the scratch, per device id
 
-__global__ void noallocDiagKernel(int nv, const int* rowPtr, const int* colIdx, int* diagSlot, double* zeroDiag) {
+// Checks the caller's block-CSR structure while locating the diagonal blocks:
+// row pointers non-negative and non-decreasing, column indices in range, and
+// exactly one diagonal block per row (an SPD matrix has a nonsingular
+// diagonal block in every row; the block-Jacobi inverse needs it).  A failure
+// sets a bit of *bad; the caller then reads no block.
+__global__ void noallocDiagKernel(int nv, const int* rowPtr, const int* colIdx, int* diagSlot, double* zeroDiag, int* bad) {
     CIPC_KERNEL_LOOP(r, nv) {
-        int s = -1;
-        for (int k = rowPtr[r]; k < rowPtr[r + 1]; ++k)
-            if (colIdx[k] == r) { s = k; break; }
+        const int b = rowPtr[r], e = rowPtr[r + 1];
+        int s = -1, nd = 0;
+        if (b < 0 || e < b) {
+            atomicOr(bad, 1);
+        } else {
+            for (int k = b; k < e; ++k) {
+                const int cl = colIdx[k];
+                if (cl < 0 || cl >= nv) { atomicOr(bad, 2); break; }
+                if (cl == r) { s = k; ++nd; }
+            }
+            if (nd != 1) atomicOr(bad, 4);
+        }
         diagSlot[r] = s;
         for (int q = 0; q < 9; ++q) zeroDiag[9 * r + q] = 0.0;
     }
@@ -1634,13 +1650,22 @@ extern "C" int cipc_gpu_pcg_bsr_noalloc(int nv, const int* rowPtr, const int* co
     double* scal = parts + NOALLOC_PARTS;
     int* ints = reinterpret_cast<int*>(scal + 16);
     int* flag = ints;
+    int* bad = ints + 1;
     int* diagSlot = ints + 64;
     double* partA = parts;
     double* partB = parts + 512;
     double* partC = parts + 1024;
     int vb = vecBlocks(nv);
     int sb = std::max(1, std::min((nv * GROUP + VB - 1) / VB, MAXPART));
-    launch(noallocDiagKernel, vb, VB, 0, s, nv, rowPtr, colIdx, diagSlot, zeroDiag);
+    // the structure check runs (and is read back) before any kernel reads a
+    // block through the caller's column indices
+    int hbad = 0;
+    if (cudaMemsetAsync(bad, 0, sizeof(int), s) != cudaSuccess) return CIPC_ERR_CUDA;
+    launch(noallocDiagKernel, vb, VB, 0, s, nv, rowPtr, colIdx, diagSlot, zeroDiag, bad);
+    if (cudaGetLastError() != cudaSuccess) return CIPC_ERR_CUDA;
+    if (cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CIPC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CIPC_ERR_CUDA;
+    if (hbad) return CIPC_ERR_INVALID_ARGUMENT;
     launch(dinvKernel<double>, vb, VB, 0, s, nv, diagSlot, vals, (const int*)nullptr, (const int*)nullptr, (const int*)nullptr,
            (const double*)nullptr, zeroDiag, Dinv);
     launch(pcgInitKernel<double>, vb, VB, 0, s, nv, rhs, Dinv, sol, r, z, p, partA, partB);

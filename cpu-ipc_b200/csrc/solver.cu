@@ -643,6 +643,13 @@ int cipc_gpu_set_kappa(cipc_gpu_context* h, double kappa) {
     return guarded(h, [&](Ctx& c) { c.P.kappa = kappa; });
 }
 
+int cipc_gpu_set_intersection_rule(cipc_gpu_context* h, int rule) {
+    return guarded(h, [&](Ctx& c) {
+        if (rule != CIPC_INTERSECT_TOLERANT && rule != CIPC_INTERSECT_REFERENCE) throw InvalidArgument("unknown intersection rule");
+        c.coplanarTol = rule == CIPC_INTERSECT_REFERENCE ? 0.0 : 1e-12;
+    });
+}
+
 int cipc_gpu_get_counts(cipc_gpu_context* h, long long* o) {
     return guarded(h, [&](Ctx& c) {
         o[0] = c.nv; o[1] = c.nsf; o[2] = c.nsv; o[3] = c.nse; o[4] = c.nb; o[5] = c.nt; o[6] = c.nf; o[7] = c.nnzb; o[8] = c.nDynB;
@@ -957,13 +964,19 @@ extern "C" int cipc_gpu_pcg_bsr(int nv, const int* rowPtr, const int* colIdx, co
             c.mixed = options->precision == CIPC_PRECISION_MIXED;
         }
         int nnzb = rowPtr[nv];
+        if (nnzb < 0 || rowPtr[0] < 0) return fail("row pointers must be non-negative and non-decreasing", CIPC_ERR_INVALID_ARGUMENT);
         c.nnzb = nnzb;
         std::vector<int> rp(rowPtr, rowPtr + nv + 1), ci(colIdx, colIdx + nnzb), diag(nv, -1);
-        for (int r = 0; r < nv; ++r)
+        for (int r = 0; r < nv; ++r) {
+            if (rp[r] < 0 || rp[r + 1] < rp[r]) return fail("row pointers must be non-negative and non-decreasing", CIPC_ERR_INVALID_ARGUMENT);
+            int nd = 0;
             for (int k = rp[r]; k < rp[r + 1]; ++k) {
                 if (ci[k] < 0 || ci[k] >= nv) return fail("column index out of range", CIPC_ERR_INVALID_ARGUMENT);
-                if (ci[k] == r) diag[r] = k;
+                if (ci[k] == r) { diag[r] = k; ++nd; }
             }
+            // the block-Jacobi inverse needs the row's one diagonal block
+            if (nd != 1) return fail("every block row needs exactly one diagonal block", CIPC_ERR_INVALID_ARGUMENT);
+        }
         CIPC_CUDA(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
         upload(c.rowPtr, rp); upload(c.colIdx, ci); upload(c.diagSlot, diag);
         std::vector<double> v(vals, vals + 9 * (size_t)nnzb);

@@ -4,6 +4,7 @@
 #include "cipc_internal.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 namespace cipc {
@@ -14,8 +15,9 @@ constexpr int RB = 256;
 template <int OP>
 __device__ __forceinline__ double combine(double a, double b) {
     if (OP == 0) return a + b;
-    if (OP == 1) return a > b ? a : b;
-    if (OP == 2) return a < b ? a : b;
+    // max and min carry a NaN forward whatever the order of the operands
+    if (OP == 1) return (a > b || a != a) ? a : b;
+    if (OP == 2) return (a < b || a != a) ? a : b;
     return a + b;
 }
 template <int OP>
@@ -94,7 +96,11 @@ void fetchSums(Ctx& c, double* h, int nslots) {
 double deviceMax(Ctx& c, const double* v, int n) { return reduce<1>(c, v, nullptr, n); }
 double deviceMin(Ctx& c, const double* v, int n, double init) { return std::min(init, reduce<2>(c, v, nullptr, n)); }
 double deviceDot(Ctx& c, const double* a, const double* b, int n) { return reduce<3>(c, a, b, n); }
-double deviceInfNorm(Ctx& c, const double* v, int n) { return std::max(0.0, reduce<4>(c, v, nullptr, n)); }
+double deviceInfNorm(Ctx& c, const double* v, int n) {
+    const double m = reduce<4>(c, v, nullptr, n);
+    if (!std::isfinite(m)) throw std::runtime_error("non-finite entry in a search direction or vector norm");
+    return std::max(0.0, m);
+}
 
 void checkStatus(Ctx& c, const char* stage) {
     int st = 0;
@@ -108,7 +114,12 @@ void checkStatus(Ctx& c, const char* stage) {
         if (st & CIPC_ST_CAPACITY) msg += " candidate buffer capacity exceeded;";
         if (st & CIPC_ST_CCD_CAP) msg += " CCD iteration cap;";
         if (st & CIPC_ST_JACOBI_CAP) msg += " eigen-solver sweep cap;";
-        if (st & CIPC_ST_TC_TIMEOUT) msg += " tensor-core completion wait timed out;";
+        if (st & CIPC_ST_TC_TIMEOUT) {
+            // a late tensor-core operation may have written freed tensor
+            // memory: no further network pass runs on this context
+            c.tcFault = true;
+            msg += " tensor-core completion wait timed out (the learned preconditioner is disabled for this context);";
+        }
         throw std::runtime_error(msg);
     }
 }

@@ -116,6 +116,15 @@ int cipc_gpu_set_state(cipc_gpu_context* ctx, int which, const double* in);
  * volumeRate, stretchS, shearS, plateRigidity, dt, newtonThr */
 int cipc_gpu_get_scalars(cipc_gpu_context* ctx, double* out14);
 int cipc_gpu_set_kappa(cipc_gpu_context* ctx, double kappa);
+/* Segment-triangle test of the intersection check (isIntersected /
+ * IglUtils::segTriIntersect, IPCSolver.cpp:476-542, ContactMechanics.h:47-71).
+ * CIPC_INTERSECT_TOLERANT (default) also skips a segment whose two plane
+ * distances are both within 1e-12 of zero relative to |n| times its reach
+ * (near-coplanar through rounding on rotated meshes);
+ * CIPC_INTERSECT_REFERENCE is the reference's exact rule (signs and
+ * det == 0 only). */
+enum { CIPC_INTERSECT_TOLERANT = 0, CIPC_INTERSECT_REFERENCE = 1 };
+int cipc_gpu_set_intersection_rule(cipc_gpu_context* ctx, int rule);
 /* counts: nv, nsf, nsv, nse, nbend, nt, nf, nnzb (static BSR blocks),
  * contact BSR blocks of the last assembly */
 int cipc_gpu_get_counts(cipc_gpu_context* ctx, long long* out9);
@@ -214,7 +223,10 @@ int cipc_gpu_precond_stats(cipc_gpu_context* ctx, long long* out3);
 
 /* Stand-alone GPU PCG on a caller-given matrix (full symmetric 3x3-block CSR,
  * FP64 values, 9 per block row-major) - the backend switch of
- * NewtonLinearSystem::solve (NewtonLinearSystem.cpp:41-53) without a scene. */
+ * NewtonLinearSystem::solve (NewtonLinearSystem.cpp:41-53) without a scene.
+ * Row pointers must be non-negative and non-decreasing, column indices in
+ * [0, nv), and every block row must hold exactly one diagonal block;
+ * otherwise CIPC_ERR_INVALID_ARGUMENT. */
 int cipc_gpu_pcg_bsr(int nv, const int* rowPtr, const int* colIdx, const double* vals, const double* rhs, double* sol,
                      const cipc_linear_options* options, int* iterations, double* relResidual, char* err, int errlen);
 
@@ -225,9 +237,11 @@ int cipc_gpu_pcg_bsr(int nv, const int* rowPtr, const int* colIdx, const double*
  * pointers the caller owns (rowPtr nv+1, colIdx and vals as in
  * cipc_gpu_pcg_bsr, rhs and sol 3*nv); the function allocates nothing and
  * keeps its scratch vectors in a fixed array inside the library, sized for at
- * most CIPC_NOALLOC_MAX_ROWS block rows (about 8.2 MB, held on every GPU that
- * loads the library until the process exits); larger nv returns
- * CIPC_ERR_INVALID_ARGUMENT.  The first call on a device resolves that array's
+ * most CIPC_NOALLOC_MAX_ROWS block rows (8,008,064 bytes, 7.6 MiB, held on
+ * every GPU that loads the library until the process exits); larger nv
+ * returns CIPC_ERR_INVALID_ARGUMENT.  The matrix structure is checked on the
+ * device with the rules cipc_gpu_pcg_bsr applies on the host (same error
+ * code) before any block is read.  The first call on a device resolves that array's
  * device address with the device current, so make the first call on each
  * device outside any stream capture.  Every call shares the array: calls
  * that overlap on the GPU (other streams or threads) race and must be

@@ -77,6 +77,7 @@ def lib():
         L.cipc_oracle_info.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.cipc_oracle_scalars.argtypes = [vp, dp]
         L.cipc_oracle_set_kappa.argtypes = [vp, C.c_double]
+        L.cipc_oracle_set_intersection_rule.argtypes = [vp, C.c_int]
         L.cipc_oracle_get.argtypes = [vp, C.c_int, dp]
         L.cipc_oracle_set.argtypes = [vp, C.c_int, dp]
         L.cipc_oracle_surface.argtypes = [vp, ip, ip, ip]
@@ -200,6 +201,12 @@ class Oracle:
 
     def set_kappa(self, k):
         self.L.cipc_oracle_set_kappa(self.h, float(k))
+
+    def set_intersection_rule(self, rule):
+        """'tolerant' (default): near-coplanar segments within a 1e-12
+        relative tolerance count as coplanar; 'reference': the reference's
+        exact rule (ContactMechanics.h:47-71)."""
+        self.L.cipc_oracle_set_intersection_rule(self.h, {"tolerant": 0, "reference": 1}[rule])
 
     _FIELDS = {"x": 0, "vel": 1, "vprev": 2, "xtilde": 3, "rest": 4}
 

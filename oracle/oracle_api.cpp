@@ -134,6 +134,9 @@ void cipc_oracle_scalars(void* h, double* o) {
     std::memcpy(o, v, sizeof(v));
 }
 void cipc_oracle_set_kappa(void* h, double k) { static_cast<Ctx*>(h)->m.kappa = k; }
+void cipc_oracle_set_intersection_rule(void* h, int rule) {
+    static_cast<Ctx*>(h)->m.coplanarTol = rule == 1 ? 0.0 : 1e-12;
+}
 
 static std::vector<V3>* field(Mesh& m, int which) {
     switch (which) {

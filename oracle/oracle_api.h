@@ -45,6 +45,10 @@ void cipc_oracle_info(void* h, long long* counts);
  * stretchS, shearS, plateRigidity, dt, newtonThr */
 void cipc_oracle_scalars(void* h, double* out);
 void cipc_oracle_set_kappa(void* h, double kappa);
+/* segment-triangle test of the intersection check: 0 skips near-coplanar
+ * segments within a 1e-12 relative tolerance (default), 1 is the
+ * reference's exact rule (ContactMechanics.h:47-71) */
+void cipc_oracle_set_intersection_rule(void* h, int rule);
 /* which: 0 x, 1 vel, 2 vprev, 3 xtilde, 4 rest, 5 mass(nv) */
 void cipc_oracle_get(void* h, int which, double* out);
 void cipc_oracle_set(void* h, int which, const double* in);

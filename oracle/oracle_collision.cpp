@@ -467,18 +467,20 @@ void selfLargestFeasibleStepCCD(const Mesh& m, BroadPhase& bp, const std::vector
 // IglUtils::segTriIntersect, ContactMechanics.h:47-71 (Cramer's rule stands
 // in for the full-pivot LU solve of the same 3x3 system).  The reference skips
 // coplanar pairs (coplanar contact is caught by the distances) but tests only
-// exact signs and det == 0; a segment whose two plane distances are both
-// within COPLANAR_TOL of zero (relative to |n| times its reach from t0) is
-// taken as coplanar too, so rounding on rotated meshes cannot report the
-// edges and triangles of one flat face as intersecting.
-static constexpr double COPLANAR_TOL = 1e-12;
-static bool segTriIntersect(const V3& e0, const V3& e1, const V3& t0, const V3& t1, const V3& t2) {
+// exact signs and det == 0; with coplanarTol > 0 a segment whose two plane
+// distances are both within coplanarTol of zero (relative to |n| times its
+// reach from t0) is taken as coplanar too, so rounding on rotated meshes
+// cannot report the edges and triangles of one flat face as intersecting.
+// coplanarTol = 0 is the reference's rule exactly.
+static bool segTriIntersect(const V3& e0, const V3& e1, const V3& t0, const V3& t1, const V3& t2, double coplanarTol) {
     V3 c0 = t1 - t0, c1 = t2 - t0, c2 = e0 - e1;
     V3 n = cross(c0, c1);
     const double d0 = dot(n, e0 - t0), d1 = dot(n, e1 - t0);
     if (d0 * d1 > 0.0) return false;
-    const double tol = COPLANAR_TOL * norm(n) * std::max(norm(e0 - t0), norm(e1 - t0));
-    if (std::fabs(d0) <= tol && std::fabs(d1) <= tol) return false;
+    if (coplanarTol > 0.0) {
+        const double tol = coplanarTol * norm(n) * std::max(norm(e0 - t0), norm(e1 - t0));
+        if (std::fabs(d0) <= tol && std::fabs(d1) <= tol) return false;
+    }
     M3 A;
     for (int k = 0; k < 3; ++k) { A.a[k][0] = c0[k]; A.a[k][1] = c1[k]; A.a[k][2] = c2[k]; }
     double det = det3(A);
@@ -506,7 +508,7 @@ bool isIntersected(const Mesh& m, BroadPhase& bp) {
             const I2& E = m.surfEdges[e];
             if (E.first == F[0] || E.first == F[1] || E.first == F[2] || E.second == F[0] || E.second == F[1] || E.second == F[2]) continue;
             if (isCollider(m.btype[E.first]) && isCollider(m.btype[E.second]) && isCollider(m.btype[F[0]]) && isCollider(m.btype[F[1]]) && isCollider(m.btype[F[2]])) continue;
-            if (segTriIntersect(m.x[E.first], m.x[E.second], m.x[F[0]], m.x[F[1]], m.x[F[2]])) return true;
+            if (segTriIntersect(m.x[E.first], m.x[E.second], m.x[F[0]], m.x[F[1]], m.x[F[2]], m.coplanarTol)) return true;
         }
     }
     return false;

@@ -75,6 +75,9 @@ struct Mesh {
     double dt = 0.01, drag = 0, Hhat = 1e-6, Fhat = 1e-6, dTol = 1e-18, kappa = 0;
     double bboxDiag2 = 0, newtonThr = 1e-2, meanMass = 0, avgEdge = 0;
     bool use_barrier = true, apply_gravity = true, quasi_static = false;
+    // segment-triangle coplanarity: relative tolerance (1e-12), or 0 for the
+    // reference's exact rule (signs and det == 0 only)
+    double coplanarTol = 1e-12;
 
     std::vector<V3> x, rest, vel, vprev, xtilde;
     std::vector<I4> tets;

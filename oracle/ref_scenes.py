@@ -4,19 +4,28 @@ Restates the scene builders of CPU IPC/Simulator.cpp:265-399, the parameter
 file Assets/scene/parameterSetting.txt and the Gmsh/OBJ loaders of
 CPU IPC/SimulationMesh.cpp:174-362, 545-716, so the oracle can be pinned
 against the known answers the reference's documentation quotes.  The meshes
-are read from the reference checkout when it is present; nothing here is
-shipped or used on the GPU path.
+are read from tests/golden/assets (copies of the reference's Assets files,
+MPL-2.0, see the NOTICE there); CIPC_REFERENCE_ASSETS names another Assets
+directory instead.  Nothing here is shipped or used by the library.
 """
 import math
 import os
 
 import numpy as np
 
-REFERENCE_ASSETS = os.environ.get("CIPC_REFERENCE_ASSETS", "/root/reference/Assets")
+BUNDLED_ASSETS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden", "assets")
+REFERENCE_ASSETS = os.environ.get("CIPC_REFERENCE_ASSETS", BUNDLED_ASSETS)
+
+SCENE_FILES = {
+    "twisting_mat": ["tetrahedraMesh/ipcmesh/mat40x40.msh"],
+    "cloth_bunny": ["triangleMesh/planes/plane1024.obj", "tetrahedraMesh/bunny.msh"],
+    "bunny2": ["tetrahedraMesh/bunny2.msh"],
+}
 
 
-def assets_available():
-    return os.path.isdir(REFERENCE_ASSETS)
+def assets_available(scene="twisting_mat"):
+    """Whether the mesh files of a reference scene are present."""
+    return all(os.path.isfile(os.path.join(REFERENCE_ASSETS, f)) for f in SCENE_FILES[scene])
 
 
 def load_gmsh(path, scale=1.0, offset=(0.0, 0.0, 0.0)):

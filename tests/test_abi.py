@@ -4,6 +4,7 @@ import ctypes as C
 import os
 import re
 
+import numpy as np
 import pytest
 
 import cipc
@@ -84,3 +85,35 @@ def test_create_rejects_unknown_bending_model():
     sc["params"] = dict(sc["params"], quad_bending=3)
     rc, h, msg = _create(sc, cipc.linear_options())
     assert rc == 1 and not h.value and "bending model" in msg
+
+
+def _small_block_system(nv=6):
+    cols = [sorted({r, (r + 1) % nv, (r - 1) % nv}) for r in range(nv)]
+    ci = np.array([c for row in cols for c in row], np.int32)
+    rp = np.concatenate([[0], np.cumsum([len(row) for row in cols])]).astype(np.int32)
+    vals = np.zeros((len(ci), 3, 3))
+    for r in range(nv):
+        for k in range(rp[r], rp[r + 1]):
+            vals[k] = 4 * np.eye(3) if ci[k] == r else -0.5 * np.eye(3)
+    return rp, ci, vals, np.ones(3 * nv)
+
+
+@pytest.mark.parametrize("fault", ["missing_diagonal", "duplicate_diagonal", "column_out_of_range", "decreasing_row_pointer"])
+def test_pcg_bsr_rejects_malformed_structure(fault):
+    """The stand-alone PCG refuses a malformed block-CSR matrix with an
+    invalid-argument code before it touches the device."""
+    rp, ci, vals, b = _small_block_system()
+    ci = ci.copy()
+    rp = rp.copy()
+    row = list(ci[rp[2]:rp[3]])
+    if fault == "missing_diagonal":
+        ci[rp[2] + row.index(2)] = 0
+    elif fault == "duplicate_diagonal":
+        ci[rp[2] + [k for k, c in enumerate(row) if c != 2][0]] = 2
+    elif fault == "column_out_of_range":
+        ci[4] = 6
+    else:
+        rp[3] = rp[2] - 1
+    with pytest.raises(cipc.CipcError) as e:
+        cipc.pcg_bsr(rp, ci, vals, b)
+    assert e.value.code == 1

@@ -2,7 +2,10 @@
 
 The reference ships no test suite; its documentation quotes the RESULT line
 of cipc_headless for its demo scenes.  These tests run the oracle on the same
-scenes (meshes read from the reference checkout when present) and compare.
+scenes (the reference's meshes, copied under tests/golden/assets) and
+compare.  The scenes that step run under both segment-triangle intersection
+rules, the reference's exact one and the default that also skips
+near-coplanar segments: the known answers hold under either.
 """
 import json
 import os
@@ -15,12 +18,16 @@ import ref_scenes
 HERE = os.path.dirname(os.path.abspath(__file__))
 KAT = json.load(open(os.path.join(HERE, "golden", "kat_values.json")))
 
-needs_assets = pytest.mark.skipif(not ref_scenes.assets_available(), reason="reference assets not present")
+needs_assets = pytest.mark.skipif(not ref_scenes.assets_available("cloth_bunny") or not ref_scenes.assets_available("twisting_mat"),
+                                  reason="reference assets not present")
+RULES = pytest.mark.parametrize("rule", ["tolerant", "reference"])
 
 
 @needs_assets
-def test_twisting_mat_one_step(oracle_mod):
+@RULES
+def test_twisting_mat_one_step(oracle_mod, rule):
     o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=False), linear="direct", threads=8)
+    o.set_intersection_rule(rule)
     st = o.step()
     x = o.get("x")
     k = KAT["twisting_mat_1_step"]
@@ -57,8 +64,10 @@ def test_twisting_mat_five_steps_multifrontal(oracle_mod):
 
 
 @needs_assets
-def test_twisting_mat_soft_five_steps(oracle_mod):
+@RULES
+def test_twisting_mat_soft_five_steps(oracle_mod, rule):
     o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=True), linear="direct", threads=8)
+    o.set_intersection_rule(rule)
     for _ in range(5):
         st = o.step()
     x = o.get("x")
@@ -69,8 +78,10 @@ def test_twisting_mat_soft_five_steps(oracle_mod):
 
 
 @needs_assets
-def test_twisting_mat_five_steps(oracle_mod):
+@RULES
+def test_twisting_mat_five_steps(oracle_mod, rule):
     o = oracle_mod.Oracle(ref_scenes.twisting_mat(soft=False), linear="direct", threads=8)
+    o.set_intersection_rule(rule)
     for _ in range(5):
         st = o.step()
     x = o.get("x")
@@ -82,10 +93,12 @@ def test_twisting_mat_five_steps(oracle_mod):
 
 
 @needs_assets
-def test_cloth_bunny_one_step(oracle_mod):
+@RULES
+def test_cloth_bunny_one_step(oracle_mod, rule):
     sc = ref_scenes.cloth_bunny()
     k = KAT["cloth_bunny_1_step"]
     o = oracle_mod.Oracle(sc, linear="direct", threads=8)
+    o.set_intersection_rule(rule)
     assert o.nv == k["vertices"] and o.nt == k["tets"] and o.nsf == k["surface_faces"]
     st = o.step()
     assert st["newton"] == k["newton"]
@@ -104,7 +117,8 @@ def test_cloth_bunny_loader_positions():
 
 
 @needs_assets
-def test_cloth_bunny_hinge_bending_one_step(oracle_mod):
+@RULES
+def test_cloth_bunny_hinge_bending_one_step(oracle_mod, rule):
     """The reference built without USE_QUADRATIC_BENDING bends the cloth with
     dihedral-angle hinges; its documentation quotes the first step of the
     cloth-bunny scene in that build.  The hinge Hessian blocks are full 3x3
@@ -112,6 +126,7 @@ def test_cloth_bunny_hinge_bending_one_step(oracle_mod):
     sc = ref_scenes.cloth_bunny(hinge=True)
     k = KAT["cloth_bunny_hinge_1_step"]
     o = oracle_mod.Oracle(sc, linear="direct", threads=8)
+    o.set_intersection_rule(rule)
     assert o.nsf == k["surface_faces"]
     st = o.step()
     assert st["newton"] == k["newton"]
@@ -120,13 +135,15 @@ def test_cloth_bunny_hinge_bending_one_step(oracle_mod):
     assert st["matrixNnz"] == k["matrix_nnz"]
 
 
-@needs_assets
-def test_bunny2_one_step(oracle_mod):
+@pytest.mark.skipif(not ref_scenes.assets_available("bunny2"), reason="bunny2 mesh not present")
+@RULES
+def test_bunny2_one_step(oracle_mod, rule):
     # the two-bunny PARDISO benchmark scene: its documented first step
     sc = ref_scenes.bunny2()
     k = KAT["bunny2_1_step"]
     assert len(sc["x"]) == k["vertices"] and len(sc["tets"]) == k["tets"]
     o = oracle_mod.Oracle(sc, linear="multifrontal", threads=os.cpu_count() or 1)
+    o.set_intersection_rule(rule)
     assert o.nsf == k["surface_faces"]
     st = o.step()
     assert st["newton"] == k["newton"]

@@ -44,33 +44,87 @@ def _spd_block_system(nv=400, seed=0):
     return rp, ci, vals, b, A
 
 
+def _noalloc_call(rp, ci, vals, b, tol, sol_fill=float("nan")):
+    """One call of the allocation-free entry point on device copies of the
+    arrays (torch owns them, as the host's own allocator would)."""
+    import torch
+
+    nv = len(rp) - 1
+    dev = torch.device("cuda", 0)
+    d_rp = torch.from_numpy(np.ascontiguousarray(rp, np.int32)).to(dev)
+    d_ci = torch.from_numpy(np.ascontiguousarray(ci, np.int32)).to(dev)
+    d_vals = torch.from_numpy(np.ascontiguousarray(vals, np.float64).reshape(-1)).to(dev)
+    d_b = torch.from_numpy(np.ascontiguousarray(b, np.float64)).to(dev)
+    d_sol = torch.full((3 * nv,), sol_fill, dtype=torch.float64, device=dev)
+    it = C.c_int(0)
+    rr = C.c_double(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = cipc.lib().cipc_gpu_pcg_bsr_noalloc(nv, d_rp.data_ptr(), d_ci.data_ptr(), d_vals.data_ptr(), d_b.data_ptr(), d_sol.data_ptr(),
+                                             tol, 10000, C.c_void_p(stream), C.byref(it), C.byref(rr))
+    torch.cuda.synchronize()
+    return rc, d_sol.cpu().numpy(), it.value
+
+
+def _check_against_allocating(nv, seed):
+    rp, ci, vals, b, A = _spd_block_system(nv=nv, seed=seed)
+    tol = 1e-8
+    x_ref, it_ref, _ = cipc.pcg_bsr(rp, ci, vals, b, precision="fp64", tol=tol)
+    for call in range(2):
+        rc, x, it = _noalloc_call(rp, ci, vals, b, tol)
+        assert rc == 0, f"call {call}: rc {rc}"
+        assert np.linalg.norm(A @ x - b) <= 1e-6 * np.linalg.norm(b)
+        assert it == it_ref
+        assert np.allclose(x, x_ref, rtol=1e-9, atol=1e-12 * np.abs(x_ref).max())
+
+
 def test_noalloc_pcg_matches_allocating_entry_point():
     import torch
 
     torch.cuda.set_device(0)
-    rp, ci, vals, b, A = _spd_block_system()
-    nv = len(rp) - 1
-    tol = 1e-8
-    x_ref, it_ref, _ = cipc.pcg_bsr(rp, ci, vals, b, precision="fp64", tol=tol)
-    dev = torch.device("cuda", 0)
-    d_rp = torch.from_numpy(rp).to(dev)
-    d_ci = torch.from_numpy(ci).to(dev)
-    d_vals = torch.from_numpy(vals.reshape(-1)).to(dev)
-    d_b = torch.from_numpy(b).to(dev)
-    L = cipc.lib()
-    stream = torch.cuda.current_stream().cuda_stream
-    for call in range(2):
-        d_sol = torch.full((3 * nv,), float("nan"), dtype=torch.float64, device=dev)
-        it = C.c_int(0)
-        rr = C.c_double(0)
-        rc = L.cipc_gpu_pcg_bsr_noalloc(nv, d_rp.data_ptr(), d_ci.data_ptr(), d_vals.data_ptr(), d_b.data_ptr(), d_sol.data_ptr(),
-                                        tol, 10000, C.c_void_p(stream), C.byref(it), C.byref(rr))
-        torch.cuda.synchronize()
-        assert rc == 0, f"call {call}: rc {rc}"
-        x = d_sol.cpu().numpy()
-        assert np.linalg.norm(A @ x - b) <= 1e-6 * np.linalg.norm(b)
-        assert it.value == it_ref
-        assert np.allclose(x, x_ref, rtol=1e-9, atol=1e-12 * np.abs(x_ref).max())
+    _check_against_allocating(400, 0)
+
+
+def test_noalloc_at_the_row_limit():
+    """A system of exactly CIPC_NOALLOC_MAX_ROWS block rows fills the whole
+    scratch array; it matches the allocating entry point, twice in a row."""
+    import torch
+
+    torch.cuda.set_device(0)
+    _check_against_allocating(cipc.NOALLOC_MAX_ROWS, 3)
+
+
+def _drop_diagonal(rp, ci, vals, row):
+    keep = np.ones(len(ci), bool)
+    keep[rp[row] + int(np.nonzero(ci[rp[row]:rp[row + 1]] == row)[0][0])] = False
+    rp2 = rp.copy()
+    rp2[row + 1:] -= 1
+    return rp2, ci[keep], vals[keep]
+
+
+def test_noalloc_rejects_malformed_structure():
+    """A row without its diagonal block, a duplicated diagonal block and a
+    column index out of range are refused by both PCG entry points before
+    any block is read (the solution buffer stays untouched); a valid call
+    afterwards still solves."""
+    import torch
+
+    torch.cuda.set_device(0)
+    rp, ci, vals, b, A = _spd_block_system(nv=64, seed=5)
+    bad = [_drop_diagonal(rp, ci, vals, 17)]
+    ci_dup = ci.copy()
+    ci_dup[rp[9] + int(np.nonzero(ci[rp[9]:rp[10]] != 9)[0][0])] = 9  # a second diagonal block in row 9
+    bad.append((rp, ci_dup, vals))
+    ci_oob = ci.copy()
+    ci_oob[5] = 64
+    bad.append((rp, ci_oob, vals))
+    for brp, bci, bvals in bad:
+        rc, x, _ = _noalloc_call(brp, bci, bvals, b, 1e-8, sol_fill=7.0)
+        assert rc == 1
+        assert np.all(x == 7.0)
+        with pytest.raises(cipc.CipcError):
+            cipc.pcg_bsr(brp, bci, bvals, b, precision="fp64", tol=1e-8)
+    rc, x, _ = _noalloc_call(rp, ci, vals, b, 1e-8)
+    assert rc == 0 and np.linalg.norm(A @ x - b) <= 1e-6 * np.linalg.norm(b)
 
 
 def test_noalloc_rejects_oversized_systems():
