@@ -1,11 +1,13 @@
 """Benchmark of the GPU IPC time step (one JSON line on rank 0).
 
-A "step" is one solveIPCStep of the cloth-drape scene: a 128x128-vertex 1 m
-cloth (32,258 triangles, Baraff-Witkin membrane + quadratic bending,
-self-contact, friction 0.3) 0.1 m above a fixed 0.5 m tetrahedral cube
-(10^3 cells, 6 tets per cell), dt = 0.005 s.  Inputs are synthetic (the
-reference's benchmark scenes are not in its repository); the mesh is
-generated here with the sizes the configuration states.
+A "step" is one solveIPCStep of the pile scene: 64 cubes of 0.2 m (12^3
+cells, 6 tets per cell: 663,552 tets, 140,608 vertices) at seeded random
+rotations and positions in a 1.5 m box, dropped into a static open box,
+Neo-Hookean E ~ U[5e4, 5e5], nu 0.4, friction 0.2, dt = 0.01 s, relative dhat
+1e-3, Newton threshold 1e-2 (the reference's parameterSetting.txt value).
+Inputs are synthetic (the reference's benchmark scenes are not in its
+repository); the meshes are generated here with the sizes the configuration
+states.
 
   value    steps/s over all ranks, device time from CUDA events on the
            library's stream, state resident in HBM; L2 is flushed (256 MiB
@@ -21,24 +23,25 @@ generated here with the sizes the configuration states.
            on the library's stream around every launch).
 The learned preconditioner is trained online on the Newton systems of the
 first --train-steps steps (Adam on the GPU, not timed), then frozen.  Timing
-starts after --settle-steps untimed steps (40: the cloth has reached the
-cube), so the timed steps are in contact like most of the configuration's
-400 steps.  The same run also times the plain FP64 block-Jacobi GPU path on
-the same frames.
+starts after --settle-steps untimed steps and the warm-up (pile: 30, the
+lower layers of cubes rest on the box and on each other; cloth: 40, the
+cloth has reached the cube), so the timed steps are in contact.  The same
+run also times the plain FP64 block-Jacobi GPU path on the same frames.
 Multi-GPU: replicas only (one independent simulation per rank, weak scaling).
 
---scene pile measures the pile configuration instead: 64 cubes of 0.2 m
-(12^3 cells, 6 tets per cell: 663,552 tets, 140,608 vertices) at seeded
-random rotations, dropped into a static open box, dt = 0.01 s.
+--scene cloth_drape measures the cloth-drape configuration instead: a
+128x128-vertex 1 m cloth (32,258 triangles, Baraff-Witkin membrane +
+quadratic bending, friction 0.3) 0.1 m above a fixed 0.5 m tetrahedral cube
+(10^3 cells), dt = 0.005 s.
 
 --impl reference times the reference's CPU path on the host cores.  The
 reference itself cannot be compiled here (Eigen, oneTBB, oneMKL and
 SuiteSparse are absent), so its FP64 restatement (oracle/) stands in, with
 the reference's default linear solver, PARDISO, restated as a parallel
-multifrontal Cholesky under a nested-dissection ordering.  For
-the cloth drape it starts from the oracle's own state after the settle steps
-(oracle/states/), then runs the same warm-up, so it times the same frames as
-the GPU arm; cpu_baseline does the same without the warm-up.
+multifrontal Cholesky under a nested-dissection ordering.  Both CPU legs
+start from the oracle's own state at the first timed frame of the GPU arm
+(oracle/states/, settle + warm-up steps; or at the last settle step, then the
+warm-up), so they time the same frames as the GPU arm.
 """
 import argparse
 import json
@@ -62,14 +65,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="cloth_drape", choices=["cloth_drape", "pile"])
+    ap.add_argument("--scene", default="pile", choices=["cloth_drape", "pile"])
     ap.add_argument("--cloth", type=int, default=128)
     ap.add_argument("--pile-cubes", type=int, default=64)
     ap.add_argument("--pile-cells", type=int, default=12)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--precond", default="learned", choices=["jacobi", "learned", "fsai"])
-    ap.add_argument("--settle-steps", type=int, default=40, help="untimed steps before warm-up: the cloth reaches the cube")
-    ap.add_argument("--train-steps", type=int, default=40, help="settle steps whose last Newton system trains the network")
+    ap.add_argument("--settle-steps", type=int, default=None, help="untimed steps before warm-up (pile 30, cloth 40: in contact)")
+    ap.add_argument("--train-steps", type=int, default=None, help="settle steps whose last Newton system trains the network (default: all)")
     ap.add_argument("--train-iters", type=int, default=60)
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 block-Jacobi path")
     ap.add_argument("--roofline-kernel", default="pcg")
@@ -77,7 +80,12 @@ def parse():
     ap.add_argument("--profile-timed", action="store_true",
                     help="bracket the device-timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.settle_steps is None:
+        a.settle_steps = 30 if a.scene == "pile" else 40
+    if a.train_steps is None:
+        a.train_steps = a.settle_steps
+    return a
 
 
 def make_scene(args, cipc):
@@ -86,23 +94,21 @@ def make_scene(args, cipc):
     return cipc.scene_cloth_drape(args.cloth, 10)
 
 
-def workload(args, detail=False):
-    """Name (and with detail the description) of the measured workload."""
+def workload(args):
+    """Name of the measured workload (the same string on both arms)."""
+    if args.scene == "pile":
+        return f"pile_{args.pile_cubes}x{args.pile_cells}"
+    return f"cloth_drape_{args.cloth}"
+
+
+def describe(args):
     if args.scene == "pile":
         n, c = args.pile_cubes, args.pile_cells
-        name = f"pile_{n}x{c}"
-        if detail:
-            name += (f": {n} cubes of 0.2 m ({c}^3 cells x 6 tets each, {n * 6 * c ** 3} tets, {n * (c + 1) ** 3} vertices) "
-                     "at seeded random rotations and positions in a 1.5 m box, dropped into a static open box; "
-                     "Neo-Hookean E ~ U[5e4, 5e5], nu=0.4, mu=0.2, dt=0.01, dhat=1e-3")
-        return name
-    name = f"cloth_drape_{args.cloth}"
-    if detail:
-        name += (f": {args.cloth}x{args.cloth}-vertex 1 m cloth ({2 * (args.cloth - 1) ** 2} tris, BW membrane E=1e4, "
-                 "quadratic bending k_b=1e-3, mu=0.3) 0.1 m above a fixed 0.5 m tet cube (10^3 cells x 6 tets), dt=0.005, dhat=1e-3")
-    else:
-        name += f" (cloth {args.cloth}x{args.cloth} + 10^3-cell tet cube)"
-    return name
+        return (f"{n} cubes of 0.2 m ({c}^3 cells x 6 tets each, {n * 6 * c ** 3} tets, {n * (c + 1) ** 3} vertices) "
+                "at seeded random rotations and positions in a 1.5 m box, dropped into a static open box; "
+                "Neo-Hookean E ~ U[5e4, 5e5], nu=0.4, friction 0.2, dt=0.01, relative dhat 1e-3")
+    return (f"{args.cloth}x{args.cloth}-vertex 1 m cloth ({2 * (args.cloth - 1) ** 2} tris, BW membrane E=1e4, "
+            "quadratic bending k_b=1e-3, friction 0.3) 0.1 m above a fixed 0.5 m tet cube (10^3 cells x 6 tets), dt=0.005, relative dhat 1e-3")
 
 
 def dist_setup():
@@ -210,25 +216,21 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def oracle_at_settled_frame(args, scene, threads):
-    """The FP64 oracle on the bench scene, at the frame the GPU arm's warm-up
-    starts from when a saved state exists.
-
-    For the cloth drape the oracle's own state after --settle-steps steps
-    (written by oracle/states/make_contact_state.py) is restored, so the CPU
-    legs time the same contact frames as the GPU arm.  Without a saved state
-    for this scene they start at frame 0 (free fall: cheaper steps).
+def oracle_at_frame(args, scene, threads, frame):
+    """The FP64 oracle on the bench scene, restored from the oracle's own saved
+    state (oracle/states/, written by make_contact_state.py) at `frame`, the
+    latest saved frame at or before it, or frame 0 when none is saved.
     Returns (oracle, index of the next step)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     o = oracle.Oracle(scene, linear="multifrontal", threads=threads)
-    if args.scene == "cloth_drape":
-        path = os.path.join(ROOT, "oracle", "states", f"cloth_drape_{args.cloth}_frame{args.settle_steps}.npz")
+    for f in range(frame, 0, -1):
+        path = os.path.join(ROOT, "oracle", "states", f"{scene['name']}_frame{f}.npz")
         if os.path.exists(path):
             try:
                 return o, o.restore_state(path)
-            except ValueError:  # saved from another version of the scene: time from frame 0
-                pass
+            except ValueError:  # saved from another version of the scene
+                break
     return o, 0
 
 
@@ -236,10 +238,16 @@ def frames(first, n, restored):
     return f"frames {first}-{first + n - 1}" + (" (from the restored contact-phase state)" if restored else " (from the start of the scene)")
 
 
+def first_timed_frame(args):
+    """Index of the GPU arm's first timed step (settle + warm-up steps)."""
+    return args.settle_steps + max(3, args.warmup)
+
+
 def cpu_baseline(args, scene, seconds, steps_cap=50):
-    """The FP64 oracle on the same scene, all host cores, bounded by time."""
+    """The FP64 oracle on the same scene and frames, all host cores, bounded
+    by time (at least one step)."""
     threads = host_threads()
-    o, f0 = oracle_at_settled_frame(args, scene, threads)
+    o, f0 = oracle_at_frame(args, scene, threads, first_timed_frame(args))
     t0 = time.time()
     n = 0
     while n < steps_cap:
@@ -258,12 +266,15 @@ def run_reference(args, world, rank):
     import cipc
     scene = make_scene(args, cipc)
     threads = host_threads()
-    o, f0 = oracle_at_settled_frame(args, scene, threads)
+    first = first_timed_frame(args)
+    o, f0 = oracle_at_frame(args, scene, threads, first)
     budget = 150.0
-    t0 = time.time()
     w = n = 0
+    t1 = time.time()
     try:
-        while w < max(3, args.warmup) and time.time() - t0 < budget / 4:
+        # steps from the restored frame up to the GPU arm's first timed frame
+        # (none when the state of that frame is saved)
+        while f0 + w < first:
             o.step(); w += 1
         t1 = time.time()
         while n < args.steps and (n == 0 or time.time() - t1 < budget):
@@ -275,14 +286,17 @@ def run_reference(args, world, rank):
         return
     dt = time.time() - t1
     v = n / dt
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": n, "warmup": w,
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": n, "warmup": args.warmup,
             "ms_per_step": 1000 * dt / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": workload(args),
+            "data": "synthetic", "config": {"workload": workload(args), "description": describe(args),
+                                            "newton_threshold": scene["params"]["newtonThr"],
                                             "solver": "FP64 CPU restatement of the reference pipeline; linear solve by a parallel multifrontal "
                                                       "Cholesky under nested dissection (the PARDISO algorithm class)",
-                                            "timed_frames": f"{f0 + w}-{f0 + w + n - 1}"},
+                                            "timed_frames": f"{f0 + w}-{f0 + w + n - 1}",
+                                            "warm_start": (f"restored the oracle's saved state at frame {f0}" if f0 else "frame 0") +
+                                                          (f", then {w} untimed steps" if w else "")},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{frames(f0 + w, n, f0 > 0)} after {w} warm-up steps; the reference itself does not compile here"},
+                             "sample": f"{frames(f0 + w, n, f0 > 0)}, bounded to {budget:.0f} s; the reference itself does not compile here"},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -447,7 +461,7 @@ def main():
                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic("pcg"),
                     "algorithmic_bytes_per_launch": bytes_, "bytes_per_iteration": per_it, "launches": r["nprof"],
                     "mean_launch_us": 1000 * avg_ms, "share_of_step_time": r["prof_ms"] / r["ms"]}
-        cfg = {"workload": workload(args, detail=True),
+        cfg = {"workload": workload(args), "description": describe(args), "newton_threshold": scene["params"]["newtonThr"],
                "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
                "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
                "ms_per_newton_iteration": max_ms / max(1, r["newton"]),

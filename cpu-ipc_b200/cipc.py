@@ -98,6 +98,7 @@ def lib():
         L.cipc_gpu_step_bounds.argtypes = [vp, _dp, C.c_double, _dp]
         L.cipc_gpu_intersected.argtypes = [vp, _ip]
         L.cipc_gpu_pcg_bsr.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, C.POINTER(LinearOptions), _ip, _dp, C.c_char_p, C.c_int]
+        L.cipc_gpu_accd.argtypes = [C.c_int, _ip, _dp, _dp, C.c_double, _dp, C.c_char_p, C.c_int]
         L.cipc_gpu_timed_steps.argtypes = [vp, C.c_int, C.POINTER(StepStats), _dp]
         L.cipc_gpu_profile.argtypes = [vp, C.c_int, C.c_int]
         L.cipc_gpu_profile_read.argtypes = [vp, C.POINTER(C.c_longlong), _dp]
@@ -122,7 +123,7 @@ EXPORTED_SYMBOLS = [
     "cipc_gpu_get_state", "cipc_gpu_set_state", "cipc_gpu_get_scalars", "cipc_gpu_set_kappa", "cipc_gpu_set_intersection_rule", "cipc_gpu_get_counts",
     "cipc_gpu_get_surface", "cipc_gpu_build_collision_sets", "cipc_gpu_get_active_sets", "cipc_gpu_friction_init",
     "cipc_gpu_assemble", "cipc_gpu_export_matrix", "cipc_gpu_solve", "cipc_gpu_energy", "cipc_gpu_step_bounds",
-    "cipc_gpu_intersected", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
+    "cipc_gpu_intersected", "cipc_gpu_accd", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
     "cipc_gpu_kernel_launches", "cipc_gpu_pcg_bsr_noalloc", "cipc_gpu_export_bsr", "cipc_gpu_precond_num_params",
     "cipc_gpu_precond_set_weights", "cipc_gpu_precond_get_weights", "cipc_gpu_precond_loss", "cipc_gpu_precond_train",
     "cipc_gpu_precond_stats", "cipc_gpu_precond_factor",
@@ -413,6 +414,24 @@ def pcg_bsr(row_ptr, col_idx, vals, rhs, precision="fp64", tol=1e-6, max_iter=10
     if rc != CIPC_OK:
         raise CipcError(rc, err.value.decode())
     return sol, it.value, rr.value
+
+
+def accd(kind, positions, displacements, eta=0.2):
+    """Conservative time of impact of independent candidate pairs on the GPU
+    (kind 0 point-triangle, 1 edge-edge; positions and displacements n x 4 x 3)."""
+    L = lib()
+    k = np.ascontiguousarray(kind, np.int32).reshape(-1)
+    p = np.ascontiguousarray(positions, np.float64).reshape(-1)
+    d = np.ascontiguousarray(displacements, np.float64).reshape(-1)
+    n = len(k)
+    if p.size != 12 * n or d.size != 12 * n:
+        raise ValueError("positions and displacements need 12 values per pair")
+    out = np.zeros(n)
+    err = C.create_string_buffer(512)
+    rc = L.cipc_gpu_accd(n, _i(k), _d(p), _d(d), float(eta), _d(out), err, 512)
+    if rc != CIPC_OK:
+        raise CipcError(rc, err.value.decode())
+    return out
 
 
 # ---------------------------------------------------------------------------

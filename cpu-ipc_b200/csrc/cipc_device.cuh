@@ -181,6 +181,7 @@ CIPC_HD void jacobiSym3(T S[3][3], T V[3][3]) {
         T off = S[0][1] * S[0][1] + S[0][2] * S[0][2] + S[1][2] * S[1][2];
         T dg = S[0][0] * S[0][0] + S[1][1] * S[1][1] + S[2][2] * S[2][2];
         if (off <= T(1e-34) * dg || off == T(0)) break;
+#pragma unroll
         for (int pq = 0; pq < 3; ++pq) {
             int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
             T apq = S[p][q];
@@ -215,7 +216,9 @@ CIPC_HD void svd3(const T F[3][3], T U[3][3], T s[3], T V[3][3]) {
     jacobiSym3(S, V);
     T ev[3] = {S[0][0], S[1][1], S[2][2]};
     // sort descending with V columns
+#pragma unroll
     for (int a = 0; a < 2; ++a)
+#pragma unroll
         for (int b = 0; b < 2 - a; ++b)
             if (ev[b] < ev[b + 1]) {
                 T t = ev[b]; ev[b] = ev[b + 1]; ev[b + 1] = t;
@@ -229,9 +232,9 @@ CIPC_HD void svd3(const T F[3][3], T U[3][3], T s[3], T V[3][3]) {
         for (int j = 0; j < 3; ++j) R[i][j] = F[i][0] * V[0][j] + F[i][1] * V[1][j] + F[i][2] * V[2][j];
     T Q[3][3];
     for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Q[i][j] = (i == j) ? T(1) : T(0);
-    const int pr[3][2] = {{1, 0}, {2, 0}, {2, 1}};
+#pragma unroll
     for (int g = 0; g < 3; ++g) {
-        int i = pr[g][0], j = pr[g][1];
+        const int i = g == 0 ? 1 : 2, j = g == 2 ? 1 : 0;  // (1,0), (2,0), (2,1)
         T a = R[j][j], b = R[i][j];
         T r = sqrt(a * a + b * b);
         T c = T(1), sn = T(0);

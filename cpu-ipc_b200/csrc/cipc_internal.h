@@ -226,6 +226,7 @@ inline void profEnd(Ctx& c, int kind) {
 // ---- launchers (elastic.cu) ----
 void buildStaticPattern(Ctx& c, const std::vector<int>& tets, const std::vector<int>& tris, const std::vector<int>& bendV);
 void assembleElastic(Ctx& c);          // vtxGrad, diagExtra, element blocks, static BSR values, element gradient
+void tetGradient(Ctx& c);              // elemG of the tetrahedra only (no Hessian)
 double elasticEnergy(Ctx& c);          // (SNH + BW + bending) * dt^2 + inertia + soft, FP64
 void gatherGradient(Ctx& c);           // grad = vtxGrad + element + dynamic contributions
 void initKappaGradE(Ctx& c, double* gE);  // inertia + tet elastic gradient into device buffer gE
@@ -237,6 +238,7 @@ void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, boo
 void buildCollisionSets(Ctx& c, bool rehash);
 void groundActiveSet(Ctx& c);
 bool isIntersected(Ctx& c);
+void accdBatch(int n, const int* kind, const double* p, const double* d, double eta, double* toi);  // host arrays
 double groundStepBound(Ctx& c);
 double partialCCD(Ctx& c, double alpha);
 double cflBound(Ctx& c);

@@ -764,4 +764,48 @@ double fullCCDDir(Ctx& c, const double* d, double alpha) {
 
 double fullCCD(Ctx& c, double alpha) { return fullCCDDir(c, c.dir, alpha); }
 
+
+// Additive CCD on a batch of independent candidate pairs (the per-pair time
+// of impact of Self_largestFeasibleStepSize, ContactMechanics.cpp:3704-3752,
+// AdditiveCCD.cpp:221-329): kind 0 point-triangle (point, t0, t1, t2), kind 1
+// edge-edge (a0, a1, b0, b1); 12 positions and 12 displacements per pair.
+namespace {
+__global__ void accdBatchKernel(int n, const int* kind, const double* p, const double* d, double eta, double* toi, int* status) {
+    CIPC_KERNEL_LOOP(k, n) {
+        const double* q = p + 12 * (size_t)k;
+        const double* m = d + 12 * (size_t)k;
+        d3 x[4], v[4];
+        for (int a = 0; a < 4; ++a) {
+            x[a] = mk(q[3 * a], q[3 * a + 1], q[3 * a + 2]);
+            v[a] = mk(m[3 * a], m[3 * a + 1], m[3 * a + 2]);
+        }
+        toi[k] = kind[k] == 0 ? pointTriangleCCD(x[0], x[1], x[2], x[3], v[0], v[1], v[2], v[3], eta, status)
+                              : edgeEdgeCCD(x[0], x[1], x[2], x[3], v[0], v[1], v[2], v[3], eta, status);
+    }
+}
+}  // namespace
+
+void accdBatch(int n, const int* kind, const double* p, const double* d, double eta, double* toi) {
+    DBuf<int> dk, st;
+    DBuf<double> dp, dd, dt;
+    try {
+        dk.reserve(n); dp.reserve(12 * (size_t)n); dd.reserve(12 * (size_t)n); dt.reserve(n); st.reserve(1);
+        CIPC_CUDA(cudaMemcpy(dk.p, kind, sizeof(int) * n, cudaMemcpyHostToDevice));
+        CIPC_CUDA(cudaMemcpy(dp.p, p, sizeof(double) * 12 * (size_t)n, cudaMemcpyHostToDevice));
+        CIPC_CUDA(cudaMemcpy(dd.p, d, sizeof(double) * 12 * (size_t)n, cudaMemcpyHostToDevice));
+        CIPC_CUDA(cudaMemset(st.p, 0, sizeof(int)));
+        launch(accdBatchKernel, blocksFor(n), TB, 0, (cudaStream_t)0, n, (const int*)dk.p, (const double*)dp.p, (const double*)dd.p, eta,
+               dt.p, st.p);
+        CIPC_CUDA(cudaGetLastError());
+        int hs = 0;
+        CIPC_CUDA(cudaMemcpy(toi, dt.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        CIPC_CUDA(cudaMemcpy(&hs, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (hs & CIPC_ST_CCD_CAP) throw std::runtime_error("a pair reached the CCD iteration cap");
+    } catch (...) {
+        dk.free(); dp.free(); dd.free(); dt.free(); st.free();
+        throw;
+    }
+    dk.free(); dp.free(); dd.free(); dt.free(); st.free();
+}
+
 }  // namespace cipc

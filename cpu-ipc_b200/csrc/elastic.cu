@@ -45,123 +45,215 @@ __global__ void softKernel(int ns, const int* idx, const double* target, double 
     }
 }
 
-// G rows: dF/dx_a = G[a][c] (column c of F), a = 0..3.
-__device__ __forceinline__ void tetG(const double* Di, double G[4][3]) {
-    for (int c = 0; c < 3; ++c) {
-        G[1][c] = Di[0 * 3 + c];
-        G[2][c] = Di[1 * 3 + c];
-        G[3][c] = Di[2 * 3 + c];
-        G[0][c] = -(G[1][c] + G[2][c] + G[3][c]);
+// Stable Neo-Hookean tetrahedra (PK1 Elasticity.cpp:1144-1170, Hessian and
+// makePD 1337-1479, scatter IPCSolver.cpp:139-164), tiled in two phases.
+//
+// Phase 1, one thread per tetrahedron: F = Ds Dm^-1, the gradient
+// vol dt^2 P(F) G^T, and the Hessian's analytic eigensystem in F space - the
+// rotation-aware SVD F = U diag(s) V^T, 3 scaling modes (a 3x3 eigenproblem
+// in the singular-value basis) and 3 twist + 3 flip modes with closed-form
+// eigenvalues mu Ic/(Ic+1) +/- lambda (J - alpha) s_k.  Each mode m with
+// eigenvalue e_m > 0 leaves w_m[a] = sqrt(vol dt^2 e_m) Q_m G_a (3 values per
+// vertex a) in shared memory, so that the projected 12x12 Hessian is
+// sum_m w_m w_m^T (the PSD projection of project_StabbleNHK_2_H_3D's 9x9
+// matrix pulled back through PFPX).
+//
+// Phase 2, the CTA's threads over (tetrahedron, lower block, block row):
+// each forms 3 entries of one lower 3x3 block, sum_m w_m[a][r] w_m[b][q],
+// and stores them next to its neighbours' (the tile's element blocks are one
+// contiguous range of elemH, 90 values per tetrahedron).  Blocks touching a
+// constrained vertex are zeroed as the reference drops them.
+// ---------------------------------------------------------------------------
+template <class T>
+struct TetTile;
+template <>
+struct TetTile<float> { static constexpr int N = 128; };
+template <>
+struct TetTile<double> { static constexpr int N = 64; };
+constexpr int TET_W = 109;  // 9 modes x 4 vertices x 3, padded to an odd stride (bank spread)
+
+// mode m (0..8) of the SNH Hessian eigensystem: eigenvalue and Q_m (3x3)
+template <class T>
+__device__ __forceinline__ T snhMode(int m, const T U[3][3], const T V[3][3], const T W[3][3], const T A[3][3], const T s[3], T Ut, T lJ,
+                                     T Q[3][3]) {
+    if (m < 3) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) Q[r][c] = U[r][0] * W[0][m] * V[c][0] + U[r][1] * W[1][m] * V[c][1] + U[r][2] * W[2][m] * V[c][2];
+        return A[m][m];
     }
+    const int t = (m - 3) % 3;
+    const int i = t == 2 ? 1 : 0, j = t == 0 ? 1 : 2, k = 3 - i - j;
+    const bool twist = m < 6;
+    const T sg = twist ? T(-1) : T(1);
+    const T isq2 = T(0.70710678118654752440);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Q[r][c] = isq2 * (U[r][i] * V[c][j] + sg * U[r][j] * V[c][i]);
+    return twist ? Ut + lJ * s[k] : Ut - lJ * s[k];
 }
 
-// Stable Neo-Hookean Hessian, projected to PSD through its analytic
-// eigensystem: 3 scaling modes (3x3 eigenproblem in the singular-value
-// basis), 3 twist and 3 flip modes with closed-form eigenvalues
-// mu*Ic/(Ic+1) +/- lambda*(J-alpha)*sigma_k.  Equals makePD of the closed-form
-// 9x9 matrix of project_StabbleNHK_2_H_3D.
-template <class T>
-__device__ void snhProjectedBlocks(const double Fd[3][3], double mu, double lam, const double G[4][3], double scale, T* out) {
-    T F[3][3], U[3][3], V[3][3], s[3];
-    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) F[i][j] = T(Fd[i][j]);
-    svd3<T>(F, U, s, V);
-    T Ic = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
-    T J = s[0] * s[1] * s[2];
-    T Ut = T(mu) * Ic / (Ic + T(1));
-    T lJ = T(lam) * (J - T(1) - T(3) * T(mu) / (T(4) * T(lam)));
-    T gC = T(mu) / (T(2) * (Ic + T(1)) * (Ic + T(1)));
-    T cf[3] = {s[1] * s[2], s[0] * s[2], s[0] * s[1]};
-    T A[3][3];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-            A[i][j] = gC * T(4) * s[i] * s[j] + T(lam) * cf[i] * cf[j];
-            if (i == j) A[i][j] += Ut;
-            else A[i][j] += lJ * s[3 - i - j];
-        }
-    T W[3][3];
-    jacobiSym3<T>(A, W);
-    T acc[10][9];
-    for (int b = 0; b < 10; ++b) for (int e = 0; e < 9; ++e) acc[b][e] = T(0);
-    const T isq2 = T(0.70710678118654752440);
-    for (int m = 0; m < 9; ++m) {
-        T ev;
-        T Q[3][3];
-        if (m < 3) {
-            ev = A[m][m];
-            if (!(ev > T(0))) continue;
+template <class T, bool HESS>
+__global__ void __launch_bounds__(TetTile<T>::N) tetKernel(int nt, const int* tets, const double* x, const double* DmInv, const double* vol,
+                                                           const double* tmu, const double* tlam, const int* btype, double dt2, double* elemG,
+                                                           T* elemH) {
+    constexpr int N = TetTile<T>::N;
+    // dynamic shared memory (tetSmemBytes): gradients, modes, free flags
+    extern __shared__ __align__(16) unsigned char tetSmem[];
+    double* sg = reinterpret_cast<double*>(tetSmem);
+    T* sw = reinterpret_cast<T*>(tetSmem + sizeof(double) * 12 * N);
+    unsigned char* sfree = tetSmem + sizeof(double) * 12 * N + (HESS ? sizeof(T) * TET_W * N : 0);
+    const int tid = threadIdx.x;
+    for (int base = blockIdx.x * N; base < nt; base += gridDim.x * N) {
+        const int cnt = min(N, nt - base);
+        if (tid < cnt) {
+            const int i = base + tid;
+            int v[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) v[a] = tets[4 * i + a];
+            double Di[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Di[k] = DmInv[9 * (size_t)i + k];
+            const d3 x0 = ld3(x, v[0]);
+            const d3 e1 = ld3(x, v[1]) - x0, e2 = ld3(x, v[2]) - x0, e3 = ld3(x, v[3]) - x0;
+            const double Ds[3][3] = {{e1.x, e2.x, e3.x}, {e1.y, e2.y, e3.y}, {e1.z, e2.z, e3.z}};
+            double F[3][3];
+#pragma unroll
             for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c)
-                    Q[r][c] = U[r][0] * W[0][m] * V[c][0] + U[r][1] * W[1][m] * V[c][1] + U[r][2] * W[2][m] * V[c][2];
-        } else {
-            int t = (m - 3) % 3;
-            int i = t == 2 ? 1 : 0, j = t == 0 ? 1 : 2, k = 3 - i - j;
-            bool twist = m < 6;
-            ev = twist ? Ut + lJ * s[k] : Ut - lJ * s[k];
-            if (!(ev > T(0))) continue;
-            T sg = twist ? T(-1) : T(1);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) F[r][c] = Ds[r][0] * Di[c] + Ds[r][1] * Di[3 + c] + Ds[r][2] * Di[6 + c];
+            const double u = tmu[i], lr = tlam[i];
+            double I2 = 0;
+#pragma unroll
             for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) Q[r][c] = isq2 * (U[r][i] * V[c][j] + sg * U[r][j] * V[c][i]);
-        }
-        T w[4][3];
-        for (int a = 0; a < 4; ++a)
-            for (int r = 0; r < 3; ++r) w[a][r] = Q[r][0] * T(G[a][0]) + Q[r][1] * T(G[a][1]) + Q[r][2] * T(G[a][2]);
-        for (int a = 0; a < 4; ++a)
-            for (int b = 0; b <= a; ++b) {
-                T* blk = acc[lowerIdx(a, b)];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) I2 += F[r][c] * F[r][c];
+            double cof[3][3];
+            cof[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+            cof[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+            cof[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+            cof[1][0] = F[2][1] * F[0][2] - F[2][2] * F[0][1];
+            cof[1][1] = F[2][2] * F[0][0] - F[2][0] * F[0][2];
+            cof[1][2] = F[2][0] * F[0][1] - F[2][1] * F[0][0];
+            cof[2][0] = F[0][1] * F[1][2] - F[1][1] * F[0][2];
+            cof[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+            cof[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+            const double J = F[0][0] * cof[0][0] + F[0][1] * cof[0][1] + F[0][2] * cof[0][2];
+            const double ca = u * (1 - 1 / (I2 + 1)), cb = lr * (J - 1 - u * 3 / (lr * 4));
+            // G rows: dF/dx_a = G[a][c] (column c of F)
+            double G[4][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                G[1][c] = Di[c]; G[2][c] = Di[3 + c]; G[3][c] = Di[6 + c];
+                G[0][c] = -(G[1][c] + G[2][c] + G[3][c]);
+            }
+            const double sc = vol[i] * dt2;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
                 for (int r = 0; r < 3; ++r) {
-                    T er = ev * w[a][r];
-                    for (int q = 0; q < 3; ++q) blk[3 * r + q] += er * w[b][q];
+                    double f = 0;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f += (ca * F[r][c] + cb * cof[r][c]) * G[a][c];
+                    sg[12 * tid + 3 * a + r] = sc * f;
+                }
+            if (HESS) {
+                unsigned char fr = 0;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) fr |= (btype[v[a]] == 0 ? 1 : 0) << a;
+                sfree[tid] = fr;
+                T Ft[3][3], U[3][3], V[3][3], s[3];
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) Ft[r][c] = T(F[r][c]);
+                svd3<T>(Ft, U, s, V);
+                const T Ic = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+                const T Jt = s[0] * s[1] * s[2];
+                const T Ut = T(u) * Ic / (Ic + T(1));
+                const T lJ = T(lr) * (Jt - T(1) - T(3) * T(u) / (T(4) * T(lr)));
+                const T gC = T(u) / (T(2) * (Ic + T(1)) * (Ic + T(1)));
+                const T cf[3] = {s[1] * s[2], s[0] * s[2], s[0] * s[1]};
+                T A[3][3];
+#pragma unroll
+                for (int p = 0; p < 3; ++p)
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        A[p][q] = gC * T(4) * s[p] * s[q] + T(lr) * cf[p] * cf[q];
+                        if (p == q) A[p][q] += Ut;
+                        else A[p][q] += lJ * s[3 - p - q];
+                    }
+                T W[3][3];
+                jacobiSym3<T>(A, W);
+                T* w = sw + TET_W * tid;
+#pragma unroll
+                for (int m = 0; m < 9; ++m) {
+                    T Q[3][3];
+                    const T ev = snhMode<T>(m, U, V, W, A, s, Ut, lJ, Q);
+                    const T coef = ev > T(0) ? sqrt(T(sc) * ev) : T(0);
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int r = 0; r < 3; ++r)
+                            w[12 * m + 3 * a + r] = coef * (Q[r][0] * T(G[a][0]) + Q[r][1] * T(G[a][1]) + Q[r][2] * T(G[a][2]));
                 }
             }
+        }
+        __syncthreads();
+        // the tile's gradients: 12 consecutive doubles per tetrahedron
+        for (int o = tid; o < 12 * cnt; o += N) elemG[(size_t)12 * base + o] = sg[o];
+        if (HESS) {
+            // (tetrahedron, lower block, block row) items: 3 consecutive
+            // entries of elemH each, consecutive items consecutive in memory
+            T* out = elemH + (size_t)90 * base;
+            for (int it = tid; it < 30 * cnt; it += N) {
+                const int t = it / 30, rest = it - 30 * t;
+                const int blk = rest / 3, r = rest - 3 * blk;
+                const int a = blk >= 6 ? 3 : (blk >= 3 ? 2 : (blk >= 1 ? 1 : 0));
+                const int b = blk - a * (a + 1) / 2;  // lowerIdx(a, b) = blk
+                const T* w = sw + TET_W * t;
+                T h0 = T(0), h1 = T(0), h2 = T(0);
+#pragma unroll
+                for (int m = 0; m < 9; ++m) {
+                    const T wa = w[12 * m + 3 * a + r];
+                    h0 += wa * w[12 * m + 3 * b];
+                    h1 += wa * w[12 * m + 3 * b + 1];
+                    h2 += wa * w[12 * m + 3 * b + 2];
+                }
+                const unsigned fr = sfree[t];
+                const bool keep = ((fr >> a) & 1u) && ((fr >> b) & 1u);
+                T* o = out + 90 * t + 9 * blk + 3 * r;
+                o[0] = keep ? h0 : T(0);
+                o[1] = keep ? h1 : T(0);
+                o[2] = keep ? h2 : T(0);
+            }
+        }
+        __syncthreads();
     }
-    for (int b = 0; b < 10; ++b) for (int e = 0; e < 9; ++e) out[9 * b + e] = T(scale) * acc[b][e];
 }
 
-template <class T>
-__global__ void tetKernel(int nt, const int* tets, const double* x, const double* DmInv, const double* vol, const double* tmu,
-                          const double* tlam, const int* btype, double dt2, double* elemG, T* elemH) {
-    CIPC_KERNEL_LOOP(i, nt) {
-        int v[4];
-        for (int a = 0; a < 4; ++a) v[a] = tets[4 * i + a];
-        const double* Di = DmInv + 9 * i;
-        d3 x0 = ld3(x, v[0]);
-        d3 e1 = ld3(x, v[1]) - x0, e2 = ld3(x, v[2]) - x0, e3 = ld3(x, v[3]) - x0;
-        double Ds[3][3] = {{e1.x, e2.x, e3.x}, {e1.y, e2.y, e3.y}, {e1.z, e2.z, e3.z}};
-        double F[3][3];
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) F[r][c] = Ds[r][0] * Di[c] + Ds[r][1] * Di[3 + c] + Ds[r][2] * Di[6 + c];
-        double u = tmu[i], lr = tlam[i];
-        double I2 = 0;
-        for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) I2 += F[r][c] * F[r][c];
-        double cof[3][3];
-        cof[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
-        cof[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
-        cof[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
-        cof[1][0] = F[2][1] * F[0][2] - F[2][2] * F[0][1];
-        cof[1][1] = F[2][2] * F[0][0] - F[2][0] * F[0][2];
-        cof[1][2] = F[2][0] * F[0][1] - F[2][1] * F[0][0];
-        cof[2][0] = F[0][1] * F[1][2] - F[1][1] * F[0][2];
-        cof[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
-        cof[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
-        double J = F[0][0] * cof[0][0] + F[0][1] * cof[0][1] + F[0][2] * cof[0][2];
-        double ca = u * (1 - 1 / (I2 + 1)), cb = lr * (J - 1 - u * 3 / (lr * 4));
-        double G[4][3];
-        tetG(Di, G);
-        double sc = vol[i] * dt2;
-        for (int a = 0; a < 4; ++a)
-            for (int r = 0; r < 3; ++r) {
-                double f = 0;
-                for (int c = 0; c < 3; ++c) f += (ca * F[r][c] + cb * cof[r][c]) * G[a][c];
-                elemG[3 * (4 * i + a) + r] = sc * f;
-            }
-        T* out = elemH + (size_t)90 * i;
-        snhProjectedBlocks<T>(F, u, lr, G, sc, out);
-        bool fr[4];
-        for (int a = 0; a < 4; ++a) fr[a] = btype[v[a]] == 0;
-        for (int a = 0; a < 4; ++a)
-            for (int b = 0; b <= a; ++b)
-                if (!(fr[a] && fr[b])) for (int e = 0; e < 9; ++e) out[9 * lowerIdx(a, b) + e] = T(0);
+template <class T, bool HESS>
+constexpr size_t tetSmemBytes() {
+    return sizeof(double) * 12 * TetTile<T>::N + (HESS ? sizeof(T) * TET_W * TetTile<T>::N : 0) + TetTile<T>::N;
+}
+
+// Launch of the tiled tetrahedron kernel: one tile of N tetrahedra per CTA
+// pass, grid-stride over the tiles.  The dynamic shared memory exceeds the
+// 48 KB default, so the limit is raised once per instantiation.
+template <class T, bool HESS>
+void launchTet(Ctx& c, double dt2, T* elemH) {
+    constexpr int N = TetTile<T>::N;
+    constexpr size_t smem = tetSmemBytes<T, HESS>();
+    static bool attr = false;
+    if (!attr) {
+        CIPC_CUDA(cudaFuncSetAttribute(tetKernel<T, HESS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
     }
+    const int tiles = (c.nt + N - 1) / N;
+    launch(tetKernel<T, HESS>, std::max(1, std::min(tiles, 148 * 16)), N, smem, c.s, c.nt, c.tets, c.x, c.DmInv, c.vol, c.tetMu, c.tetLam,
+           c.btype, dt2, c.elemG, elemH);
 }
 
 // Baraff-Witkin membrane, project_baraffwitkint_H_3D + computePEPF_baraffwitkin_double.
@@ -507,7 +599,7 @@ static void assembleElasticT(Ctx& c, T* elemH, T* val) {
     double dt2 = P.dt * P.dt;
     if (c.nt) {
         profBegin(c, PROF_TET);
-        launch(tetKernel<T>, blocksFor(c.nt), TB, 0, c.s, c.nt, c.tets, c.x, c.DmInv, c.vol, c.tetMu, c.tetLam, c.btype, dt2, c.elemG, elemH);
+        launchTet<T, true>(c, dt2, elemH);
         profEnd(c, PROF_TET);
     }
     profBegin(c, PROF_TRI);
@@ -599,8 +691,16 @@ __global__ void gradEKernel(int nv, const double* x, const double* xt, const dou
 }
 }  // namespace
 
+// The tetrahedra's elastic gradients alone (elemG), for the kappa
+// initialisation: no Hessian work.
+void tetGradient(Ctx& c) {
+    if (c.nt) launchTet<float, false>(c, c.P.dt * c.P.dt, (float*)nullptr);
+    CIPC_CUDA(cudaGetLastError());
+}
+
 // computeEGradient (IPCSolver.cpp:72-106): inertia (no drag) plus the
-// tetrahedral elastic gradient.  Requires elemG from assembleElastic at x.
+// tetrahedral elastic gradient.  Requires elemG from assembleElastic or
+// tetGradient at x.
 void initKappaGradE(Ctx& c, double* gE) {
     launch(gradEKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.mass, c.gcPtr, c.gcIdx, c.elemG, 4 * c.nt, gE);
     CIPC_CUDA(cudaGetLastError());

@@ -86,7 +86,7 @@ void upperBoundKappa(double& kappa, double Hhat, double bbox2, double meanMass) 
 // initKappa (IPCSolver.cpp:770-809); `kappa` may alias c.P.kappa.
 void initKappa(Ctx& c, double& kappa) {
     if (c.nGround + c.nSelf == 0) return;
-    assembleElastic(c);  // elemG holds the tetrahedral gradient at x
+    tetGradient(c);  // elemG holds the tetrahedral gradient at x
     c.scratch.reserve(8 + 1024);
     DBuf<double>& gE = c.z;
     DBuf<double>& gc = c.Ap;
@@ -947,6 +947,27 @@ int cipc_gpu_precond_stats(cipc_gpu_context* h, long long* out) {
 }
 
 }  // extern "C"
+
+extern "C" int cipc_gpu_accd(int n, const int* kind, const double* positions, const double* displacements, double eta, double* toi, char* err,
+                             int errlen) {
+    auto fail = [&](const char* m, int code) {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", m);
+        return code;
+    };
+    if (n < 0 || (n > 0 && (!kind || !positions || !displacements || !toi)) || !(eta > 0.0 && eta <= 1.0))
+        return fail("invalid arguments", CIPC_ERR_INVALID_ARGUMENT);
+    if (n == 0) return CIPC_OK;
+    for (int k = 0; k < n; ++k)
+        if (kind[k] != 0 && kind[k] != 1) return fail("pair kind must be 0 (point-triangle) or 1 (edge-edge)", CIPC_ERR_INVALID_ARGUMENT);
+    try {
+        cipc::accdBatch(n, kind, positions, displacements, eta, toi);
+    } catch (const cipc::CudaError& e) {
+        return fail(e.what(), CIPC_ERR_CUDA);
+    } catch (const std::exception& e) {
+        return fail(e.what(), CIPC_ERR_RUNTIME);
+    }
+    return CIPC_OK;
+}
 
 extern "C" int cipc_gpu_pcg_bsr(int nv, const int* rowPtr, const int* colIdx, const double* vals, const double* rhs, double* sol,
                                 const cipc_linear_options* options, int* iterations, double* relResidual, char* err, int errlen) {

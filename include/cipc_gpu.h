@@ -221,6 +221,15 @@ int cipc_gpu_precond_factor(cipc_gpu_context* ctx, int which, float* gStatic, fl
  * were set, out[2] iterations of the last PCG launch. */
 int cipc_gpu_precond_stats(cipc_gpu_context* ctx, long long* out3);
 
+/* Additive CCD (AdditiveCCD.cpp:221-329, the per-pair time of impact of
+ * Self_largestFeasibleStepSize, ContactMechanics.cpp:3704-3752) on n
+ * independent candidate pairs, host arrays: kind[k] 0 point-triangle
+ * (positions point, t0, t1, t2), 1 edge-edge (a0, a1, b0, b1); 12 positions
+ * and 12 displacements per pair; eta = 1 - slackness (the reference uses 0.2).
+ * toi[k] in [0, 1] is the conservative step along the displacements. */
+int cipc_gpu_accd(int n, const int* kind, const double* positions, const double* displacements, double eta, double* toi, char* err,
+                  int errlen);
+
 /* Stand-alone GPU PCG on a caller-given matrix (full symmetric 3x3-block CSR,
  * FP64 values, 9 per block row-major) - the backend switch of
  * NewtonLinearSystem::solve (NewtonLinearSystem.cpp:41-53) without a scene.

@@ -1,8 +1,9 @@
 """bench.py --impl reference on the host cores, no GPU: one JSON line with the
 metric, unit and direction of the GPU arm, a cpu_baseline describing the run
-and an e2e entry without host-device copies.  A small cloth keeps it short
-(it starts from frame 0: saved contact states exist for the 128x128 cloth
-only); the restore of that saved state is covered by test_oracle_state.py."""
+and an e2e entry without host-device copies.  A small cloth without settle
+steps keeps it short (it starts from frame 0 and steps to the first timed
+frame: saved contact states exist for the bench sizes only); the restore of
+a saved state is covered by test_oracle_state.py."""
 import json
 import os
 import subprocess
@@ -13,7 +14,8 @@ BENCH = os.path.join(HERE, "..", "bench.py")
 
 
 def test_reference_arm_prints_one_contract_line():
-    r = subprocess.run([sys.executable, BENCH, "--impl", "reference", "--cloth", "16", "--steps", "2", "--warmup", "3"],
+    r = subprocess.run([sys.executable, BENCH, "--impl", "reference", "--scene", "cloth_drape", "--cloth", "16", "--settle-steps", "0",
+                        "--steps", "2", "--warmup", "3"],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     lines = [ln for ln in r.stdout.splitlines() if ln.strip()]

@@ -1,0 +1,217 @@
+"""Parity of the CUDA path with the FP64 oracle at the benchmark
+configurations' own sizes.
+
+* Two cubes of 8^3 cells (3,072 tets each), Newton tolerance 1e-6, FP64, 100
+  steps from rest: trajectories within 1e-6 of the bounding-box diagonal,
+  checked every 10 steps.
+* The 128x128 cloth drape (16,384 cloth vertices on the 10^3-cell cube) and an
+  8-cube pile of 12^3 cells, each from a contact-phase state the oracle
+  itself produced (oracle/states/): contact sets bit-exact; gradient, Newton
+  matrix and energy within 1e-10 relative; step bounds within 1e-6 and never
+  above the oracle's; then three steps of trajectory in FP64 and in mixed
+  precision with the learned factor (weights trained on the restored system,
+  then frozen), within 1e-6 of the bounding-box diagonal.
+* A twisted cylinder of 8 x 32 x 64 layers (92,160 tets, animated Dirichlet
+  caps): ten steps of trajectory.
+* Additive CCD candidate by candidate: every partial-CCD candidate pair of
+  the cloth contact state, and random near-contact pairs, against the
+  oracle's time of impact (within 1e-6 relative, never larger).
+"""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import cipc
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+STATES = os.path.join(ROOT, "oracle", "states")
+GRAD_TOL = 1e-10
+HESS_TOL = 1e-10
+ENERGY_TOL = 1e-10
+TRAJ_TOL = 1e-6
+THREADS = os.cpu_count() or 1
+
+
+def _restore_gpu(g, path, dt, apply_gravity=True):
+    """The state a saved oracle step starts from, on the GPU simulator: the
+    same fields the oracle's restore_state sets, then the collision sets at
+    the restored positions."""
+    s = np.load(path)
+    x, vel = s["x"], s["vel"]
+    xt = x + vel * dt + np.array([0.0, float(s["gravity"]) * dt * dt, 0.0])
+    g.set("x", x); g.set("vprev", x); g.set("vel", vel); g.set("xtilde", xt)
+    g.set_kappa(float(s["kappa"]))
+    g.collision_sets()
+
+
+def _canon(S):
+    return [sorted(map(tuple, S[k].tolist())) for k in ("self_active", "self_ee", "ccd")] + [sorted(S["ground"].tolist())]
+
+
+def _oracle_full_matrix(rp, col, val, n):
+    L = sp.csr_matrix((val, col, rp), shape=(n, n))
+    return (L + L.T - sp.diags(L.diagonal())).tocsr()
+
+
+def _gpu_full_matrix(g, btype):
+    r, c, v = g.export_matrix()
+    n = 3 * g.nv
+    A = sp.coo_matrix((v, (r, c)), shape=(n, n)).tocsr()
+    free = np.repeat(btype == 0, 3)
+    D = sp.diags(free.astype(float))
+    return (D @ A @ D + sp.diags((~free) * A.diagonal())).tocsr()
+
+
+def test_two_cubes_8_cells_100_steps(oracle_mod):
+    sc = cipc.scene_two_cubes(8)  # Newton tolerance 1e-6
+    assert len(sc["tets"]) == 2 * 3072
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=THREADS)
+    g = cipc.Simulator(sc, surface=o.surface())
+    bb = np.sqrt(o.scalars()["bboxDiag2"])
+    worst = 0.0
+    for s in range(100):
+        o.step(); g.step()
+        if (s + 1) % 10 == 0:
+            err = np.abs(o.get("x") - g.get("x")).max() / bb
+            worst = max(worst, err)
+            assert err <= TRAJ_TOL, (s + 1, err)
+    print(f"two cubes 8^3, 100 steps: worst trajectory error {worst:.2e} x bbox")
+
+
+CONTACT_STATES = {
+    "cloth_drape_128": (lambda: cipc.scene_cloth_drape(128, 10), "cloth_drape_128_frame40.npz"),
+    "pile_8x12": (lambda: cipc.scene_pile(8, 12), "pile_8x12_frame60.npz"),
+}
+
+
+@pytest.fixture(scope="module", params=list(CONTACT_STATES))
+def contact_state(request, oracle_mod):
+    make, fname = CONTACT_STATES[request.param]
+    sc = make()
+    path = os.path.join(STATES, fname)
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=THREADS)
+    o.restore_state(path)
+    return request.param, sc, path, o
+
+
+def test_contact_state_sets_system_bounds(oracle_mod, contact_state):
+    name, sc, path, o = contact_state
+    g = cipc.Simulator(sc, surface=o.surface())
+    dt = sc["params"]["dt"]
+    _restore_gpu(g, path, dt)
+    o.restore_state(path)
+    So, Sg = o.collision_sets(), g.collision_sets()
+    co, cg = _canon(So), _canon(Sg)
+    assert len(co[0]) > 0 and len(co[2]) > 0, "the saved state must be in contact"
+    for a, b in zip(co, cg):
+        assert a == b
+    assert np.array_equal(So["self_active"], Sg["self_active"])
+    assert np.array_equal(So["ccd"], Sg["ccd"])
+    o.friction_init(); g.friction_init()
+    go, rp, col, val, rhs = o.system()
+    gg, _ = g.assemble()
+    assert np.abs(go - gg).max() <= GRAD_TOL * np.abs(go).max()
+    Ao = _oracle_full_matrix(rp, col, val, 3 * o.nv)
+    Ag = _gpu_full_matrix(g, sc["btype"])
+    assert abs(Ao - Ag).max() <= HESS_TOL * abs(Ao).max()
+    k = o.scalars()["kappa"]
+    eo, eg = o.energy(k), g.energy(k)
+    assert abs(eo - eg) <= ENERGY_TOL * abs(eo)
+    rng = np.random.default_rng(4)
+    d = rng.standard_normal((o.nv, 3)) * 0.01 * (sc["btype"] == 0)[:, None]
+    d[:, 1] = np.abs(d[:, 1])
+    bo, bg = o.step_bounds(d, 1.0), g.step_bounds(d, 1.0)
+    for key in ("ground", "partial", "cfl", "full"):
+        assert abs(bo[key] - bg[key]) <= 1e-6 * abs(bo[key]), key
+        assert bg[key] <= bo[key] * (1 + 1e-12) + 1e-300, key
+    g.close()
+
+
+def test_contact_state_three_steps(oracle_mod, contact_state):
+    """Three steps from the saved contact state: FP64 block-Jacobi, and FP32
+    blocks with the learned factor (trained on the restored state's Newton
+    system for 30 Adam iterations, then frozen)."""
+    name, sc, path, o = contact_state
+    o.restore_state(path)
+    dt = sc["params"]["dt"]
+    g64 = cipc.Simulator(sc, surface=o.surface())
+    _restore_gpu(g64, path, dt)
+    gm = cipc.Simulator(sc, surface=o.surface(), precision="mixed", precond="learned")
+    _restore_gpu(gm, path, dt)
+    gm.friction_init()
+    gm.assemble()
+    gm.precond_train(30, probes=4, lr=2e-3, seed=7)
+    _restore_gpu(gm, path, dt)
+    bb = np.sqrt(o.scalars()["bboxDiag2"])
+    for s in range(3):
+        so = o.step()
+        s64, sm = g64.step(), gm.step()
+        xo = o.get("x")
+        e64 = np.abs(xo - g64.get("x")).max() / bb
+        em = np.abs(xo - gm.get("x")).max() / bb
+        assert e64 <= TRAJ_TOL, (name, s, e64)
+        assert em <= TRAJ_TOL, (name, s, em)
+        assert so["selfContacts"] > 0
+    g64.close(); gm.close()
+
+
+def test_twist_8x32x64_ten_steps(oracle_mod):
+    sc = cipc.scene_twist(8, 32, 64)
+    assert len(sc["tets"]) == 92160
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=THREADS)
+    g = cipc.Simulator(sc, surface=o.surface())
+    bb = np.sqrt(o.scalars()["bboxDiag2"])
+    for s in range(10):
+        so, sg = o.step(), g.step()
+        assert so["newton"] == sg["newtonIterations"], s
+        err = np.abs(o.get("x") - g.get("x")).max() / bb
+        assert err <= TRAJ_TOL, (s, err)
+    g.close()
+
+
+def _pairs_from_ccd_set(o, S):
+    """Vertex quadruples of the partial-CCD candidates: (-s-1, face) is a
+    surface vertex against a face, (e, f) an edge against an edge."""
+    faces, verts, edges = o.surface()
+    kinds, quads = [], []
+    for a, b in S["ccd"]:
+        if a < 0:
+            kinds.append(0); quads.append([verts[-a - 1], *faces[b]])
+        else:
+            kinds.append(1); quads.append([*edges[a], *edges[b]])
+    return np.array(kinds, np.int32), np.array(quads, np.int64)
+
+
+def _check_toi(oracle_mod, kinds, P, D, eta=0.2):
+    tg = cipc.accd(kinds, P, D, eta)
+    to = np.array([(oracle_mod.pt_ccd if k == 0 else oracle_mod.ee_ccd)(P[i].reshape(-1), D[i].reshape(-1), eta)
+                   for i, k in enumerate(kinds)])
+    assert np.all(np.abs(tg - to) <= 1e-6 * np.abs(to)), np.abs(tg - to).max()
+    assert np.all(tg <= to * (1 + 1e-12))
+    return tg, to
+
+
+def test_ccd_time_of_impact_per_candidate(oracle_mod):
+    sc = cipc.scene_cloth_drape(128, 10)
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=THREADS)
+    o.restore_state(os.path.join(STATES, "cloth_drape_128_frame40.npz"))
+    S = o.collision_sets()
+    kinds, quads = _pairs_from_ccd_set(o, S)
+    assert len(kinds) > 100 and 0 < kinds.sum() < len(kinds)
+    x = o.get("x")
+    rng = np.random.default_rng(9)
+    disp = rng.standard_normal((o.nv, 3)) * 2e-3 * (sc["btype"] == 0)[:, None]
+    disp[:, 1] -= 3e-3 * (sc["btype"] == 0)  # downwards, into the cube
+    tg, to = _check_toi(oracle_mod, kinds, x[quads], disp[quads])
+    assert (to < 1).sum() > 0, "some candidates must collide within the step"
+    # random near-contact pairs over four decades of scale
+    n = 4000
+    kinds = rng.integers(0, 2, n).astype(np.int32)
+    scale = 10.0 ** rng.uniform(-3, 1, n)[:, None, None]
+    P = rng.standard_normal((n, 4, 3)) * scale
+    D = rng.standard_normal((n, 4, 3)) * scale * 2
+    _check_toi(oracle_mod, kinds, P, D)
