@@ -101,7 +101,6 @@ struct Ctx {
 
     // host mirrors needed by the driver
     std::vector<int> hBtype, hSoftIdx, hDirIdx;
-    std::vector<double> hRest;
     int dirMotion = 0, softMotion = 0;
     double dirRate = 0, softRate = 0;
 

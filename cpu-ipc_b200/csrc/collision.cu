@@ -18,11 +18,14 @@
 #include "cipc_internal.h"
 #include "geometry.cuh"
 
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
 
 namespace cipc {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -236,48 +239,78 @@ __global__ void refitKernel(int n, const int* left, const int* right, const int*
     }
 }
 
+// Escape (rope) index of every node: the next node of a depth-first walk
+// once the node's subtree is done - the right sibling of the node or of its
+// nearest ancestor that is a left child; -1 past the last leaf.  One thread
+// per node walks up the parent links (at most the tree's depth, which the
+// 64-bit keys bound by 64).
+__global__ void escapeKernel(int n, const int* left, const int* right, const int* parent, int* escape) {
+    CIPC_KERNEL_LOOP(node, 2 * n - 1) {
+        int cur = node, e = -1;
+        for (int guard = 0; guard < 128; ++guard) {
+            const int p = parent[cur];
+            if (p < 0) break;
+            if (left[p] == cur) { e = right[p]; break; }
+            cur = p;
+        }
+        escape[node] = e;
+    }
+}
+
 struct BvhView {
     int n;
-    const int *left, *right, *leafPrim;
+    const int *left, *right, *leafPrim, *escape;
     const double *lo, *hi;
     const float4* rec;
 };
-BvhView view(const DevBvh& t) { return BvhView{t.n, t.left, t.right, t.leafPrim, t.lo, t.hi, reinterpret_cast<const float4*>(t.rec.p)}; }
+BvhView view(const DevBvh& t) {
+    return BvhView{t.n, t.left, t.right, t.leafPrim, t.escape, t.lo, t.hi, reinterpret_cast<const float4*>(t.rec.p)};
+}
 
-// Depth-first traversal; calls f(prim) for every leaf whose box overlaps the
-// query box with the gap (inclusive test, in FP64).  Internal nodes are
-// culled on their children's outward-rounded FP32 boxes, which contain the
-// FP64 boxes, so no leaf the FP64 test accepts is lost; each leaf is then
-// tested on its FP64 box.  The set of leaves reported is exactly that of a
-// walk on the FP64 boxes (the order of the calls differs, and every caller
-// sorts or reduces what it collects).
+// Stack-less depth-first traversal along escape indices; calls f(prim) once
+// for every leaf whose box overlaps the query box with the gap (inclusive
+// test, in FP64).  At an internal node one 64-byte record tests both
+// children on their outward-rounded FP32 boxes, which contain the FP64
+// boxes: a hit internal left child is entered directly (its sibling is
+// reached later by the escape index and tested on its own FP64 box); a hit
+// leaf is tested on its FP64 box and reported unless the walk entered its
+// left sibling, in which case the escape index brings the walk to it.  The
+// set of leaves reported is exactly that of a walk on the FP64 boxes (the
+// order of the calls differs, and every caller sorts or reduces what it
+// collects).  The walk visits each node at most once; a count past the node
+// count raises a status bit.
 template <class F>
 __device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, const double* qhi, double gap, int* status, F f) {
     if (t.n <= 0) return;
     if (!overlaps(qlo, qhi, t.lo, t.hi, gap)) return;  // the root (node 0)
     if (t.n == 1) { f(t.leafPrim[0]); return; }
-    int stack[64];
-    int sp = 0;
-    stack[sp++] = 0;
-    while (sp > 0) {
-        const int node = stack[--sp];
-        const float4* r = t.rec + 4 * (size_t)node;
+    const int firstLeaf = t.n - 1;
+    int cur = 0;  // an internal node whose box overlaps the query
+    for (int visits = 0; cur >= 0; ++visits) {
+        if (visits > 2 * t.n) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
+        const float4* r = t.rec + 4 * (size_t)cur;
         const float4 a = r[0], b = r[1], cc = r[2], d = r[3];
         const double lo0[3] = {a.x, a.y, a.z}, hi0[3] = {a.w, b.x, b.y};
         const double lo1[3] = {b.z, b.w, cc.x}, hi1[3] = {cc.y, cc.z, cc.w};
-        const int ch[2] = {__float_as_int(d.x), __float_as_int(d.y)};
-        const bool hit[2] = {overlaps(qlo, qhi, lo0, hi0, gap), overlaps(qlo, qhi, lo1, hi1, gap)};
-        // the right child goes on the stack first: the left subtree is walked first
-        for (int s = 1; s >= 0; --s) {
-            if (!hit[s]) continue;
-            const int cn = ch[s];
-            if (cn >= t.n - 1) {
-                if (overlaps(qlo, qhi, t.lo + 3 * cn, t.hi + 3 * cn, gap)) f(t.leafPrim[cn - (t.n - 1)]);
-            } else {
-                if (sp >= 64) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
-                stack[sp++] = cn;
+        const int c0 = __float_as_int(d.x), c1 = __float_as_int(d.y);
+        const bool h0 = overlaps(qlo, qhi, lo0, hi0, gap), h1 = overlaps(qlo, qhi, lo1, hi1, gap);
+        if (h0 && c0 < firstLeaf) { cur = c0; continue; }
+        if (h0 && overlaps(qlo, qhi, t.lo + 3 * c0, t.hi + 3 * c0, gap)) f(t.leafPrim[c0 - firstLeaf]);
+        if (h1 && c1 < firstLeaf) { cur = c1; continue; }
+        if (h1 && overlaps(qlo, qhi, t.lo + 3 * c1, t.hi + 3 * c1, gap)) f(t.leafPrim[c1 - firstLeaf]);
+        // both children done: follow escape indices to the next node to test
+        int e = t.escape[cur];
+        while (e >= 0) {
+            if (++visits > 2 * t.n) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
+            const bool hit = overlaps(qlo, qhi, t.lo + 3 * e, t.hi + 3 * e, gap);
+            if (e >= firstLeaf) {
+                if (hit) f(t.leafPrim[e - firstLeaf]);
+            } else if (hit) {
+                break;
             }
+            e = t.escape[e];
         }
+        cur = e;
     }
 }
 
@@ -290,12 +323,19 @@ __device__ __forceinline__ uint64_t ppeKey(int c0, int c1, int c2) {
     return ((M21 - v) << 42) | ((uint64_t)c1 << 21) | (uint64_t)(c2 + 1);
 }
 
+// Appends a key to a list: the lanes of a warp that emit at the same point
+// take one atomic for all of them (the leader reserves the group's slots and
+// broadcasts the base).  The list is sorted afterwards, so the order of the
+// slots does not matter.
 struct Emit {
     uint64_t* buf;
     int cap;
     int* counter;
     __device__ void operator()(uint64_t k, int* status) const {
-        int i = atomicAdd(counter, 1);
+        cg::coalesced_group g = cg::coalesced_threads();
+        int base = 0;
+        if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+        const int i = g.shfl(base, 0) + (int)g.thread_rank();
         if (i < cap) buf[i] = k;
         else raiseStatus(status, CIPC_ST_CAPACITY);
     }
@@ -574,7 +614,7 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     if (n <= 0) return;
     int nn = 2 * n - 1;
     t.keys.reserve(n); t.keysAlt.reserve(n);
-    t.left.reserve(nn); t.right.reserve(nn); t.parent.reserve(nn); t.leafPrim.reserve(n); t.flags.reserve(n);
+    t.left.reserve(nn); t.right.reserve(nn); t.parent.reserve(nn); t.escape.reserve(nn); t.leafPrim.reserve(n); t.flags.reserve(n);
     t.lo.reserve(3 * nn); t.hi.reserve(3 * nn); t.sceneBox.reserve(6);
     const int nbBox = std::max(1, std::min(148, (n + 255) / 256));
     t.boxPart.reserve(6 * (size_t)nbBox);
@@ -588,6 +628,7 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     launch(leafKernel, blocksFor(n), TB, 0, c.s, n, t.keys, t.primLo, t.primHi, t.leafPrim, t.lo, t.hi, t.flags, t.parent);
     t.rec.reserve(16 * (size_t)std::max(1, n - 1));
     if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, t.left, t.right, t.parent, t.lo, t.hi, t.flags, t.rec.p);
+    if (n > 1) launch(escapeKernel, blocksFor(nn), TB, 0, c.s, n, t.left, t.right, t.parent, t.escape);
     CIPC_CUDA(cudaGetLastError());
 }
 

@@ -60,6 +60,27 @@ __global__ void inertialTargetKernel(int nv, const double* vp, const double* vel
     }
 }
 
+// Animated boundary motion (twistingBoundaryDirection, Simulator.cpp:24-46):
+// the displacement that rotates x about the x axis by the step's angle,
+// clockwise or counter-clockwise by the side of the rest position (cs, sn:
+// cosine and sine of the angle, evaluated once on the host).  With
+// `target` the kernel writes x - displacement (the soft targets), else the
+// displacement itself into out (3 per vertex of the list).
+__global__ void motionKernel(int n, const int* idx, const double* x, const double* rest, double cs, double sn, int target, double* out) {
+    CIPC_KERNEL_LOOP(k, n) {
+        const int v = idx[k];
+        const double y = x[3 * v + 1], z = x[3 * v + 2], r0 = rest[3 * v];
+        double d1 = 0.0, d2 = 0.0;
+        if (r0 < 0.0) { d1 = cs * y + sn * z - y; d2 = -sn * y + cs * z - z; }
+        else if (r0 > 0.0) { d1 = cs * y - sn * z - y; d2 = sn * y + cs * z - z; }
+        if (target) {
+            out[3 * k] = x[3 * v]; out[3 * k + 1] = y - d1; out[3 * k + 2] = z - d2;
+        } else {
+            out[3 * v] = 0.0; out[3 * v + 1] = d1; out[3 * v + 2] = d2;
+        }
+    }
+}
+
 using Clock = std::chrono::steady_clock;
 double ms(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); }
 
@@ -290,15 +311,6 @@ int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
     return k;
 }
 
-// twistingBoundaryDirection (Simulator.cpp:24-46) with a rate parameter.
-void motionDir(int motion, double rate, const double* x, const double* rest, double frac, double dt, double* out) {
-    out[0] = out[1] = out[2] = 0.0;
-    if (motion != CIPC_MOTION_TWIST_X) return;
-    double ang = rate * dt * frac, cs = std::cos(ang), sn = std::sin(ang);
-    if (rest[0] < 0.0) { out[0] = 0; out[1] = cs * x[1] + sn * x[2] - x[1]; out[2] = -sn * x[1] + cs * x[2] - x[2]; }
-    else if (rest[0] > 0.0) { out[0] = 0; out[1] = cs * x[1] - sn * x[2] - x[1]; out[2] = sn * x[1] + cs * x[2] - x[2]; }
-}
-
 void solveIPCStep(Ctx& c, cipc_step_stats& st) {
     std::memset(&st, 0, sizeof(st));
     st.frame = c.stepIndex;
@@ -311,42 +323,36 @@ void solveIPCStep(Ctx& c, cipc_step_stats& st) {
     initKappa(c, P.kappa);
     frictionInitialize(c);
     int nv = c.nv;
-    bool needHost = (!c.hSoftIdx.empty() && c.softMotion != CIPC_MOTION_NONE) || (!c.hDirIdx.empty() && c.dirMotion != CIPC_MOTION_NONE);
-    std::vector<double> hx;
-    if (needHost) {
-        hx.resize(3 * (size_t)nv);
-        CIPC_CUDA(cudaMemcpy(hx.data(), c.x.p, sizeof(double) * 3 * nv, cudaMemcpyDeviceToHost));
+    // animated boundaries, on the device from the positions at the start of
+    // the step (IPCSolver.cpp:1120-1155)
+    const int ns = (int)c.hSoftIdx.size(), nd = (int)c.hDirIdx.size();
+    if (ns && c.softMotion == CIPC_MOTION_TWIST_X) {
+        const double ang = c.softRate * P.dt;
+        launch(motionKernel, blocksFor(ns), TB, 0, c.s, ns, (const int*)c.softIdx, (const double*)c.x, (const double*)c.rest, std::cos(ang),
+               std::sin(ang), 1, (double*)c.softTarget);
     }
-    if (!c.hSoftIdx.empty() && c.softMotion != CIPC_MOTION_NONE) {
-        std::vector<double> tg(3 * c.hSoftIdx.size());
-        for (size_t k = 0; k < c.hSoftIdx.size(); ++k) {
-            int v = c.hSoftIdx[k];
-            double d[3];
-            motionDir(c.softMotion, c.softRate, &hx[3 * v], &c.hRest[3 * v], 1.0, P.dt, d);
-            for (int q = 0; q < 3; ++q) tg[3 * k + q] = hx[3 * v + q] - d[q];
-        }
-        CIPC_CUDA(cudaMemcpy(c.softTarget.p, tg.data(), tg.size() * sizeof(double), cudaMemcpyHostToDevice));
-    }
-    if (!c.hDirIdx.empty() && c.dirMotion != CIPC_MOTION_NONE) {
-        std::vector<double> d(3 * (size_t)nv, 0.0);
-        auto dirs = [&](double frac, const std::vector<double>& xs) {
-            std::fill(d.begin(), d.end(), 0.0);
-            for (int v : c.hDirIdx) motionDir(c.dirMotion, c.dirRate, &xs[3 * v], &c.hRest[3 * v], frac, P.dt, &d[3 * v]);
-            CIPC_CUDA(cudaMemcpy(c.Ap.p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
-        };
+    if (nd && c.dirMotion == CIPC_MOTION_TWIST_X) {
         c.Ap.reserve(3 * (size_t)nv);
-        double na = 1;
-        dirs(na, hx);
-        na = fullCCDDir(c, c.Ap, na);
-        dirs(na, hx);
         CIPC_CUDA(cudaMemcpyAsync(c.x0.p, c.x.p, sizeof(double) * 3 * nv, cudaMemcpyDeviceToDevice, c.s));
+        // the Dirichlet vertices' displacement for the fraction `frac` of the
+        // step's rotation (zero elsewhere), from the start-of-step positions x0
+        auto dirs = [&](double frac) {
+            CIPC_CUDA(cudaMemsetAsync(c.Ap.p, 0, sizeof(double) * 3 * nv, c.s));
+            const double ang = c.dirRate * P.dt * frac;
+            launch(motionKernel, blocksFor(nd), TB, 0, c.s, nd, (const int*)c.dirIdx, (const double*)c.x0, (const double*)c.rest, std::cos(ang),
+                   std::sin(ang), 0, (double*)c.Ap);
+        };
+        double na = 1;
+        dirs(na);
+        na = fullCCDDir(c, c.Ap, na);
+        dirs(na);
         stepForward(c, c.x0, c.Ap, 1.0, true);
         rebuildTrees(c);
         int ni = 0;
         while (isIntersected(c)) {
             if (ni++ >= 64 || na <= std::numeric_limits<double>::epsilon()) throw std::runtime_error("animated boundary update remains intersecting");
             na /= 2.0;
-            dirs(na, hx);
+            dirs(na);
             stepForward(c, c.x0, c.Ap, 1.0, true);
             rebuildTrees(c);
         }
@@ -452,7 +458,6 @@ Ctx* createContext(const cipc_scene_desc* s, const cipc_linear_options* o) {
         P.softW = s->softW;
         P.useBarrier = s->use_barrier; P.applyGravity = s->apply_gravity; P.quasiStatic = s->quasi_static;
         c->hBtype.assign(s->btype, s->btype + s->nv);
-        c->hRest = in.x;
         if (s->nsoft > 0) c->hSoftIdx.assign(s->softIdx, s->softIdx + s->nsoft);
         if (s->ndir > 0) c->hDirIdx.assign(s->dirIdx, s->dirIdx + s->ndir);
         c->softMotion = s->softMotion; c->softRate = s->softRate; c->dirMotion = s->dirMotion; c->dirRate = s->dirRate;
