@@ -98,6 +98,7 @@ struct Ctx {
     // a tensor-core completion wait timed out: the network's forward pass is
     // refused for the rest of the context's life
     bool tcFault = false;
+    DBuf<double> stepScal;  // device scalars of the chained step bounds
 
     // host mirrors needed by the driver
     std::vector<int> hBtype, hSoftIdx, hDirIdx;
@@ -232,11 +233,16 @@ void initKappaGradE(Ctx& c, double* gE);  // inertia + tet elastic gradient into
 
 // ---- launchers (collision.cu) ----
 void buildBvh(Ctx& c, DevBvh& t, int n);
-void computeFaceBoxes(Ctx& c, const double* x, const double* d, double step, bool swept);
-void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, bool swept);
+void computeFaceBoxes(Ctx& c, const double* x, const double* d, double step, bool swept, const double* stepPtr = nullptr);
+void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, bool swept, const double* stepPtr = nullptr);
 void buildCollisionSets(Ctx& c, bool rehash);
 void groundActiveSet(Ctx& c);
 bool isIntersected(Ctx& c);
+// Step bounds chained on the device (ground, partial CCD, CFL, full CCD and
+// the merge rule of IPCSolver.cpp:943-990) with one read-back.
+double stepBoundsDevice(Ctx& c);
+void deviceMinTo(Ctx& c, const double* v, int n, double* dst);
+void deviceMaxTo(Ctx& c, const double* v, int n, double* dst);
 void accdBatch(int n, const int* kind, const double* p, const double* d, double eta, double* toi);  // host arrays
 double groundStepBound(Ctx& c);
 double partialCCD(Ctx& c, double alpha);

@@ -51,7 +51,9 @@ __device__ __forceinline__ void sweptAdd(double lo[3], double hi[3], d3 p, d3 d,
     boxAdd(lo, hi, p - step * d);
 }
 
-__global__ void faceBoxKernel(int n, const int* faces, const double* x, const double* d, double step, int swept, double* lo, double* hi) {
+__global__ void faceBoxKernel(int n, const int* faces, const double* x, const double* d, double stepVal, const double* stepPtr, int swept,
+                              double* lo, double* hi) {
+    const double step = stepPtr ? *stepPtr : stepVal;
     CIPC_KERNEL_LOOP(f, n) {
         double l[3], h[3];
         boxInit(l, h);
@@ -63,7 +65,9 @@ __global__ void faceBoxKernel(int n, const int* faces, const double* x, const do
         for (int k = 0; k < 3; ++k) { lo[3 * f + k] = l[k]; hi[3 * f + k] = h[k]; }
     }
 }
-__global__ void edgeBoxKernel(int n, const int* edges, const double* x, const double* d, double step, int swept, double* lo, double* hi) {
+__global__ void edgeBoxKernel(int n, const int* edges, const double* x, const double* d, double stepVal, const double* stepPtr, int swept,
+                              double* lo, double* hi) {
+    const double step = stepPtr ? *stepPtr : stepVal;
     CIPC_KERNEL_LOOP(e, n) {
         double l[3], h[3];
         boxInit(l, h);
@@ -500,8 +504,9 @@ __global__ void partialCCDKernel(int nPT, int nEE, const uint64_t* ccdPT, const 
     }
 }
 
-__global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, const double* dir, double step,
-                             BvhView tree, double eta, double* out, int* status) {
+__global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, const double* dir, double stepVal,
+                             const double* stepPtr, BvhView tree, double eta, double* out, int* status) {
+    const double step = stepPtr ? *stepPtr : stepVal;
     CIPC_KERNEL_LOOP(svI, nsv) {
         int vI = surfVerts[svI];
         d3 p = ld3(x, vI), dp = ld3(dir, vI);
@@ -521,7 +526,8 @@ __global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, co
 }
 
 __global__ void fullEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* dir, const double* treeBoxLo,
-                             const double* treeBoxHi, double eeStep, BvhView tree, double eta, double* out, int* status) {
+                             const double* treeBoxHi, double eeStepVal, const double* eeStepPtr, BvhView tree, double eta, double* out, int* status) {
+    const double eeStep = eeStepPtr ? *eeStepPtr : eeStepVal;
     CIPC_KERNEL_LOOP(eJ, ne) {
         int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
         d3 q0 = ld3(x, g0), q1 = ld3(x, g1), dq0 = ld3(dir, g0), dq1 = ld3(dir, g1);
@@ -598,15 +604,17 @@ int bitsFor(int m) {
 
 }  // namespace
 
-void computeFaceBoxes(Ctx& c, const double* x, const double* d, double step, bool swept) {
+// Primitive boxes of the face / edge tree at x, or swept from x to
+// x - step * d (step read from *stepPtr on the device when it is given).
+void computeFaceBoxes(Ctx& c, const double* x, const double* d, double step, bool swept, const double* stepPtr) {
     c.faceTree.primLo.reserve(3 * std::max(1, c.nsf));
     c.faceTree.primHi.reserve(3 * std::max(1, c.nsf));
-    if (c.nsf) launch(faceBoxKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, x, d, step, swept, c.faceTree.primLo, c.faceTree.primHi);
+    if (c.nsf) launch(faceBoxKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, x, d, step, stepPtr, swept, c.faceTree.primLo, c.faceTree.primHi);
 }
-void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, bool swept) {
+void computeEdgeBoxes(Ctx& c, const double* x, const double* d, double step, bool swept, const double* stepPtr) {
     c.edgeTree.primLo.reserve(3 * std::max(1, c.nse));
     c.edgeTree.primHi.reserve(3 * std::max(1, c.nse));
-    if (c.nse) launch(edgeBoxKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, x, d, step, swept, c.edgeTree.primLo, c.edgeTree.primHi);
+    if (c.nse) launch(edgeBoxKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, x, d, step, stepPtr, swept, c.edgeTree.primLo, c.edgeTree.primHi);
 }
 
 void buildBvh(Ctx& c, DevBvh& t, int n) {
@@ -787,15 +795,15 @@ double fullCCDDir(Ctx& c, const double* d, double alpha) {
     c.energyBuf.reserve(std::max(std::max(c.nsv, c.nse), 1));
     if (c.nsv) {
         profBegin(c, PROF_FULLCCD);
-        launch(fullPTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, step, view(c.faceTree), 1.0 - 0.8, c.energyBuf,
-                                                       c.status);
+        launch(fullPTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, step, (const double*)nullptr, view(c.faceTree),
+               1.0 - 0.8, c.energyBuf, c.status);
         profEnd(c, PROF_FULLCCD);
         step = std::min(step, deviceMin(c, c.energyBuf, c.nsv, 1e308));
     }
     if (c.nse) {
         profBegin(c, PROF_FULLCCD);
-        launch(fullEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi, step, view(c.edgeTree),
-                                                       1.0 - 0.8, c.energyBuf, c.status);
+        launch(fullEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi, step,
+               (const double*)nullptr, view(c.edgeTree), 1.0 - 0.8, c.energyBuf, c.status);
         profEnd(c, PROF_FULLCCD);
         step = std::min(step, deviceMin(c, c.energyBuf, c.nse, 1e308));
     }
@@ -804,6 +812,96 @@ double fullCCDDir(Ctx& c, const double* d, double alpha) {
 }
 
 double fullCCD(Ctx& c, double alpha) { return fullCCDDir(c, c.dir, alpha); }
+
+namespace {
+// Scalars of the chained step bounds (stepBoundsDevice), one thread each.
+// s: 0 ground min, 1 partial-CCD min, 2 max surface move, 3 entry step,
+// 4 full point-triangle min, 5 edge-edge entry step, 6 full edge-edge min,
+// 7 merged step, 8 status word.
+__global__ void stepEntryKernel(double* s, int nsv) {
+    double a = nsv ? s[0] : 1.0;
+    a = fmin(1.0, a);
+    if (a <= 0) a = 1;
+    s[3] = a;
+    s[5] = a;
+}
+__global__ void stepEeEntryKernel(double* s) { s[5] = fmin(s[3], s[4]); }
+__global__ void stepMergeKernel(double* s, int nsv, int nse, int nPartial, int barrier, double sqrtHhat, const int* status) {
+    const double alpha = s[3];
+    double a = alpha;
+    if (barrier) {
+        const double partial = nPartial ? fmin(alpha, s[1]) : alpha;
+        const double mx = nsv ? fmax(0.0, s[2]) : 0.0;
+        const double aCFL = mx > 0.0 ? sqrtHhat / (mx * 2.0) : 1.0;
+        double full = alpha;
+        if (nsv) full = fmin(full, s[4]);
+        if (nse) full = fmin(full, s[6]);
+        a = fmin(a, aCFL);
+        if (partial > 2.0 * aCFL) {
+            a = fmin(partial, full);
+            a = fmax(a, aCFL);
+        }
+        s[1] = partial; s[2] = aCFL; s[6] = full;
+    }
+    s[7] = a;
+    s[8] = (double)*status;
+}
+}  // namespace
+
+// The step bound of one Newton iteration (IPCSolver.cpp:943-990) without
+// host round trips between its stages: the ground bound gives the entry step,
+// the partial CCD, CFL bound and the swept full CCD (entry step read on the
+// device, the edge-edge pass starting from the point-triangle result) write
+// device scalars, and one kernel applies the merge rule.  One read-back.
+double stepBoundsDevice(Ctx& c) {
+    c.stepScal.reserve(16);
+    double* s = c.stepScal.p;
+    const int nPartial = c.nCcdPT + c.nCcdEE;
+    c.energyBuf.reserve(std::max(std::max(std::max(c.nsv, c.nse), nPartial), 1));
+    if (c.nsv) {
+        launch(groundBoundKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.x, c.dir, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2],
+               c.P.groundD, 0.8, c.energyBuf);
+        deviceMinTo(c, c.energyBuf, c.nsv, s + 0);
+    }
+    launch(stepEntryKernel, 1, 1, 0, c.s, s, c.nsv);
+    if (c.P.useBarrier) {
+        if (nPartial) {
+            launch(partialCCDKernel, blocksFor(nPartial), TB, 0, c.s, c.nCcdPT, c.nCcdEE, c.ccdPT, c.ccdEE, c.surfVerts, c.faces, c.edges, c.x, c.dir,
+                   1.0 - 0.8, c.energyBuf, c.status);
+            deviceMinTo(c, c.energyBuf, nPartial, s + 1);
+        }
+        if (c.nsv) {
+            launch(surfMoveKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.dir, c.energyBuf);
+            deviceMaxTo(c, c.energyBuf, c.nsv, s + 2);
+        }
+        computeFaceBoxes(c, c.x, c.dir, 0.0, true, s + 3);
+        buildBvh(c, c.faceTree, c.nsf);
+        computeEdgeBoxes(c, c.x, c.dir, 0.0, true, s + 3);
+        buildBvh(c, c.edgeTree, c.nse);
+        if (c.nsv) {
+            profBegin(c, PROF_FULLCCD);
+            launch(fullPTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, c.dir, 0.0, (const double*)(s + 3),
+                   view(c.faceTree), 1.0 - 0.8, c.energyBuf, c.status);
+            profEnd(c, PROF_FULLCCD);
+            deviceMinTo(c, c.energyBuf, c.nsv, s + 4);
+            launch(stepEeEntryKernel, 1, 1, 0, c.s, s);
+        }
+        if (c.nse) {
+            profBegin(c, PROF_FULLCCD);
+            launch(fullEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.dir, c.edgeTree.primLo, c.edgeTree.primHi, 0.0,
+                   (const double*)(s + 5), view(c.edgeTree), 1.0 - 0.8, c.energyBuf, c.status);
+            profEnd(c, PROF_FULLCCD);
+            deviceMinTo(c, c.energyBuf, c.nse, s + 6);
+        }
+    }
+    launch(stepMergeKernel, 1, 1, 0, c.s, s, c.nsv, c.nse, nPartial, c.P.useBarrier ? 1 : 0, std::sqrt(c.P.Hhat), (const int*)c.status.p);
+    CIPC_CUDA(cudaGetLastError());
+    double h[9];
+    CIPC_CUDA(cudaMemcpyAsync(h, s, sizeof(h), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    if (h[8] != 0.0) checkStatus(c, "step bounds");
+    return h[7];
+}
 
 
 // Additive CCD on a batch of independent candidate pairs (the per-pair time

@@ -271,20 +271,8 @@ int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
             st.linearSolveMilliseconds += ms(t1, t2);
             break;
         }
-        double alpha = groundStepBound(c);
-        alpha = std::min(1.0, alpha);
-        if (alpha <= 0) alpha = 1;
-        if (c.P.useBarrier) {
-            double partial = partialCCD(c, alpha);
-            double aCFL = cflBound(c);
-            double full = fullCCD(c, alpha);
-            alpha = std::min(alpha, aCFL);
-            if (partial > 2.0 * aCFL) {
-                alpha = std::min(partial, full);
-                alpha = std::max(alpha, aCFL);
-            }
-        }
-        sync(c);
+        // ground bound, partial CCD, CFL bound, full CCD and their merge
+        double alpha = stepBoundsDevice(c);
         auto t3 = Clock::now();
         bool accepted = lineSearch(c, alpha, kappa, st, ec);
         sync(c);

@@ -89,6 +89,23 @@ void deviceSumTo(Ctx& c, const double* v, int n, int slot) {
     launch(partialKernel<0>, nb, RB, 0, c.s, v, (const double*)nullptr, n, chunk, c.scratch.p + 8);
     launch(finalKernel<0>, 1, RB, 0, c.s, (const double*)(c.scratch.p + 8), nb, c.sums.p + slot);
 }
+// Minimum / maximum of v[0..n) into the device scalar *dst without a host
+// synchronisation (the identity, +-1e308, for n <= 0).
+void deviceMinTo(Ctx& c, const double* v, int n, double* dst) {
+    int nb = n > 0 ? std::min(1024, (n + 4 * RB - 1) / (4 * RB)) : 0;
+    int chunk = n > 0 ? (n + nb - 1) / nb : 0;
+    c.scratch.reserve(nb + 8);
+    if (nb) launch(partialKernel<2>, nb, RB, 0, c.s, v, (const double*)nullptr, n, chunk, c.scratch.p + 8);
+    launch(finalKernel<2>, 1, RB, 0, c.s, (const double*)(c.scratch.p + 8), nb, dst);
+}
+void deviceMaxTo(Ctx& c, const double* v, int n, double* dst) {
+    int nb = n > 0 ? std::min(1024, (n + 4 * RB - 1) / (4 * RB)) : 0;
+    int chunk = n > 0 ? (n + nb - 1) / nb : 0;
+    c.scratch.reserve(nb + 8);
+    if (nb) launch(partialKernel<1>, nb, RB, 0, c.s, v, (const double*)nullptr, n, chunk, c.scratch.p + 8);
+    launch(finalKernel<1>, 1, RB, 0, c.s, (const double*)(c.scratch.p + 8), nb, dst);
+}
+
 void fetchSums(Ctx& c, double* h, int nslots) {
     CIPC_CUDA(cudaMemcpyAsync(h, c.sums.p, sizeof(double) * nslots, cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaStreamSynchronize(c.s));
