@@ -159,6 +159,7 @@ struct Ctx {
     DBuf<int> dynRowStart, dynRowEnd, dynCol, dynSrcStart;
     DBuf<double> dynBD;
     DBuf<float> dynBF;
+    DBuf<unsigned char> groundTmp;  // temporary storage of the ground-set selection (runs beside the PP/PE encoding)
     DBuf<unsigned char> sortTmp;
 
     // PCG
@@ -228,6 +229,8 @@ void buildStaticPattern(Ctx& c, const std::vector<int>& tets, const std::vector<
 void assembleElastic(Ctx& c);          // vtxGrad, diagExtra, element blocks, static BSR values, element gradient
 void tetGradient(Ctx& c);              // elemG of the tetrahedra only (no Hessian)
 double elasticEnergy(Ctx& c);          // (SNH + BW + bending) * dt^2 + inertia + soft, FP64
+void elasticEnergySums(Ctx& c, int slot0);
+double elasticEnergyCombine(const Ctx& c, const double* h);
 void gatherGradient(Ctx& c);           // grad = vtxGrad + element + dynamic contributions
 void initKappaGradE(Ctx& c, double* gE);  // inertia + tet elastic gradient into device buffer gE
 
@@ -253,6 +256,8 @@ void dirichletBound(Ctx& c, double& alpha);
 // ---- launchers (contact.cu) ----
 int contactAssemble(Ctx& c);           // barrier + mollified + friction gradient/Hessian -> dynamic lists; returns collisions
 double contactEnergy(Ctx& c, double kappa);
+void contactEnergySums(Ctx& c, int slot0);
+double contactEnergyCombine(const Ctx& c, double kappa, const double* h);
 void frictionInitialize(Ctx& c);
 void contactGradientKappa(Ctx& c, double* gc);  // ground + self barrier gradient with coefficient 1
 void closeConstraintCheck(Ctx& c, bool& update);

@@ -647,17 +647,27 @@ static void buildStaticTrees(Ctx& c) {
     buildBvh(c, c.edgeTree, c.nse);
 }
 
-void groundActiveSet(Ctx& c) {
+// Ground::calculateActivateSet: the surface vertices within dHat of the
+// ground, in order, into c.ground; their count lands in counters[15] (read
+// back by the caller).
+void groundActiveSetLaunch(Ctx& c) {
     c.ground.reserve(std::max(1, c.nsv));
     c.counts.reserve(std::max(1, c.nsv) + 1);
-    if (c.nsv == 0) { c.nGround = 0; return; }
+    c.counters.reserve(16);
+    if (c.nsv == 0) {
+        CIPC_CUDA(cudaMemsetAsync(c.counters.p + 15, 0, sizeof(int), c.s));
+        return;
+    }
     launch(groundFlagKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.x, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2], c.P.groundD,
                                                        c.P.Hhat, c.counts);
     size_t bytes = 0;
-    c.counters.reserve(16);
     cub::DeviceSelect::Flagged(nullptr, bytes, c.surfVerts.p, c.counts.p, c.ground.p, c.counters.p + 15, c.nsv, c.s);
-    c.sortTmp.reserve(bytes + 16);
-    CIPC_CUDA(cub::DeviceSelect::Flagged(c.sortTmp.p, bytes, c.surfVerts.p, c.counts.p, c.ground.p, c.counters.p + 15, c.nsv, c.s));
+    c.groundTmp.reserve(bytes + 16);
+    CIPC_CUDA(cub::DeviceSelect::Flagged(c.groundTmp.p, bytes, c.surfVerts.p, c.counts.p, c.ground.p, c.counters.p + 15, c.nsv, c.s));
+}
+
+void groundActiveSet(Ctx& c) {
+    groundActiveSetLaunch(c);
     int n = 0;
     CIPC_CUDA(cudaMemcpyAsync(&n, c.counters.p + 15, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaStreamSynchronize(c.s));
@@ -673,6 +683,7 @@ void buildCollisionSets(Ctx& c, bool rehash) {
         int caps[6] = {(int)std::max<size_t>(c.ccdPT.cap, 1024), (int)std::max<size_t>(c.kPT.cap, 1024), (int)std::max<size_t>(c.kPPE.cap, 1024),
                        (int)std::max<size_t>(c.ccdEE.cap, 1024), (int)std::max<size_t>(c.kEE.cap, 1024), (int)std::max<size_t>(c.kMoll.cap, 1024)};
         int cnt[6];
+        int stWord = 0;
         bool fits = false;
         for (int attempt = 0; attempt < 4; ++attempt) {
             c.ccdPT.reserve(caps[0]); c.kPT.reserve(caps[1]); c.kPPE.reserve(caps[2]);
@@ -691,6 +702,7 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             profEnd(c, PROF_ACTIVE);
             CIPC_CUDA(cudaGetLastError());
             CIPC_CUDA(cudaMemcpyAsync(cnt, c.counters.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
+            CIPC_CUDA(cudaMemcpyAsync(&stWord, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
             CIPC_CUDA(cudaStreamSynchronize(c.s));
             fits = true;
             for (int k = 0; k < 6; ++k)
@@ -699,7 +711,7 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             int st = 0;  // clear the capacity bit before retrying (only when another attempt follows)
             CIPC_CUDA(cudaMemcpyAsync(c.status.p, &st, sizeof(int), cudaMemcpyHostToDevice, c.s));
         }
-        checkStatus(c, "active set");
+        if (stWord) checkStatus(c, "active set");
         // the counts size the sorts and decodes below: never past what the
         // last launch could write
         if (!fits) throw std::runtime_error("active-set candidate counts exceed their buffers after four attempts");
@@ -723,8 +735,17 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             cub::DeviceRunLengthEncode::Encode(nullptr, bytes, c.kPPE.p, c.uniq.p, c.runs.p, c.counters.p + 6, cnt[2], c.s);
             c.sortTmp.reserve(bytes + 16);
             CIPC_CUDA(cub::DeviceRunLengthEncode::Encode(c.sortTmp.p, bytes, c.kPPE.p, c.uniq.p, c.runs.p, c.counters.p + 6, cnt[2], c.s));
-            CIPC_CUDA(cudaMemcpyAsync(&nu, c.counters.p + 6, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        } else {
+            CIPC_CUDA(cudaMemsetAsync(c.counters.p + 6, 0, sizeof(int), c.s));
+        }
+        // the ground set is selected meanwhile; both counts come back at once
+        groundActiveSetLaunch(c);
+        {
+            int h[10];
+            CIPC_CUDA(cudaMemcpyAsync(h, c.counters.p + 6, 10 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
             CIPC_CUDA(cudaStreamSynchronize(c.s));
+            nu = h[0];
+            c.nGround = h[9];
         }
         c.nPPE = nu;
         c.nSelf = c.nPT + c.nEE + c.nPPE;
@@ -736,8 +757,9 @@ void buildCollisionSets(Ctx& c, bool rehash) {
         c.eeIe.reserve(2 * std::max(c.nMoll, 1));
         if (c.nMoll) launch(decodeMollKernel, blocksFor(c.nMoll), TB, 0, c.s, c.nMoll, c.kMoll, c.edges, c.selfEE, c.eeIe);
         CIPC_CUDA(cudaGetLastError());
+    } else {
+        groundActiveSet(c);
     }
-    groundActiveSet(c);
 }
 
 bool isIntersected(Ctx& c) {
@@ -748,10 +770,11 @@ bool isIntersected(Ctx& c) {
                                                                    c.P.groundD, c.counters.p + 7);
     if (c.nsf) launch(intersectKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, view(c.edgeTree), c.coplanarTol, c.counters.p + 7,
                             c.status);
-    int f = 0;
+    int f = 0, st = 0;
     CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaStreamSynchronize(c.s));
-    checkStatus(c, "intersection test");
+    if (st) checkStatus(c, "intersection test");
     return f != 0;
 }
 

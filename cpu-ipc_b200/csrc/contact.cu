@@ -685,46 +685,55 @@ void finalizeDynamic(Ctx& c) {
     CIPC_CUDA(cudaGetLastError());
 }
 
-double contactEnergy(Ctx& c, double kappa) {
+// The contact energy's term sums into device slots slot0 .. slot0 + 4 (no
+// host synchronisation); contactEnergyCombine adds them in a fixed order.
+void contactEnergySums(Ctx& c, int slot0) {
     const SimParams& P = c.P;
     int n = std::max(std::max(c.nGround, c.nSelf), std::max(c.nMoll, std::max(c.nFric, c.nFricG)));
     c.energyBuf.reserve(std::max(n, 1));
-    // every term's sum stays on the device until one read-back; the terms
-    // combine on the host in the fixed order below
     if (c.nGround) {
         launch(groundEnergyKernel, blocksFor(c.nGround), TB, 0, c.s, c.nGround, c.ground, c.x, P.groundN[0], P.groundN[1], P.groundN[2], P.groundD, P.Hhat,
                                                                 c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nGround, 0);
+        deviceSumTo(c, c.energyBuf, c.nGround, slot0 + 0);
     }
     if (c.nSelf) {
         launch(selfEnergyKernel, blocksFor(c.nSelf), TB, 0, c.s, c.nSelf, c.selfActive, c.x, P.Hhat, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nSelf, 1);
+        deviceSumTo(c, c.energyBuf, c.nSelf, slot0 + 1);
     }
     if (c.nMoll) {
         launch(mollEnergyKernel, blocksFor(c.nMoll), TB, 0, c.s, c.nMoll, c.selfEE, c.eeIe, c.edges, c.x, c.rest, P.Hhat, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nMoll, 2);
+        deviceSumTo(c, c.energyBuf, c.nMoll, slot0 + 2);
     }
     double eps2 = P.Fhat * P.dt * P.dt;
     if (c.nFric) {
         launch(frictionEnergyKernel, blocksFor(c.nFric), TB, 0, c.s, c.nFric, c.fricSet, c.x, c.vp, c.fricCoord, c.fricBasis, c.fricLambda, eps2, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nFric, 3);
+        deviceSumTo(c, c.energyBuf, c.nFric, slot0 + 3);
     }
     if (c.nFricG) {
         launch(frictionGroundEnergyKernel, blocksFor(c.nFricG), TB, 0, c.s, c.nFricG, c.fricGround, c.fricGLambda, c.x, c.vp, P.groundN[0], P.groundN[1],
                                                                         P.groundN[2], eps2, P.friction, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nFricG, 4);
+        deviceSumTo(c, c.energyBuf, c.nFricG, slot0 + 4);
     }
+}
+
+double contactEnergyCombine(const Ctx& c, double kappa, const double* h) {
     if (!(c.nGround || c.nSelf || c.nMoll || c.nFric || c.nFricG)) return 0.0;
-    double h[5];
-    fetchSums(c, h, 5);
     double bsum = 0;
     if (c.nGround) bsum += h[0];
     if (c.nSelf) bsum += h[1];
     if (c.nMoll) bsum += h[2];
     double E = kappa * bsum;
-    if (c.nFric) E += P.friction * h[3];
+    if (c.nFric) E += c.P.friction * h[3];
     if (c.nFricG) E += h[4];
     return E;
+}
+
+double contactEnergy(Ctx& c, double kappa) {
+    if (!(c.nGround || c.nSelf || c.nMoll || c.nFric || c.nFricG)) return 0.0;
+    contactEnergySums(c, 0);
+    double h[5];
+    fetchSums(c, h, 5);
+    return contactEnergyCombine(c, kappa, h);
 }
 
 // Friction::initialize at the current x with kappa = P.kappa.

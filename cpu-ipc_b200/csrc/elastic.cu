@@ -635,44 +635,53 @@ void gatherGradient(Ctx& c) {
     CIPC_CUDA(cudaGetLastError());
 }
 
-double elasticEnergy(Ctx& c) {
+// The elastic energy's term sums into device slots slot0 .. slot0 + 4 (no
+// host synchronisation); elasticEnergyCombine adds them in a fixed order.
+void elasticEnergySums(Ctx& c, int slot0) {
     const SimParams& P = c.P;
     int n = std::max(std::max(c.nt, c.nf), std::max(c.nb, c.nv));
     c.energyBuf.reserve(std::max(n, 1));
-    // every term's sum stays on the device until one read-back; the terms
-    // combine on the host in the fixed order below
     const int ns = (int)c.hSoftIdx.size();
     if (c.nt) {
         launch(tetEnergyKernel, blocksFor(c.nt), TB, 0, c.s, c.nt, c.tets, c.x, c.DmInv, c.vol, c.tetMu, c.tetLam, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nt, 0);
+        deviceSumTo(c, c.energyBuf, c.nt, slot0 + 0);
     }
     if (c.nf) {
         launch(triEnergyKernel, blocksFor(c.nf), TB, 0, c.s, c.nf, c.tris, c.x, c.DmInv2, c.area, P.stretchS, P.shearS, P.strainRate, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nf, 1);
+        deviceSumTo(c, c.energyBuf, c.nf, slot0 + 1);
     }
     if (c.nb) {
         if (c.hinge)
             launch(hingeEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, (const double*)c.hingeW, (const double*)c.hingeTh0, c.x, c.energyBuf);
         else
             launch(bendEnergyKernel, blocksFor(c.nb), TB, 0, c.s, c.nb, c.bendV, c.bendQ, c.x, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, c.nb, 2);
+        deviceSumTo(c, c.energyBuf, c.nb, slot0 + 2);
     }
     launch(inertiaEnergyKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.x, c.xt, c.vp, c.mass, P.drag, c.energyBuf);
-    deviceSumTo(c, c.energyBuf, c.nv, 3);
+    deviceSumTo(c, c.energyBuf, c.nv, slot0 + 3);
     if (ns) {
         launch(softEnergyKernel, blocksFor(ns), TB, 0, c.s, ns, c.softIdx, c.softTarget, P.softW, c.x, c.energyBuf);
-        deviceSumTo(c, c.energyBuf, ns, 4);
+        deviceSumTo(c, c.energyBuf, ns, slot0 + 4);
     }
-    double h[5];
-    fetchSums(c, h, 5);
+}
+
+double elasticEnergyCombine(const Ctx& c, const double* h) {
+    const SimParams& P = c.P;
     double E = 0;
     if (c.nt) E += h[0];
     if (c.nf) E += h[1];
     if (c.nb) E += 0.5 * P.plateRigidity * h[2];
     E *= P.dt * P.dt;
     E += h[3];
-    if (ns) E += h[4];
+    if (!c.hSoftIdx.empty()) E += h[4];
     return E;
+}
+
+double elasticEnergy(Ctx& c) {
+    elasticEnergySums(c, 0);
+    double h[5];
+    fetchSums(c, h, 5);
+    return elasticEnergyCombine(c, h);
 }
 
 namespace {

@@ -90,7 +90,15 @@ void stepForward(Ctx& c, const double* x0, const double* d, double alpha, bool a
     launch(stepForwardKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, x0, d, c.btype, alpha, all ? 1 : 0, c.x);
 }
 
-double totalEnergy(Ctx& c, double kappa) { return elasticEnergy(c) + contactEnergy(c, kappa); }
+// Elastic plus contact energy with one read-back of all term sums.
+double totalEnergy(Ctx& c, double kappa) {
+    elasticEnergySums(c, 0);
+    const bool contact = c.nGround || c.nSelf || c.nMoll || c.nFric || c.nFricG;
+    if (contact) contactEnergySums(c, 5);
+    double h[10];
+    fetchSums(c, h, contact ? 10 : 5);
+    return elasticEnergyCombine(c, h) + (contact ? contactEnergyCombine(c, kappa, h + 5) : 0.0);
+}
 
 void suggestKappa(double& kappa, double Hhat, double bbox2, double meanMass) {
     double d = 1.0e-16 * bbox2, t = d - Hhat;
@@ -578,7 +586,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
         DBuf<uint64_t>* us[] = {&c.ccdPT, &c.ccdEE, &c.kPT, &c.kEE, &c.kMoll, &c.kPPE, &c.kTmp, &c.uniq, &c.dynHKey, &c.dynHKeyAlt,
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();
-        c.sortTmp.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
+        c.sortTmp.free(); c.groundTmp.free(); c.stepScal.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
         for (cudaEvent_t e : c.profEv) cudaEventDestroy(e);
         if (c.s) cudaStreamDestroy(c.s);
         delete h->c;
