@@ -86,6 +86,9 @@ def lib():
         L.cipc_gpu_get_scalars.argtypes = [vp, _dp]
         L.cipc_gpu_set_kappa.argtypes = [vp, C.c_double]
         L.cipc_gpu_set_intersection_rule.argtypes = [vp, C.c_int]
+        L.cipc_gpu_set_online_training.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_ulonglong]
+        L.cipc_gpu_set_system_dump.argtypes = [vp, C.c_char_p]
+        L.cipc_gpu_hook_systems.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.cipc_gpu_get_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.cipc_gpu_get_surface.argtypes = [vp, _ip, _ip, _ip]
         L.cipc_gpu_build_collision_sets.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -126,7 +129,8 @@ EXPORTED_SYMBOLS = [
     "cipc_gpu_intersected", "cipc_gpu_accd", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
     "cipc_gpu_kernel_launches", "cipc_gpu_pcg_bsr_noalloc", "cipc_gpu_export_bsr", "cipc_gpu_precond_num_params",
     "cipc_gpu_precond_set_weights", "cipc_gpu_precond_get_weights", "cipc_gpu_precond_loss", "cipc_gpu_precond_train",
-    "cipc_gpu_precond_stats", "cipc_gpu_precond_factor",
+    "cipc_gpu_precond_stats", "cipc_gpu_precond_factor", "cipc_gpu_set_online_training", "cipc_gpu_set_system_dump",
+    "cipc_gpu_hook_systems",
 ]
 NOALLOC_MAX_ROWS = 32768
 
@@ -284,6 +288,20 @@ class Simulator:
     def set_kappa(self, k):
         self._chk(self.L.cipc_gpu_set_kappa(self.h, float(k)))
 
+    def set_online_training(self, iterations, probes=4, lr=1e-3, seed=0):
+        """Adam iterations of the network on every Newton system as it is
+        assembled (0 turns it off)."""
+        self._chk(self.L.cipc_gpu_set_online_training(self.h, int(iterations), int(probes), float(lr), int(seed)))
+
+    def set_system_dump(self, directory):
+        """Write every Newton system to `directory` (None turns it off)."""
+        self._chk(self.L.cipc_gpu_set_system_dump(self.h, None if directory is None else str(directory).encode()))
+
+    def hook_systems(self):
+        n = C.c_longlong(0)
+        self._chk(self.L.cipc_gpu_hook_systems(self.h, C.byref(n)))
+        return n.value
+
     def set_intersection_rule(self, rule):
         """'tolerant' (default) or 'reference' (the reference's exact
         segment-triangle coplanarity rule)."""
@@ -414,6 +432,38 @@ def pcg_bsr(row_ptr, col_idx, vals, rhs, precision="fp64", tol=1e-6, max_iter=10
     if rc != CIPC_OK:
         raise CipcError(rc, err.value.decode())
     return sol, it.value, rr.value
+
+
+def read_system(path):
+    """A Newton system written by Simulator.set_system_dump (file layout in
+    include/cipc_gpu.h, cipc_gpu_set_system_dump)."""
+    with open(path, "rb") as f:
+        buf = f.read()
+    if buf[:8] != b"CIPCSYS1":
+        raise ValueError(f"{path} is not a dumped Newton system")
+    nv, nnzb, ndyn, vb, frame, newton = np.frombuffer(buf, np.int32, 6, 8)
+    off = 32
+    def take(dtype, n):
+        nonlocal off
+        a = np.frombuffer(buf, dtype, n, off)
+        off += a.nbytes
+        return a
+    vt = np.float32 if vb == 4 else np.float64
+    out = dict(frame=int(frame), newton=int(newton))
+    out["row_ptr"] = take(np.int32, nv + 1)
+    out["col"] = take(np.int32, nnzb)
+    out["val"] = take(vt, 9 * nnzb).reshape(nnzb, 3, 3)
+    out["dyn_row_start"] = take(np.int32, nv)
+    out["dyn_row_end"] = take(np.int32, nv)
+    out["dyn_col"] = take(np.int32, ndyn) if ndyn else np.zeros(0, np.int32)
+    out["dyn_val"] = take(vt, 9 * ndyn).reshape(ndyn, 3, 3) if ndyn else np.zeros((0, 3, 3), vt)
+    out["diag_extra"] = take(np.float64, 9 * nv).reshape(nv, 3, 3)
+    out["rhs"] = take(np.float64, 3 * nv).reshape(nv, 3)
+    out["x"] = take(np.float64, 3 * nv).reshape(nv, 3)
+    out["btype"] = take(np.int32, nv)
+    if off != len(buf):
+        raise ValueError(f"{path}: {len(buf) - off} trailing bytes")
+    return out
 
 
 def accd(kind, positions, displacements, eta=0.2):

@@ -99,6 +99,14 @@ struct Ctx {
     // refused for the rest of the context's life
     bool tcFault = false;
     DBuf<double> stepScal;  // device scalars of the chained step bounds
+    // hook at the linear-solve seam (NewtonLinearSystem::solve): Adam
+    // iterations of the network on every assembled Newton system, and/or a
+    // dump of every system to files in dumpDir
+    int hookTrainIters = 0, hookTrainProbes = 4;
+    double hookTrainLr = 1e-3;
+    unsigned long long hookTrainSeed = 0;
+    long long hookSystems = 0;  // systems the hook has seen
+    std::string dumpDir;
 
     // host mirrors needed by the driver
     std::vector<int> hBtype, hSoftIdx, hDirIdx;

@@ -251,8 +251,65 @@ static void requireSystem(const Ctx& c) {
     if (!c.assembled) throw InvalidArgument("no assembled Newton system: step or assemble first");
 }
 
-void linearSolve(Ctx& c) {
+// The Newton system at the solve seam, as a file: magic "CIPCSYS1", then
+// int32 nv, nnzb, ndyn, value bytes (4 or 8), frame, Newton index; static
+// BSR row pointers (nv+1) and columns (nnzb), values (9 per block), contact
+// BSR row starts and ends (nv each), columns (ndyn), values (9 per block);
+// FP64 per-vertex diagonal extras (9 nv), right-hand side (3 nv), positions
+// (3 nv); int32 boundary types (nv).
+static void dumpSystem(Ctx& c, int newton) {
+    const int nv = c.nv, nnzb = c.nnzb, ndyn = c.nDynB, vb = c.mixed ? 4 : 8;
+    char name[64];
+    std::snprintf(name, sizeof(name), "/system_%06d_%03d.bin", c.stepIndex, newton);
+    const std::string path = c.dumpDir + name;
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write " + path);
+    auto put = [&](const void* p, size_t bytes) {
+        if (bytes && std::fwrite(p, 1, bytes, f) != bytes) { std::fclose(f); throw std::runtime_error("short write to " + path); }
+    };
+    auto dev = [&](const void* d, size_t bytes) {
+        std::vector<char> h(bytes);
+        if (bytes) CIPC_CUDA(cudaMemcpy(h.data(), d, bytes, cudaMemcpyDeviceToHost));
+        put(h.data(), bytes);
+    };
+    sync(c);
+    const int head[6] = {nv, nnzb, ndyn, vb, c.stepIndex, newton};
+    put("CIPCSYS1", 8);
+    put(head, sizeof(head));
+    dev(c.rowPtr.p, sizeof(int) * (nv + 1));
+    dev(c.colIdx.p, sizeof(int) * (size_t)nnzb);
+    dev(c.mixed ? (const void*)c.valF.p : (const void*)c.valD.p, (size_t)vb * 9 * nnzb);
+    if (ndyn) {
+        dev(c.dynRowStart.p, sizeof(int) * nv);
+        dev(c.dynRowEnd.p, sizeof(int) * nv);
+        dev(c.dynCol.p, sizeof(int) * (size_t)ndyn);
+        dev(c.mixed ? (const void*)c.dynBF.p : (const void*)c.dynBD.p, (size_t)vb * 9 * ndyn);
+    } else {
+        std::vector<int> z(2 * (size_t)nv, 0);
+        put(z.data(), sizeof(int) * z.size());
+    }
+    dev(c.diagExtra.p, sizeof(double) * 9 * nv);
+    dev(c.rhs.p, sizeof(double) * 3 * nv);
+    dev(c.x.p, sizeof(double) * 3 * nv);
+    dev(c.btype.p, sizeof(int) * nv);
+    std::fclose(f);
+}
+
+void linearSolve(Ctx& c, int newton = 0) {
     buildRhs(c);
+    if (c.hookTrainIters > 0 || !c.dumpDir.empty()) {
+        if (!c.dumpDir.empty()) dumpSystem(c, newton);
+        if (c.hookTrainIters > 0) {
+            if (!c.mpReady) mpnnInitWeights(c, 1);
+            mpnnPrepare(c);
+            for (int it = 0; it < c.hookTrainIters; ++it) {
+                mpnnForward(c);
+                mpnnLoss(c, c.hookTrainProbes, nullptr, c.hookTrainSeed + 104729ull * (unsigned long long)(c.mpStep + 1), true);
+                mpnnAdam(c, c.hookTrainLr);
+            }
+        }
+        ++c.hookSystems;
+    }
     pcgSolve(c);
     CIPC_CUDA(cudaMemcpyAsync(c.dir.p, c.sol.p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToDevice, c.s));
 }
@@ -267,7 +324,7 @@ int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
         st.collisions += assembleAll(c);
         sync(c);
         auto t1 = Clock::now();
-        linearSolve(c);
+        linearSolve(c, k);
         st.pcgIterations += c.lastPcgIters;
         st.pcgRelativeResidual = std::max(st.pcgRelativeResidual, c.lastPcgRelRes);
         st.matrixBlocks = std::max<long long>(st.matrixBlocks, (long long)c.nnzb + c.nDynB);
@@ -919,6 +976,25 @@ int cipc_gpu_precond_train(cipc_gpu_context* h, int iterations, int probes, doub
         }
         sync(c);
     });
+}
+
+int cipc_gpu_set_online_training(cipc_gpu_context* h, int iterations, int probes, double learningRate, unsigned long long seed) {
+    return guarded(h, [&](Ctx& c) {
+        if (iterations < 0 || (iterations > 0 && (probes < 1 || !(learningRate > 0))))
+            throw InvalidArgument("online training needs non-negative iterations, probes and a positive rate");
+        c.hookTrainIters = iterations;
+        c.hookTrainProbes = probes;
+        c.hookTrainLr = learningRate;
+        c.hookTrainSeed = seed;
+    });
+}
+
+int cipc_gpu_set_system_dump(cipc_gpu_context* h, const char* directory) {
+    return guarded(h, [&](Ctx& c) { c.dumpDir = directory ? directory : ""; });
+}
+
+int cipc_gpu_hook_systems(cipc_gpu_context* h, long long* count) {
+    return guarded(h, [&](Ctx& c) { *count = c.hookSystems; });
 }
 
 int cipc_gpu_precond_factor(cipc_gpu_context* h, int which, float* gStatic, float* gContact) {

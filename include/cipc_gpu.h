@@ -210,6 +210,23 @@ int cipc_gpu_precond_loss(cipc_gpu_context* ctx, int probes, const float* probeV
  * `probes` probe vectors per step; losses of the first and last step. */
 int cipc_gpu_precond_train(cipc_gpu_context* ctx, int iterations, int probes, double learningRate, unsigned long long seed, double* lossFirst,
                            double* lossLast);
+/* Hook at the linear-solve seam of every Newton iteration
+ * (NewtonLinearSystem::solve, NewtonLinearSystem.cpp:39; no counterpart in
+ * the reference otherwise).  With iterations > 0 the network takes that many
+ * Adam steps on each assembled Newton system before it is solved (the
+ * systems the simulator produces train the network as they arise; 0 turns
+ * it off). */
+int cipc_gpu_set_online_training(cipc_gpu_context* ctx, int iterations, int probes, double learningRate, unsigned long long seed);
+/* With a directory, every Newton system is written there before its solve,
+ * one file per system (system_<frame>_<newton>.bin: magic "CIPCSYS1", int32
+ * nv, nnzb, ndyn, value bytes, frame, Newton index; static BSR row pointers,
+ * columns, values; contact BSR row starts, ends, columns, values; FP64
+ * diagonal extras, right-hand side, positions; int32 boundary types).  NULL
+ * or "" turns it off. */
+int cipc_gpu_set_system_dump(cipc_gpu_context* ctx, const char* directory);
+/* Newton systems the hook has trained on or written since creation. */
+int cipc_gpu_hook_systems(cipc_gpu_context* ctx, long long* count);
+
 /* Builds the factor of preconditioner `which` (CIPC_PRECOND_LEARNED: the
  * network forward; CIPC_PRECOND_FSAI: the exact factorised sparse
  * approximate inverse of the same pattern) on the last assembled system and
