@@ -41,6 +41,7 @@ struct Options {
     int cells = 10;
     int precision = CIPC_PRECISION_MIXED;
     int precond = CIPC_PRECOND_BLOCK_JACOBI;
+    int broadPhase = CIPC_BROAD_PHASE_LBVH;  // cipc_headless --broad-phase
     bool writeOutput = true;
     bool verbose = false;
     bool disableBarrier = false;
@@ -59,6 +60,7 @@ void usage(const char* exe) {
               << "  --linear-solver gpu-pcg\n"
               << "  --precision fp64|mixed  (default mixed)\n"
               << "  --precond jacobi|learned|fsai (default jacobi)\n"
+              << "  --broad-phase lbvh|spatial-hash (default lbvh)\n"
               << "  --weights FILE          learned-preconditioner weights (raw float32)\n"
               << "  --output DIRECTORY      metrics.csv, timeCost.txt and tempData/ go here\n"
               << "  --resume                start from the checkpoint in DIRECTORY/tempData\n"
@@ -107,6 +109,11 @@ Options parse(int argc, char** argv) {
             else if (v == "learned") o.precond = CIPC_PRECOND_LEARNED;
             else if (v == "fsai") o.precond = CIPC_PRECOND_FSAI;
             else throw std::invalid_argument("unknown preconditioner: " + v);
+        } else if (a == "--broad-phase") {
+            std::string v = value("--broad-phase");
+            if (v == "lbvh") o.broadPhase = CIPC_BROAD_PHASE_LBVH;
+            else if (v == "spatial-hash") o.broadPhase = CIPC_BROAD_PHASE_SPATIAL_HASH;
+            else throw std::invalid_argument("unknown broad phase: " + v);
         } else if (a == "--disable-barrier") o.disableBarrier = true;
         else if (a == "--resume") o.resume = true;
         else if (a == "--write-checkpoints") o.writeCheckpoints = true;
@@ -413,6 +420,7 @@ int main(int argc, char** argv) {
         lo_.relativeTolerance = 1e-6;
         lo_.maximumIterations = 10000;
         check(cipc_gpu_create(&d, &lo_, &ctx), nullptr, "cipc_gpu_create");
+        if (o.broadPhase != CIPC_BROAD_PHASE_LBVH) check(cipc_gpu_set_broad_phase(ctx, o.broadPhase), ctx, "cipc_gpu_set_broad_phase");
 
         if (!o.weights.empty()) {
             int n = cipc_gpu_precond_num_params();

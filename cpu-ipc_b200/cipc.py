@@ -86,6 +86,7 @@ def lib():
         L.cipc_gpu_get_scalars.argtypes = [vp, _dp]
         L.cipc_gpu_set_kappa.argtypes = [vp, C.c_double]
         L.cipc_gpu_set_intersection_rule.argtypes = [vp, C.c_int]
+        L.cipc_gpu_set_broad_phase.argtypes = [vp, C.c_int]
         L.cipc_gpu_set_online_training.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_ulonglong]
         L.cipc_gpu_set_system_dump.argtypes = [vp, C.c_char_p]
         L.cipc_gpu_hook_systems.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -123,7 +124,7 @@ def lib():
 
 EXPORTED_SYMBOLS = [
     "cipc_gpu_create", "cipc_gpu_destroy", "cipc_gpu_last_error", "cipc_gpu_create_error", "cipc_gpu_step",
-    "cipc_gpu_get_state", "cipc_gpu_set_state", "cipc_gpu_get_scalars", "cipc_gpu_set_kappa", "cipc_gpu_set_intersection_rule", "cipc_gpu_get_counts",
+    "cipc_gpu_get_state", "cipc_gpu_set_state", "cipc_gpu_get_scalars", "cipc_gpu_set_kappa", "cipc_gpu_set_intersection_rule", "cipc_gpu_set_broad_phase", "cipc_gpu_get_counts",
     "cipc_gpu_get_surface", "cipc_gpu_build_collision_sets", "cipc_gpu_get_active_sets", "cipc_gpu_friction_init",
     "cipc_gpu_assemble", "cipc_gpu_export_matrix", "cipc_gpu_solve", "cipc_gpu_energy", "cipc_gpu_step_bounds",
     "cipc_gpu_intersected", "cipc_gpu_accd", "cipc_gpu_pcg_bsr", "cipc_gpu_timed_steps", "cipc_gpu_profile", "cipc_gpu_profile_read",
@@ -301,6 +302,10 @@ class Simulator:
         n = C.c_longlong(0)
         self._chk(self.L.cipc_gpu_hook_systems(self.h, C.byref(n)))
         return n.value
+
+    def set_broad_phase(self, backend):
+        """'lbvh' (default) or 'spatial-hash'."""
+        self._chk(self.L.cipc_gpu_set_broad_phase(self.h, {"lbvh": 0, "spatial-hash": 1}[backend]))
 
     def set_intersection_rule(self, rule):
         """'tolerant' (default) or 'reference' (the reference's exact

@@ -79,6 +79,12 @@ struct DevBvh {
     DBuf<double> sceneBox;     // 6
     DBuf<double> boxPart;      // 6 per block of the scene-box reduction
     DBuf<float> rec;           // 16 per internal node: both children's boxes (rounded outward) and indices
+    // spatial-hash backend over the same primitive boxes: (cell key,
+    // primitive) pairs sorted by key, and the primitives too large to insert
+    int hashPairs = 0;
+    DBuf<uint64_t> hashKey, hashKeyAlt;
+    DBuf<int> hashPrim, hashPrimAlt, hashCount, hashOffset, hashBig, hashBigFlag;
+    DBuf<unsigned char> hashTmp;
 };
 
 struct Ctx {
@@ -86,6 +92,7 @@ struct Ctx {
     int nv = 0, nt = 0, nf = 0, nb = 0, nsf = 0, nsv = 0, nse = 0;
     int mixed = 0;             // 0 FP64 Hessian/SpMV, 1 FP32
     int precond = 0;           // 0 block-Jacobi, 1 learned
+    int broadPhase = 0;        // CIPC_BROAD_PHASE_LBVH or CIPC_BROAD_PHASE_SPATIAL_HASH
     double pcgTol = 1e-6;
     int pcgMaxIter = 10000;
     SimParams P;

@@ -15,6 +15,7 @@
 // * Partial CCD, full (swept) CCD, ground bound, CFL bound and the
 //   edge-triangle intersection test (IPCSolver.cpp:476-542, 943-990;
 //   ContactMechanics.cpp:3704-3867; FeasibleStep.cpp:8-40).
+#include "../../include/cipc_gpu.h"
 #include "cipc_internal.h"
 #include "geometry.cuh"
 
@@ -318,6 +319,106 @@ __device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, co
     }
 }
 
+// ---------------------------------------------------------------------------
+// Spatial-hash backend (the reference's SpatialHash, CollisionBroadPhase.cpp:
+// 11-763, as an A/B alternative to the LBVH): every primitive box is entered
+// in the cubic cells of edge `h` (the mean surface edge length, as the
+// reference's sh.build(mesh, averageEdgeLenth)) that it touches, as
+// (cell key, primitive) pairs sorted by key.  A query visits the cells of its
+// box grown by the gap (and one cell more on each side, against rounding),
+// finds each cell's run by binary search, and reports a primitive only in the
+// lowest cell it shares with the query, after the same inclusive FP64 box
+// test as the LBVH walk - so both backends report the same set.  Primitives
+// touching more than HASH_MAX_CELLS cells are kept in a list that every query
+// tests; a query touching more than HASH_MAX_QUERY cells tests all
+// primitives.
+// ---------------------------------------------------------------------------
+constexpr int HASH_MAX_CELLS = 64;
+constexpr long long HASH_MAX_QUERY = 4096;
+constexpr int HASH_BIAS = 1 << 20;  // cell coordinates are offset into [0, 2^21)
+
+struct HashView {
+    int n, pairs;
+    double inv;
+    const uint64_t* key;
+    const int* prim;
+    const int* big;
+    const int* nbig;
+    const double *plo, *phi;
+};
+
+__device__ __forceinline__ int hashCell(double v, double inv) {
+    const double c = floor(v * inv) + (double)HASH_BIAS;
+    return (int)fmin(fmax(c, 0.0), (double)(2 * HASH_BIAS - 1));
+}
+__device__ __forceinline__ uint64_t hashKeyOf(int ix, int iy, int iz) {
+    return ((uint64_t)ix << 42) | ((uint64_t)iy << 21) | (uint64_t)iz;
+}
+
+template <class F>
+__device__ __forceinline__ void traverse(const HashView& t, const double* qlo, const double* qhi, double gap, int* status, F f) {
+    if (t.n <= 0) return;
+    int lo[3], hi[3];
+    long long cells = 1;
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = max(hashCell(qlo[k] - gap, t.inv) - 1, 0);
+        hi[k] = min(hashCell(qhi[k] + gap, t.inv) + 1, 2 * HASH_BIAS - 1);
+        cells *= (long long)(hi[k] - lo[k] + 1);
+    }
+    if (cells > HASH_MAX_QUERY) {  // a large query box: test every primitive
+        for (int p = 0; p < t.n; ++p)
+            if (overlaps(qlo, qhi, t.plo + 3 * p, t.phi + 3 * p, gap)) f(p);
+        return;
+    }
+    for (int iz = lo[2]; iz <= hi[2]; ++iz)
+        for (int iy = lo[1]; iy <= hi[1]; ++iy)
+            for (int ix = lo[0]; ix <= hi[0]; ++ix) {
+                const uint64_t key = hashKeyOf(ix, iy, iz);
+                int a = 0, b = t.pairs;  // first pair with a key >= key
+                while (a < b) {
+                    const int m = (a + b) >> 1;
+                    if (t.key[m] < key) a = m + 1;
+                    else b = m;
+                }
+                for (int k = a; k < t.pairs && t.key[k] == key; ++k) {
+                    const int p = t.prim[k];
+                    const double* pl = t.plo + 3 * p;
+                    // the lowest cell the primitive shares with the query
+                    if (max(hashCell(pl[0], t.inv), lo[0]) != ix || max(hashCell(pl[1], t.inv), lo[1]) != iy ||
+                        max(hashCell(pl[2], t.inv), lo[2]) != iz)
+                        continue;
+                    if (overlaps(qlo, qhi, pl, t.phi + 3 * p, gap)) f(p);
+                }
+            }
+    const int nb = *t.nbig;
+    for (int b = 0; b < nb; ++b) {
+        const int p = t.big[b];
+        if (overlaps(qlo, qhi, t.plo + 3 * p, t.phi + 3 * p, gap)) f(p);
+    }
+}
+
+__global__ void hashCountKernel(int n, const double* plo, const double* phi, double inv, int* count, int* bigFlag) {
+    CIPC_KERNEL_LOOP(p, n) {
+        long long cells = 1;
+        for (int k = 0; k < 3; ++k) cells *= (long long)(hashCell(phi[3 * p + k], inv) - hashCell(plo[3 * p + k], inv) + 1);
+        const bool big = cells > HASH_MAX_CELLS;
+        count[p] = big ? 0 : (int)cells;
+        bigFlag[p] = big ? 1 : 0;
+    }
+}
+
+__global__ void hashEmitKernel(int n, const double* plo, const double* phi, double inv, const int* offset, const int* count, uint64_t* key, int* prim) {
+    CIPC_KERNEL_LOOP(p, n) {
+        if (count[p] == 0) continue;
+        int lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) { lo[k] = hashCell(plo[3 * p + k], inv); hi[k] = hashCell(phi[3 * p + k], inv); }
+        int o = offset[p];
+        for (int iz = lo[2]; iz <= hi[2]; ++iz)
+            for (int iy = lo[1]; iy <= hi[1]; ++iy)
+                for (int ix = lo[0]; ix <= hi[0]; ++ix) { key[o] = hashKeyOf(ix, iy, iz); prim[o] = p; ++o; }
+    }
+}
+
 __device__ __forceinline__ bool isCollider(int t) { return t >= 2; }
 
 // Packed PP/PE key: lexicographic order of (c0 = -v-1, c1, c2) with c3 = -1.
@@ -345,7 +446,8 @@ struct Emit {
     }
 };
 
-__global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, BvhView tree, double sq,
+template <class View>
+__global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, View tree, double sq,
                                double Hhat, Emit ccd, Emit ptk, Emit ppe, int* status) {
     CIPC_KERNEL_LOOP(svI, nsv) {
         int vI = surfVerts[svI];
@@ -372,7 +474,8 @@ __global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, 
     }
 }
 
-__global__ void activeEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* rest, BvhView tree, double sq,
+template <class View>
+__global__ void activeEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* rest, View tree, double sq,
                                double Hhat, Emit ccd, Emit eek, Emit moll, Emit ppe, int* status) {
     CIPC_KERNEL_LOOP(eI, ne) {
         int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
@@ -504,8 +607,9 @@ __global__ void partialCCDKernel(int nPT, int nEE, const uint64_t* ccdPT, const 
     }
 }
 
+template <class View>
 __global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, const double* dir, double stepVal,
-                             const double* stepPtr, BvhView tree, double eta, double* out, int* status) {
+                             const double* stepPtr, View tree, double eta, double* out, int* status) {
     const double step = stepPtr ? *stepPtr : stepVal;
     CIPC_KERNEL_LOOP(svI, nsv) {
         int vI = surfVerts[svI];
@@ -525,8 +629,9 @@ __global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, co
     }
 }
 
+template <class View>
 __global__ void fullEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* dir, const double* treeBoxLo,
-                             const double* treeBoxHi, double eeStepVal, const double* eeStepPtr, BvhView tree, double eta, double* out, int* status) {
+                             const double* treeBoxHi, double eeStepVal, const double* eeStepPtr, View tree, double eta, double* out, int* status) {
     const double eeStep = eeStepPtr ? *eeStepPtr : eeStepVal;
     CIPC_KERNEL_LOOP(eJ, ne) {
         int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
@@ -556,7 +661,8 @@ __global__ void fullEEKernel(int ne, const int* edges, const int* btype, const d
     }
 }
 
-__global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, BvhView tree, double coplanarTol,
+template <class View>
+__global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, View tree, double coplanarTol,
                                 int* flag, int* status) {
     CIPC_KERNEL_LOOP(f, nsf) {
         int f0 = faces[3 * f], f1 = faces[3 * f + 1], f2 = faces[3 * f + 2];
@@ -640,11 +746,71 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     CIPC_CUDA(cudaGetLastError());
 }
 
+// The spatial-hash tables of one primitive set from its boxes (primLo/Hi).
+void buildHash(Ctx& c, DevBvh& t, int n) {
+    t.n = n;
+    t.hashPairs = 0;
+    t.hashBig.reserve(std::max(1, n)); t.hashBigFlag.reserve(std::max(1, n));
+    t.hashCount.reserve(std::max(1, n)); t.hashOffset.reserve(std::max(1, n));
+    c.counters.reserve(16);
+    if (n <= 0) return;
+    const double inv = 1.0 / c.P.avgEdge;
+    launch(hashCountKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, inv, t.hashCount, t.hashBigFlag);
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, t.hashCount.p, t.hashOffset.p, n, c.s);
+    size_t b2 = 0;
+    cub::DeviceSelect::Flagged(nullptr, b2, cub::CountingInputIterator<int>(0), t.hashBigFlag.p, t.hashBig.p, c.counters.p + 11, n, c.s);
+    t.hashTmp.reserve(std::max(bytes, b2) + 16);
+    CIPC_CUDA(cub::DeviceScan::ExclusiveSum(t.hashTmp.p, bytes, t.hashCount.p, t.hashOffset.p, n, c.s));
+    int last[2];
+    CIPC_CUDA(cudaMemcpyAsync(&last[0], t.hashOffset.p + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaMemcpyAsync(&last[1], t.hashCount.p + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    const int pairs = last[0] + last[1];
+    t.hashPairs = pairs;
+    t.hashKey.reserve(std::max(1, pairs)); t.hashKeyAlt.reserve(std::max(1, pairs));
+    t.hashPrim.reserve(std::max(1, pairs)); t.hashPrimAlt.reserve(std::max(1, pairs));
+    launch(hashEmitKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, inv, (const int*)t.hashOffset, (const int*)t.hashCount, t.hashKeyAlt,
+           t.hashPrimAlt);
+    if (pairs > 0) {
+        size_t b3 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, b3, t.hashKeyAlt.p, t.hashKey.p, t.hashPrimAlt.p, t.hashPrim.p, pairs, 0, 63, c.s);
+        t.hashTmp.reserve(b3 + 16);
+        CIPC_CUDA(cub::DeviceRadixSort::SortPairs(t.hashTmp.p, b3, t.hashKeyAlt.p, t.hashKey.p, t.hashPrimAlt.p, t.hashPrim.p, pairs, 0, 63, c.s));
+    }
+    // the primitives too large for the cells (their ids in order)
+    cub::CountingInputIterator<int> ids(0);
+    size_t b4 = 0;
+    cub::DeviceSelect::Flagged(nullptr, b4, ids, t.hashBigFlag.p, t.hashBig.p, c.counters.p + (&t == &c.edgeTree ? 14 : 11), n, c.s);
+    t.hashTmp.reserve(b4 + 16);
+    CIPC_CUDA(cub::DeviceSelect::Flagged(t.hashTmp.p, b4, ids, t.hashBigFlag.p, t.hashBig.p, c.counters.p + (&t == &c.edgeTree ? 14 : 11), n,
+                                         c.s));
+    CIPC_CUDA(cudaGetLastError());
+}
+
+HashView hview(Ctx& c, const DevBvh& t) {
+    return HashView{t.n, t.hashPairs, 1.0 / c.P.avgEdge, t.hashKey, t.hashPrim, t.hashBig, c.counters.p + (&t == &c.edgeTree ? 14 : 11),
+                    t.primLo, t.primHi};
+}
+
+// The broad-phase structure of one primitive set, LBVH or spatial hash.
+void buildBroad(Ctx& c, DevBvh& t, int n) {
+    if (c.broadPhase == CIPC_BROAD_PHASE_SPATIAL_HASH) buildHash(c, t, n);
+    else buildBvh(c, t, n);
+}
+
+// Calls k(view) with the selected backend's view of tree t.
+template <class K>
+void withView(Ctx& c, const DevBvh& t, K k) {
+    if (c.broadPhase == CIPC_BROAD_PHASE_SPATIAL_HASH) k(hview(c, t));
+    else k(view(t));
+}
+
 static void buildStaticTrees(Ctx& c) {
     computeFaceBoxes(c, c.x, c.x, 0.0, false);
-    buildBvh(c, c.faceTree, c.nsf);
+    buildBroad(c, c.faceTree, c.nsf);
     computeEdgeBoxes(c, c.x, c.x, 0.0, false);
-    buildBvh(c, c.edgeTree, c.nse);
+    buildBroad(c, c.edgeTree, c.nse);
 }
 
 // Ground::calculateActivateSet: the surface vertices within dHat of the
@@ -694,11 +860,11 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             Emit eCcdEE{c.ccdEE, caps[3], c.counters.p + 3}, eEE{c.kEE, caps[4], c.counters.p + 4}, eMoll{c.kMoll, caps[5], c.counters.p + 5};
             profBegin(c, PROF_ACTIVE);
             if (c.nsv)
-                launch(activePTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, view(c.faceTree), sq, c.P.Hhat,
-                                                                  eCcdPT, ePT, ePPE, c.status);
+                withView(c, c.faceTree, [&](auto v) { launch(activePTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, v, sq, c.P.Hhat,
+                                                                  eCcdPT, ePT, ePPE, c.status); });
             if (c.nse)
-                launch(activeEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.rest, view(c.edgeTree), sq, c.P.Hhat, eCcdEE,
-                                                                  eEE, eMoll, ePPE, c.status);
+                withView(c, c.edgeTree, [&](auto v) { launch(activeEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.rest, v, sq, c.P.Hhat, eCcdEE,
+                                                                  eEE, eMoll, ePPE, c.status); });
             profEnd(c, PROF_ACTIVE);
             CIPC_CUDA(cudaGetLastError());
             CIPC_CUDA(cudaMemcpyAsync(cnt, c.counters.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
@@ -768,8 +934,8 @@ bool isIntersected(Ctx& c) {
     if (c.nGround)
         launch(groundIntersectKernel, blocksFor(c.nGround), TB, 0, c.s, c.nGround, c.ground, c.x, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2],
                                                                    c.P.groundD, c.counters.p + 7);
-    if (c.nsf) launch(intersectKernel, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, view(c.edgeTree), c.coplanarTol, c.counters.p + 7,
-                            c.status);
+    if (c.nsf) withView(c, c.edgeTree, [&](auto v) { launch(intersectKernel<decltype(v)>, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, v, c.coplanarTol, c.counters.p + 7,
+                            c.status); });
     int f = 0, st = 0;
     CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
@@ -812,21 +978,21 @@ double cflBound(Ctx& c) {
 double fullCCDDir(Ctx& c, const double* d, double alpha) {
     double step = alpha;
     computeFaceBoxes(c, c.x, d, step, true);
-    buildBvh(c, c.faceTree, c.nsf);
+    buildBroad(c, c.faceTree, c.nsf);
     computeEdgeBoxes(c, c.x, d, step, true);
-    buildBvh(c, c.edgeTree, c.nse);
+    buildBroad(c, c.edgeTree, c.nse);
     c.energyBuf.reserve(std::max(std::max(c.nsv, c.nse), 1));
     if (c.nsv) {
         profBegin(c, PROF_FULLCCD);
-        launch(fullPTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, step, (const double*)nullptr, view(c.faceTree),
-               1.0 - 0.8, c.energyBuf, c.status);
+        withView(c, c.faceTree, [&](auto v) { launch(fullPTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, step, (const double*)nullptr, v,
+               1.0 - 0.8, c.energyBuf, c.status); });
         profEnd(c, PROF_FULLCCD);
         step = std::min(step, deviceMin(c, c.energyBuf, c.nsv, 1e308));
     }
     if (c.nse) {
         profBegin(c, PROF_FULLCCD);
-        launch(fullEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi, step,
-               (const double*)nullptr, view(c.edgeTree), 1.0 - 0.8, c.energyBuf, c.status);
+        withView(c, c.edgeTree, [&](auto v) { launch(fullEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi, step,
+               (const double*)nullptr, v, 1.0 - 0.8, c.energyBuf, c.status); });
         profEnd(c, PROF_FULLCCD);
         step = std::min(step, deviceMin(c, c.energyBuf, c.nse, 1e308));
     }
@@ -898,21 +1064,21 @@ double stepBoundsDevice(Ctx& c) {
             deviceMaxTo(c, c.energyBuf, c.nsv, s + 2);
         }
         computeFaceBoxes(c, c.x, c.dir, 0.0, true, s + 3);
-        buildBvh(c, c.faceTree, c.nsf);
+        buildBroad(c, c.faceTree, c.nsf);
         computeEdgeBoxes(c, c.x, c.dir, 0.0, true, s + 3);
-        buildBvh(c, c.edgeTree, c.nse);
+        buildBroad(c, c.edgeTree, c.nse);
         if (c.nsv) {
             profBegin(c, PROF_FULLCCD);
-            launch(fullPTKernel, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, c.dir, 0.0, (const double*)(s + 3),
-                   view(c.faceTree), 1.0 - 0.8, c.energyBuf, c.status);
+            withView(c, c.faceTree, [&](auto v) { launch(fullPTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, c.dir, 0.0, (const double*)(s + 3),
+                   v, 1.0 - 0.8, c.energyBuf, c.status); });
             profEnd(c, PROF_FULLCCD);
             deviceMinTo(c, c.energyBuf, c.nsv, s + 4);
             launch(stepEeEntryKernel, 1, 1, 0, c.s, s);
         }
         if (c.nse) {
             profBegin(c, PROF_FULLCCD);
-            launch(fullEEKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.dir, c.edgeTree.primLo, c.edgeTree.primHi, 0.0,
-                   (const double*)(s + 5), view(c.edgeTree), 1.0 - 0.8, c.energyBuf, c.status);
+            withView(c, c.edgeTree, [&](auto v) { launch(fullEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.dir, c.edgeTree.primLo, c.edgeTree.primHi, 0.0,
+                   (const double*)(s + 5), v, 1.0 - 0.8, c.energyBuf, c.status); });
             profEnd(c, PROF_FULLCCD);
             deviceMinTo(c, c.energyBuf, c.nse, s + 6);
         }

@@ -644,6 +644,10 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();
         c.sortTmp.free(); c.groundTmp.free(); c.stepScal.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
+        for (DevBvh* t : {&c.faceTree, &c.edgeTree}) {
+            t->hashKey.free(); t->hashKeyAlt.free(); t->hashPrim.free(); t->hashPrimAlt.free(); t->hashCount.free(); t->hashOffset.free();
+            t->hashBig.free(); t->hashBigFlag.free(); t->hashTmp.free();
+        }
         for (cudaEvent_t e : c.profEv) cudaEventDestroy(e);
         if (c.s) cudaStreamDestroy(c.s);
         delete h->c;
@@ -699,6 +703,17 @@ int cipc_gpu_get_scalars(cipc_gpu_context* h, double* o) {
 
 int cipc_gpu_set_kappa(cipc_gpu_context* h, double kappa) {
     return guarded(h, [&](Ctx& c) { c.P.kappa = kappa; });
+}
+
+int cipc_gpu_set_broad_phase(cipc_gpu_context* h, int backend) {
+    return guarded(h, [&](Ctx& c) {
+        if (backend != CIPC_BROAD_PHASE_LBVH && backend != CIPC_BROAD_PHASE_SPATIAL_HASH) throw InvalidArgument("unknown broad-phase backend");
+        if (backend != c.broadPhase) {
+            c.broadPhase = backend;
+            rebuildTrees(c);  // the structures the next query reads
+            sync(c);
+        }
+    });
 }
 
 int cipc_gpu_set_intersection_rule(cipc_gpu_context* h, int rule) {

@@ -125,6 +125,12 @@ int cipc_gpu_set_kappa(cipc_gpu_context* ctx, double kappa);
  * det == 0 only). */
 enum { CIPC_INTERSECT_TOLERANT = 0, CIPC_INTERSECT_REFERENCE = 1 };
 int cipc_gpu_set_intersection_rule(cipc_gpu_context* ctx, int rule);
+/* Broad-phase backend (cipc_headless --broad-phase, the reference's
+ * SpatialHash or LBVH, CollisionBroadPhase.cpp:11-763, LBVH.cpp:163-282):
+ * both report the same candidate sets after the same exact box test; the
+ * LBVH is the default. */
+enum { CIPC_BROAD_PHASE_LBVH = 0, CIPC_BROAD_PHASE_SPATIAL_HASH = 1 };
+int cipc_gpu_set_broad_phase(cipc_gpu_context* ctx, int backend);
 /* counts: nv, nsf, nsv, nse, nbend, nt, nf, nnzb (static BSR blocks),
  * contact BSR blocks of the last assembly */
 int cipc_gpu_get_counts(cipc_gpu_context* ctx, long long* out9);
