@@ -4,13 +4,14 @@ configurations' own sizes.
 * Two cubes of 8^3 cells (3,072 tets each), Newton tolerance 1e-6, FP64, 100
   steps from rest: trajectories within 1e-6 of the bounding-box diagonal,
   checked every 10 steps.
-* The 128x128 cloth drape (16,384 cloth vertices on the 10^3-cell cube) and an
-  8-cube pile of 12^3 cells, each from a contact-phase state the oracle
-  itself produced (oracle/states/): contact sets bit-exact; gradient, Newton
-  matrix and energy within 1e-10 relative; step bounds within 1e-6 and never
-  above the oracle's; then three steps of trajectory in FP64 and in mixed
-  precision with the learned factor (weights trained on the restored system,
-  then frozen), within 1e-6 of the bounding-box diagonal.
+* The 128x128 cloth drape (16,384 cloth vertices on the 10^3-cell cube), the
+  64-cube pile of 12^3 cells (663,552 tets) and an 8-cube pile, each from a
+  contact-phase state the oracle itself produced (oracle/states/): contact
+  sets bit-exact; gradient, Newton matrix and energy within 1e-10 relative;
+  step bounds within 1e-6 and never above the oracle's; then (cloth and
+  8-cube pile) three steps of trajectory in FP64 and in mixed precision with
+  the learned factor (weights trained on the restored system, then frozen),
+  within 1e-6 of the bounding-box diagonal.
 * A twisted cylinder of 8 x 32 x 64 layers (92,160 tets, animated Dirichlet
   caps): ten steps of trajectory.
 * Additive CCD candidate by candidate: every partial-CCD candidate pair of
@@ -85,7 +86,12 @@ def test_two_cubes_8_cells_100_steps(oracle_mod):
 CONTACT_STATES = {
     "cloth_drape_128": (lambda: cipc.scene_cloth_drape(128, 10), "cloth_drape_128_frame40.npz"),
     "pile_8x12": (lambda: cipc.scene_pile(8, 12), "pile_8x12_frame60.npz"),
+    # the pile configuration itself (64 cubes, 663,552 tets) in the frame the
+    # bench's timed steps start from: sets, system and bounds (its oracle
+    # steps take minutes each, so its trajectory is checked on the 8-cube pile)
+    "pile_64x12": (lambda: cipc.scene_pile(64, 12), "pile_64x12_frame35.npz"),
 }
+NO_TRAJECTORY = {"pile_64x12"}
 
 
 @pytest.fixture(scope="module", params=list(CONTACT_STATES))
@@ -136,6 +142,8 @@ def test_contact_state_three_steps(oracle_mod, contact_state):
     blocks with the learned factor (trained on the restored state's Newton
     system for 30 Adam iterations, then frozen)."""
     name, sc, path, o = contact_state
+    if name in NO_TRAJECTORY:
+        pytest.skip("trajectory checked on the smaller pile")
     o.restore_state(path)
     dt = sc["params"]["dt"]
     g64 = cipc.Simulator(sc, surface=o.surface())
