@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <stdexcept>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -187,6 +188,14 @@ struct Ctx {
     int lastPcgLaunchIters = 0;
     DBuf<unsigned> pcgBar;              // grid-barrier counters of the persistent PCG
     DBuf<double> pcgPipe, pcgParts;     // pipelined PCG: six recurrence vectors, two sets of partial sums
+    // the factor packed for the streaming PCG: lower part (columns <= row) and
+    // transposed part (columns >= row, diagonal transposed) of the static
+    // slots as compact rows of FP16 blocks (9 halves each); the index lists
+    // depend only on the static pattern and are built once
+    DBuf<int> gLptr, gLcol, gLslot, gUptr, gUcol, gUslot;
+    DBuf<uint16_t> gLval, gUval;
+    int nGL = 0, nGU = 0;
+    bool factorPacked = false;
     int pcgSliceMax = -1;               // cached pipelined PCG: largest static-slot count of a block's rows
     int pcgSliceRows = 0;               // the block row count pcgSliceMax was computed for
     bool assembled = false;             // a Newton system has been assembled

@@ -15,6 +15,7 @@
 // the true residual b - A x in FP64 (FP32 blocks promoted) and stops on the
 // same FP64 criterion as the FP64 solver.
 #include "cipc_device.cuh"
+#include <cuda_fp16.h>
 #include "cipc_gpu.h"
 #include "cipc_internal.h"
 #include "fsai.h"
@@ -42,6 +43,17 @@ __device__ __forceinline__ void blockMulAdd(const MT* B, const VT* xv, VT acc[3]
     acc[0] += (VT)B[0] * xv[0] + (VT)B[1] * xv[1] + (VT)B[2] * xv[2];
     acc[1] += (VT)B[3] * xv[0] + (VT)B[4] * xv[1] + (VT)B[5] * xv[2];
     acc[2] += (VT)B[6] * xv[0] + (VT)B[7] * xv[1] + (VT)B[8] * xv[2];
+}
+
+// acc += B x for a 3x3 block of FP16 values (row-major)
+template <class VT>
+__device__ __forceinline__ void blockMulAddH(const __half* B, const VT* xv, VT acc[3]) {
+    VT b[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) b[e] = (VT)__half2float(B[e]);
+    acc[0] += b[0] * xv[0] + b[1] * xv[1] + b[2] * xv[2];
+    acc[1] += b[3] * xv[0] + b[4] * xv[1] + b[5] * xv[2];
+    acc[2] += b[6] * xv[0] + b[7] * xv[1] + b[8] * xv[2];
 }
 
 // y = A x ; partial[block] = sum over the block's rows of x . y (for p.Ap)
@@ -273,6 +285,10 @@ struct PcgArgs {
     // learned factor (null for block-Jacobi): S 9 per vertex, G slot-aligned
     const double* S;
     const float *gS, *gD;
+    // the static part of G packed by rows (null: read gS): lower part and
+    // transposed part, FP16 blocks with their columns and row offsets
+    const __half *gL, *gU;
+    const int *gLptr, *gLcol, *gUptr, *gUcol;
     VT* t;
     const VT* b;
     VT *x, *r, *z, *p, *Ap;
@@ -471,7 +487,17 @@ __device__ __forceinline__ void rowSpmv(const PcgArgs<MT, VT>& a, int row, int l
 // (G^T u)_row (TR = true: mirror slots and the transposed diagonal block)
 template <bool TR, class MT, class VT>
 __device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int lane, const VT* u, VT acc[3]) {
-    for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
+    if (a.gL) {
+        // packed rows: only the blocks of this pass, FP16
+        const int* ptr = TR ? a.gUptr : a.gLptr;
+        const int* cl = TR ? a.gUcol : a.gLcol;
+        const __half* G = TR ? a.gU : a.gL;
+        for (int k = ptr[row] + lane; k < ptr[row + 1]; k += GROUP) {
+            const int c = cl[k];
+            VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
+            blockMulAddH(G + (size_t)9 * k, xv, acc);
+        }
+    } else for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
         int c = a.col[k];
         if (TR ? c < row : c > row) continue;
         VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
@@ -1146,6 +1172,55 @@ __global__ void zeroKernel(int n3, double* x) {
 
 }  // namespace
 
+// packed[k] = the FP16 block of slot slot[k] of G (transposed where the
+// slot is stored as ~slot: the diagonal blocks of the transposed part)
+__global__ void packFactorKernel(int n, const int* slot, const float* gS, __half* out) {
+    CIPC_KERNEL_LOOP(i, 9 * n) {
+        const int k = i / 9, e = i - 9 * k;
+        const int s = slot[k];
+        const bool tr = s < 0;
+        const int src = tr ? 3 * (e % 3) + e / 3 : e;
+        out[i] = __float2half_rn(gS[(size_t)9 * (tr ? ~s : s) + src]);
+    }
+}
+
+// The factor's static blocks in the packed layout the streaming PCG reads
+// (rowFactor): per row the slots with column <= row (G), then those with
+// column >= row (G^T: the mirror slots, and the diagonal transposed).  The
+// index lists follow the static pattern and are built on the first call.
+static void packFactor(Ctx& c) {
+    const int nv = c.nv;
+    if (c.nGL == 0) {
+        std::vector<int> col(c.nnzb);
+        CIPC_CUDA(cudaMemcpy(col.data(), c.colIdx.p, sizeof(int) * c.nnzb, cudaMemcpyDeviceToHost));
+        std::vector<int> lp(nv + 1, 0), lc, ls, up(nv + 1, 0), uc, us;
+        lc.reserve(c.nnzb / 2 + nv); ls.reserve(c.nnzb / 2 + nv); uc.reserve(c.nnzb / 2 + nv); us.reserve(c.nnzb / 2 + nv);
+        for (int r = 0; r < nv; ++r) {
+            for (int k = c.hRowPtr[r]; k < c.hRowPtr[r + 1]; ++k) {
+                const int cl = col[k];
+                if (cl <= r) { lc.push_back(cl); ls.push_back(k); }
+                if (cl >= r) { uc.push_back(cl); us.push_back(cl == r ? ~k : k); }
+            }
+            lp[r + 1] = (int)lc.size();
+            up[r + 1] = (int)uc.size();
+        }
+        auto up_ = [&](DBuf<int>& d, const std::vector<int>& h) {
+            d.reserve(std::max<size_t>(h.size(), 1));
+            if (!h.empty()) CIPC_CUDA(cudaMemcpy(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+        };
+        up_(c.gLptr, lp); up_(c.gLcol, lc); up_(c.gLslot, ls); up_(c.gUptr, up); up_(c.gUcol, uc); up_(c.gUslot, us);
+        c.nGL = (int)lc.size();
+        c.nGU = (int)uc.size();
+        c.gLval.reserve(9 * (size_t)std::max(1, c.nGL));
+        c.gUval.reserve(9 * (size_t)std::max(1, c.nGU));
+    }
+    const int vb = std::max(1, std::min((9 * c.nGL + VB - 1) / VB, 148 * 16));
+    launch(packFactorKernel, vb, VB, 0, c.s, c.nGL, (const int*)c.gLslot, (const float*)c.mpGS, reinterpret_cast<__half*>(c.gLval.p));
+    const int ub = std::max(1, std::min((9 * c.nGU + VB - 1) / VB, 148 * 16));
+    launch(packFactorKernel, ub, VB, 0, c.s, c.nGU, (const int*)c.gUslot, (const float*)c.mpGS, reinterpret_cast<__half*>(c.gUval.p));
+    CIPC_CUDA(cudaGetLastError());
+}
+
 void buildRhs(Ctx& c) {
     c.rhs.reserve(3 * c.nv);
     launch(rhsKernel, vecBlocks(c.nv), VB, 0, c.s, c.nv, c.grad, c.btype, c.rhs);
@@ -1236,6 +1311,13 @@ static int pcgBlocksPerSm() {
 static bool pcgClassic() {
     static int v = -1;
     if (v < 0) { const char* e = std::getenv("CIPC_PCG_CLASSIC"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+
+// CIPC_PCG_NOPACK=1 keeps the streaming kernel on the slot-aligned FP32 factor.
+static bool pcgNoPack() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_PCG_NOPACK"); v = (e && *e == '1') ? 1 : 0; }
     return v == 1;
 }
 
@@ -1346,9 +1428,14 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
     a.dRowS = dyn ? c.dynRowStart.p : nullptr; a.dRowE = dyn ? c.dynRowEnd.p : nullptr; a.dCol = dyn ? c.dynCol.p : nullptr; a.dVal = dval;
     a.diagExtra = c.diagExtra; a.Dinv = c.Dinv; a.b = b; a.x = x; a.r = r; a.z = z; a.p = p; a.Ap = Ap;
     a.S = nullptr; a.gS = nullptr; a.gD = nullptr; a.t = nullptr;
+    a.gL = a.gU = nullptr; a.gLptr = a.gLcol = a.gUptr = a.gUcol = nullptr;
     if (learned) {
         c.mpT.reserve(3 * (size_t)c.nv);
         a.S = c.mpS.p; a.gS = c.mpGS.p; a.gD = c.mpGD.p; a.t = reinterpret_cast<VT*>(c.mpT.p);
+        if (c.factorPacked) {
+            a.gL = reinterpret_cast<const __half*>(c.gLval.p); a.gU = reinterpret_cast<const __half*>(c.gUval.p);
+            a.gLptr = c.gLptr.p; a.gLcol = c.gLcol.p; a.gUptr = c.gUptr.p; a.gUcol = c.gUcol.p;
+        }
     }
     a.partA = c.red.p; a.partB = c.red.p + PMAX; a.partC = c.red.p + 2 * PMAX;
     // pipelined kernel: six more vectors and two sets of partial sums
@@ -1392,15 +1479,23 @@ static void reservePcg(Ctx& c) {
 // Builds the factor for the current system (network forward, or the exact
 // FSAI); false when block-Jacobi is selected.
 static bool prepareLearned(Ctx& c) {
+    c.factorPacked = false;
     if (c.precond == CIPC_PRECOND_FSAI) {
         mpnnPrepare(c, false);
         fsaiBuild(c);
-        return true;
+    } else if (c.precond == CIPC_PRECOND_LEARNED) {
+        if (!c.mpReady) mpnnInitWeights(c, 1);
+        mpnnPrepare(c);
+        mpnnForward(c);
+    } else {
+        return false;
     }
-    if (c.precond != CIPC_PRECOND_LEARNED) return false;
-    if (!c.mpReady) mpnnInitWeights(c, 1);
-    mpnnPrepare(c);
-    mpnnForward(c);
+    // the streaming kernel (systems too large for the single-pass cache)
+    // reads the factor's static part packed by rows in FP16
+    if (!pcgNoPack()) {
+        packFactor(c);
+        c.factorPacked = true;
+    }
     return true;
 }
 

@@ -644,6 +644,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();
         c.sortTmp.free(); c.groundTmp.free(); c.stepScal.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
+        c.gLptr.free(); c.gLcol.free(); c.gLslot.free(); c.gUptr.free(); c.gUcol.free(); c.gUslot.free(); c.gLval.free(); c.gUval.free();
         for (DevBvh* t : {&c.faceTree, &c.edgeTree}) {
             t->hashKey.free(); t->hashKeyAlt.free(); t->hashPrim.free(); t->hashPrimAlt.free(); t->hashCount.free(); t->hashOffset.free();
             t->hashBig.free(); t->hashBigFlag.free(); t->hashTmp.free();
