@@ -124,7 +124,7 @@ __global__ void selfBarrierKernel(int n, const int* active, const double* x, con
         int kind = decode(active + 4 * i, idx);
         int np = npts(kind), nd = 3 * np;
         int ne = nd == 9 ? 10 : nd;
-        double cf;
+        double cf, ca = 0.0, cb = 0.0;
         if (lane == 0) {
             d3 p[4];
             for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
@@ -137,14 +137,21 @@ __global__ void selfBarrierKernel(int n, const int* active, const double* x, con
             distDerivs(kind, p, g, withHessian ? S.B : nullptr);
             for (int k = 0; k < nd; ++k) S.V[k] = cf * gb * g[k];
             if (!isfinite(d)) raiseStatus(status, CIPC_ST_NONFINITE);
-            if (withHessian) {
-                double a = cf * hb, b = cf * gb;
-                for (int r = 0; r < ne; ++r)
-                    for (int q = 0; q < ne; ++q)
-                        S.A[r * ne + q] = (r < nd && q < nd) ? (a * g[r]) * g[q] + b * S.B[r * nd + q] : 0.0;
-            }
+            ca = cf * hb;
+            cb = cf * gb;
         }
         __syncwarp();
+        if (withHessian) {
+            // kappa (b'' g g^T + b' H), the warp's lanes over the entries
+            ca = __shfl_sync(0xffffffffu, ca, 0);
+            cb = __shfl_sync(0xffffffffu, cb, 0);
+            const double* g = S.W;
+            for (int e = lane; e < ne * ne; e += 32) {
+                const int r = e / ne, q = e - r * ne;
+                S.A[e] = (r < nd && q < nd) ? (ca * g[r]) * g[q] + cb * S.B[r * nd + q] : 0.0;
+            }
+            __syncwarp();
+        }
         // gradient entries (4 per contact)
         if (lane < 4) {
             size_t slot = gBase + 4 * (size_t)i + lane;
