@@ -446,21 +446,41 @@ __global__ void slotReduceKernel(int nnzb, const int* hcPtr, const int* hcIdx, c
     }
 }
 
+// Per-vertex gradient: vertex terms plus the vertex's element and contact
+// contributions.  GG lanes share a vertex: each sums a fixed stride of the
+// contribution list, then the group adds the lanes' sums in a fixed order
+// (deterministic).
+constexpr int GG = 8;
 __global__ void gatherGradKernel(int nv, const double* vtxGrad, const int* gcPtr, const int* gcIdx, const double* elemG,
                                  const int* dynStart, const int* dynEnd, const int* dynIdx, const double* dynVal, double* grad) {
-    CIPC_KERNEL_LOOP(v, nv) {
-        double g[3] = {vtxGrad[3 * v], vtxGrad[3 * v + 1], vtxGrad[3 * v + 2]};
-        for (int k = gcPtr[v]; k < gcPtr[v + 1]; ++k) {
-            int e = gcIdx[k];
+    const int lane = threadIdx.x % GG;
+    const int stride = gridDim.x * blockDim.x / GG;
+    // the loop bound is the warp's first vertex, so that all 32 lanes take
+    // part in every shuffle (blockDim is a multiple of 32)
+    const int warpFirst = (blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / GG;
+    for (int w0 = warpFirst; w0 < nv; w0 += stride) {
+        const int v = w0 + (threadIdx.x & 31) / GG;
+        const bool active = v < nv;
+        double g[3] = {0.0, 0.0, 0.0};
+        if (active) for (int k = gcPtr[v] + lane; k < gcPtr[v + 1]; k += GG) {
+            const int e = gcIdx[k];
             g[0] += elemG[3 * e]; g[1] += elemG[3 * e + 1]; g[2] += elemG[3 * e + 2];
         }
-        if (dynStart) {
-            for (int k = dynStart[v]; k < dynEnd[v]; ++k) {
-                int e = dynIdx[k];
+        if (dynStart && active) {
+            for (int k = dynStart[v] + lane; k < dynEnd[v]; k += GG) {
+                const int e = dynIdx[k];
                 g[0] += dynVal[3 * e]; g[1] += dynVal[3 * e + 1]; g[2] += dynVal[3 * e + 2];
             }
         }
-        grad[3 * v] = g[0]; grad[3 * v + 1] = g[1]; grad[3 * v + 2] = g[2];
+#pragma unroll
+        for (int o = GG / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) g[q] += __shfl_down_sync(0xffffffffu, g[q], o, GG);
+        if (active && lane == 0) {
+            grad[3 * v] = vtxGrad[3 * v] + g[0];
+            grad[3 * v + 1] = vtxGrad[3 * v + 1] + g[1];
+            grad[3 * v + 2] = vtxGrad[3 * v + 2] + g[2];
+        }
     }
 }
 
@@ -630,7 +650,7 @@ void assembleElastic(Ctx& c) {
 
 void gatherGradient(Ctx& c) {
     bool dyn = c.nDynG > 0;
-    launch(gatherGradKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, c.vtxGrad, c.gcPtr, c.gcIdx, c.elemG, dyn ? c.dynGStart.p : nullptr,
+    launch(gatherGradKernel, blocksFor(GG * c.nv), TB, 0, c.s, c.nv, c.vtxGrad, c.gcPtr, c.gcIdx, c.elemG, dyn ? c.dynGStart.p : nullptr,
                                                       dyn ? c.dynGEnd.p : nullptr, dyn ? c.dynGIdx.p : nullptr, c.dynGVal, c.grad);
     CIPC_CUDA(cudaGetLastError());
 }
