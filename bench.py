@@ -170,10 +170,12 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
+def ncu_traffic(workload_name):
+    """DRAM bytes (read + write) of one launch of the PCG kernel on this
+    workload from an ncu capture (profiles/roofline_traffic.json), or None."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(p):
-        d = json.load(open(p)).get(kernel)
+        d = json.load(open(p)).get(workload_name)
         if d:
             return d.get("bytes_per_launch")
     return None
@@ -188,23 +190,24 @@ def spmv_bytes(counts, mixed):
 
 
 def pcg_iteration_bytes(counts, mixed, factor):
-    """Algorithmic bytes of one iteration of the pipelined PCG kernel: every
-    static and contact block with its column index once (A m), row pointers,
-    the diagonal extras and the block-Jacobi inverse, the gathered m, the
-    per-row recurrence vectors (z, q, s, p, x, r, u, w read and written, m
-    read and the next m written; FP64 vectors); with a factor also its
-    blocks (both triangles once), the scaling blocks twice and the extra
-    gathered vectors of its two passes."""
+    """Algorithmic bytes of one PCG iteration, as the survey's measurement
+    section defines them: every static and contact block of A with its
+    column index once (full symmetric storage: 36 B FP32 or 72 B FP64 + 4),
+    the row pointers, eight vectors of 3 FP32 per vertex, and the 3x3
+    preconditioner block per vertex (block-Jacobi inverse, or the factor's
+    scaling S).  A factor adds its blocks once: the static part as stored for
+    the streaming kernel (FP16, both the lower and the transposed part, 18 B
+    + 4 B column; the diagonal in both) and the contact part (FP32, 36 + 4)."""
     nv, nnzb, ndyn = counts[0], counts[7], counts[8]
     blk = 36 if mixed else 72
-    vec = 24
-    b = (nnzb + ndyn) * (blk + 4) + (nv + 1) * 4 + nv * 72 + nv * vec
-    b += nv * vec * 18
+    b = (nnzb + ndyn) * (blk + 4) + (nv + 1) * 4 + 8 * nv * 12 + nv * 36
     if factor:
-        b += (nnzb + ndyn) * (36 + 8) + nv * 36 + 2 * nv * 72 + 4 * nv * vec
-    else:
-        b += nv * 72
+        b += (nnzb + nv) * (18 + 4) + ndyn * (36 + 4)
     return b
+
+
+# grid barriers per PCG iteration of the pipelined kernel
+BARRIERS_PER_ITERATION = {False: 1, True: 3}
 
 
 def host_threads():
@@ -457,10 +460,13 @@ def main():
             bytes_ = per_it * r["pcg"] / r["nprof"]
             avg_ms = r["prof_ms"] / r["nprof"]
             achieved = bytes_ / (avg_ms / 1000.0) / 1e9
+            iters_per_launch = r["pcg"] / r["nprof"]
             roof = {"kernel": "pcgPipelinedKernel (whole PCG solve, one cooperative launch)", "bound": "hbm", "achieved": achieved,
-                    "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic("pcg"),
+                    "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(workload(args)),
                     "algorithmic_bytes_per_launch": bytes_, "bytes_per_iteration": per_it, "launches": r["nprof"],
-                    "mean_launch_us": 1000 * avg_ms, "share_of_step_time": r["prof_ms"] / r["ms"]}
+                    "mean_launch_us": 1000 * avg_ms, "us_per_iteration": 1000 * avg_ms / max(1e-9, iters_per_launch),
+                    "barriers_per_iteration": BARRIERS_PER_ITERATION[args.precond != "jacobi"],
+                    "share_of_step_time": r["prof_ms"] / r["ms"]}
         cfg = {"workload": workload(args), "description": describe(args), "newton_threshold": scene["params"]["newtonThr"],
                "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
                "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
