@@ -21,6 +21,7 @@
 
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 
@@ -124,8 +125,21 @@ __device__ __forceinline__ uint32_t quantize(double v) {
     return (uint32_t)v;
 }
 
-__global__ void mortonKernel(int n, const double* lo, const double* hi, const double* scene, uint64_t* keys) {
+// Morton keys (30-bit code << 32 | index).  A primitive whose box spans
+// more than bigExtent along an axis (the walls of a container, a fast swept
+// primitive) gets bit 62 instead: the sort moves it past the others, the
+// tree is built over the rest, and every query tests the few large ones
+// directly - a large box would otherwise widen all its ancestors' boxes and
+// draw every query down their paths.  *nbig counts them.
+__global__ void mortonKernel(int n, const double* lo, const double* hi, const double* scene, double bigExtent, uint64_t* keys, int* nbig) {
     CIPC_KERNEL_LOOP(i, n) {
+        bool big = false;
+        for (int k = 0; k < 3; ++k) big = big || (hi[3 * i + k] - lo[3 * i + k] > bigExtent);
+        if (big) {
+            atomicAdd(nbig, 1);
+            keys[i] = (1ull << 62) | (uint32_t)i;
+            continue;
+        }
         double c[3], q[3];
         for (int k = 0; k < 3; ++k) {
             c[k] = 0.5 * (lo[3 * i + k] + hi[3 * i + k]);
@@ -144,7 +158,8 @@ __device__ __forceinline__ int prefixLen(const uint64_t* k, int n, int a, int b)
     return x == 0 ? 64 : __clzll(x);
 }
 
-__global__ void karrasKernel(int n, const uint64_t* keys, int* left, int* right, int* parent) {
+__global__ void karrasKernel(int nAll, const int* nbig, const uint64_t* keys, int* left, int* right, int* parent) {
+    const int n = nAll - *nbig;  // leaves of the tree (the large primitives stay out)
     CIPC_KERNEL_LOOP(in, n - 1) {
         int first, last;
         if (in == 0) { first = 0; last = n - 1; }
@@ -181,8 +196,9 @@ __global__ void karrasKernel(int n, const uint64_t* keys, int* left, int* right,
     }
 }
 
-__global__ void leafKernel(int n, const uint64_t* keys, const double* plo, const double* phi, int* leafPrim, double* lo, double* hi,
-                           int* flags, int* parent) {
+__global__ void leafKernel(int nAll, const int* nbig, const uint64_t* keys, const double* plo, const double* phi, int* leafPrim, double* lo,
+                           double* hi, int* flags, int* parent) {
+    const int n = nAll - *nbig;
     CIPC_KERNEL_LOOP(s, n) {
         int prim = (int)(keys[s] & 0xffffffffu);
         leafPrim[s] = prim;
@@ -207,7 +223,10 @@ __device__ __forceinline__ int atomAddAcqRel(int* p, int v) {
 // record: the boxes of both children rounded outward to FP32 (lo down, hi
 // up) and the children's node indices, 64 bytes, so that one load tests
 // both children.
-__global__ void refitKernel(int n, const int* left, const int* right, const int* parent, double* lo, double* hi, int* flags, float* rec) {
+__global__ void refitKernel(int nAll, const int* nbig, const int* left, const int* right, const int* parent, double* lo, double* hi, int* flags,
+                            float* rec) {
+    const int n = nAll - *nbig;
+    if (n <= 1) return;
     CIPC_KERNEL_LOOP(s, n) {
         int node = s + n - 1;
         int p = parent[node];
@@ -249,7 +268,8 @@ __global__ void refitKernel(int n, const int* left, const int* right, const int*
 // nearest ancestor that is a left child; -1 past the last leaf.  One thread
 // per node walks up the parent links (at most the tree's depth, which the
 // 64-bit keys bound by 64).
-__global__ void escapeKernel(int n, const int* left, const int* right, const int* parent, int* escape) {
+__global__ void escapeKernel(int nAll, const int* nbig, const int* left, const int* right, const int* parent, int* escape) {
+    const int n = nAll - *nbig;
     CIPC_KERNEL_LOOP(node, 2 * n - 1) {
         int cur = node, e = -1;
         for (int guard = 0; guard < 128; ++guard) {
@@ -263,13 +283,17 @@ __global__ void escapeKernel(int n, const int* left, const int* right, const int
 }
 
 struct BvhView {
-    int n;
+    int nAll;         // primitives; the tree holds nAll - *nbig of them
+    const int* nbig;  // primitives kept out of the tree (their keys sort last)
+    const uint64_t* keys;
     const int *left, *right, *leafPrim, *escape;
     const double *lo, *hi;
+    const double *plo, *phi;  // primitive boxes
     const float4* rec;
 };
 BvhView view(const DevBvh& t) {
-    return BvhView{t.n, t.left, t.right, t.leafPrim, t.escape, t.lo, t.hi, reinterpret_cast<const float4*>(t.rec.p)};
+    return BvhView{t.n, t.bigCount.p, t.keys, t.left, t.right, t.leafPrim, t.escape, t.lo, t.hi, t.primLo, t.primHi,
+                   reinterpret_cast<const float4*>(t.rec.p)};
 }
 
 // Stack-less depth-first traversal along escape indices; calls f(prim) once
@@ -285,14 +309,14 @@ BvhView view(const DevBvh& t) {
 // collects).  The walk visits each node at most once; a count past the node
 // count raises a status bit.
 template <class F>
-__device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, const double* qhi, double gap, int* status, F f) {
-    if (t.n <= 0) return;
+__device__ __forceinline__ void traverseTree(const BvhView& t, int n, const double* qlo, const double* qhi, double gap, int* status, F& f) {
+    if (n <= 0) return;
     if (!overlaps(qlo, qhi, t.lo, t.hi, gap)) return;  // the root (node 0)
-    if (t.n == 1) { f(t.leafPrim[0]); return; }
-    const int firstLeaf = t.n - 1;
+    if (n == 1) { f(t.leafPrim[0]); return; }
+    const int firstLeaf = n - 1;
     int cur = 0;  // an internal node whose box overlaps the query
     for (int visits = 0; cur >= 0; ++visits) {
-        if (visits > 2 * t.n) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
+        if (visits > 2 * n) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
         const float4* r = t.rec + 4 * (size_t)cur;
         const float4 a = r[0], b = r[1], cc = r[2], d = r[3];
         const double lo0[3] = {a.x, a.y, a.z}, hi0[3] = {a.w, b.x, b.y};
@@ -306,7 +330,7 @@ __device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, co
         // both children done: follow escape indices to the next node to test
         int e = t.escape[cur];
         while (e >= 0) {
-            if (++visits > 2 * t.n) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
+            if (++visits > 2 * n) { raiseStatus(status, CIPC_ST_STACK_OVERFLOW); return; }
             const bool hit = overlaps(qlo, qhi, t.lo + 3 * e, t.hi + 3 * e, gap);
             if (e >= firstLeaf) {
                 if (hit) f(t.leafPrim[e - firstLeaf]);
@@ -316,6 +340,17 @@ __device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, co
             e = t.escape[e];
         }
         cur = e;
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, const double* qhi, double gap, int* status, F f) {
+    if (t.nAll <= 0) return;
+    const int nb = *t.nbig, n = t.nAll - nb;
+    traverseTree(t, n, qlo, qhi, gap, status, f);
+    for (int b = 0; b < nb; ++b) {
+        const int p = (int)(t.keys[n + b] & 0xffffffffu);
+        if (overlaps(qlo, qhi, t.plo + 3 * p, t.phi + 3 * p, gap)) f(p);
     }
 }
 
@@ -734,15 +769,20 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     t.boxPart.reserve(6 * (size_t)nbBox);
     launch(sceneBoxKernel, nbBox, 256, 0, c.s, n, t.primLo, t.primHi, t.boxPart);
     launch(sceneBoxFinalKernel, 1, 256, 0, c.s, nbBox, (const double*)t.boxPart, t.sceneBox);
-    launch(mortonKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, t.sceneBox, t.keys);
-    // keys are (30-bit code << 32) | index, written in index order: a stable
-    // sort on the code bits gives the order of a sort on the whole key
-    sortKeys(c, t.keys, t.keysAlt, n, 62, 32);
-    if (n > 1) launch(karrasKernel, blocksFor(n - 1), TB, 0, c.s, n, t.keys, t.left, t.right, t.parent);
-    launch(leafKernel, blocksFor(n), TB, 0, c.s, n, t.keys, t.primLo, t.primHi, t.leafPrim, t.lo, t.hi, t.flags, t.parent);
+    t.bigCount.reserve(1);
+    CIPC_CUDA(cudaMemsetAsync(t.bigCount.p, 0, sizeof(int), c.s));
+    const double bigExtent = 0.1 * std::sqrt(c.P.bboxDiag2);
+    launch(mortonKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, t.sceneBox, bigExtent, t.keys, t.bigCount.p);
+    // keys are (code << 32) | index (bit 62: kept out of the tree), written in
+    // index order: a stable sort on bits 32-62 gives the order of a sort on
+    // the whole key
+    sortKeys(c, t.keys, t.keysAlt, n, 63, 32);
+    const int* nbig = t.bigCount.p;
+    if (n > 1) launch(karrasKernel, blocksFor(n - 1), TB, 0, c.s, n, nbig, t.keys, t.left, t.right, t.parent);
+    launch(leafKernel, blocksFor(n), TB, 0, c.s, n, nbig, t.keys, t.primLo, t.primHi, t.leafPrim, t.lo, t.hi, t.flags, t.parent);
     t.rec.reserve(16 * (size_t)std::max(1, n - 1));
-    if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, t.left, t.right, t.parent, t.lo, t.hi, t.flags, t.rec.p);
-    if (n > 1) launch(escapeKernel, blocksFor(nn), TB, 0, c.s, n, t.left, t.right, t.parent, t.escape);
+    if (n > 1) launch(refitKernel, blocksFor(n), TB, 0, c.s, n, nbig, t.left, t.right, t.parent, t.lo, t.hi, t.flags, t.rec.p);
+    if (n > 1) launch(escapeKernel, blocksFor(nn), TB, 0, c.s, n, nbig, t.left, t.right, t.parent, t.escape);
     CIPC_CUDA(cudaGetLastError());
 }
 
@@ -759,7 +799,7 @@ void buildHash(Ctx& c, DevBvh& t, int n) {
     size_t bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, bytes, t.hashCount.p, t.hashOffset.p, n, c.s);
     size_t b2 = 0;
-    cub::DeviceSelect::Flagged(nullptr, b2, cub::CountingInputIterator<int>(0), t.hashBigFlag.p, t.hashBig.p, c.counters.p + 11, n, c.s);
+    cub::DeviceSelect::Flagged(nullptr, b2, thrust::counting_iterator<int>(0), t.hashBigFlag.p, t.hashBig.p, c.counters.p + 11, n, c.s);
     t.hashTmp.reserve(std::max(bytes, b2) + 16);
     CIPC_CUDA(cub::DeviceScan::ExclusiveSum(t.hashTmp.p, bytes, t.hashCount.p, t.hashOffset.p, n, c.s));
     int last[2];
@@ -779,7 +819,7 @@ void buildHash(Ctx& c, DevBvh& t, int n) {
         CIPC_CUDA(cub::DeviceRadixSort::SortPairs(t.hashTmp.p, b3, t.hashKeyAlt.p, t.hashKey.p, t.hashPrimAlt.p, t.hashPrim.p, pairs, 0, 63, c.s));
     }
     // the primitives too large for the cells (their ids in order)
-    cub::CountingInputIterator<int> ids(0);
+    thrust::counting_iterator<int> ids(0);
     size_t b4 = 0;
     cub::DeviceSelect::Flagged(nullptr, b4, ids, t.hashBigFlag.p, t.hashBig.p, c.counters.p + (&t == &c.edgeTree ? 14 : 11), n, c.s);
     t.hashTmp.reserve(b4 + 16);

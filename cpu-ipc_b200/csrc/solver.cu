@@ -647,7 +647,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
         c.gLptr.free(); c.gLcol.free(); c.gLslot.free(); c.gUptr.free(); c.gUcol.free(); c.gUslot.free(); c.gLval.free(); c.gUval.free();
         for (DevBvh* t : {&c.faceTree, &c.edgeTree}) {
             t->hashKey.free(); t->hashKeyAlt.free(); t->hashPrim.free(); t->hashPrimAlt.free(); t->hashCount.free(); t->hashOffset.free();
-            t->hashBig.free(); t->hashBigFlag.free(); t->hashTmp.free();
+            t->hashBig.free(); t->hashBigFlag.free(); t->hashTmp.free(); t->bigCount.free();
         }
         for (cudaEvent_t e : c.profEv) cudaEventDestroy(e);
         if (c.s) cudaStreamDestroy(c.s);
