@@ -81,6 +81,7 @@ struct DevBvh {
     DBuf<double> boxPart;      // 6 per block of the scene-box reduction
     DBuf<float> rec;           // 16 per internal node: both children's boxes (rounded outward) and indices
     DBuf<int> bigCount;        // primitives kept out of the tree (large boxes), tested by every query
+    double bigExtent = 0;      // the box width past which a primitive is large
     // spatial-hash backend over the same primitive boxes: (cell key,
     // primitive) pairs sorted by key, and the primitives too large to insert
     int hashPairs = 0;

@@ -283,6 +283,8 @@ __global__ void escapeKernel(int nAll, const int* nbig, const int* left, const i
 }
 
 struct BvhView {
+    static constexpr bool kSplitsBig = true;  // large primitives are kept out of the tree (see traverse2)
+    double bigExtent;  // a box wider than this along an axis is large
     int nAll;         // primitives; the tree holds nAll - *nbig of them
     const int* nbig;  // primitives kept out of the tree (their keys sort last)
     const uint64_t* keys;
@@ -292,8 +294,12 @@ struct BvhView {
     const float4* rec;
 };
 BvhView view(const DevBvh& t) {
-    return BvhView{t.n, t.bigCount.p, t.keys, t.left, t.right, t.leafPrim, t.escape, t.lo, t.hi, t.primLo, t.primHi,
+    return BvhView{t.bigExtent, t.n, t.bigCount.p, t.keys, t.left, t.right, t.leafPrim, t.escape, t.lo, t.hi, t.primLo, t.primHi,
                    reinterpret_cast<const float4*>(t.rec.p)};
+}
+
+__device__ __forceinline__ bool isLargeBox(const double* lo, const double* hi, double ext) {
+    return (hi[0] - lo[0] > ext) || (hi[1] - lo[1] > ext) || (hi[2] - lo[2] > ext);
 }
 
 // Stack-less depth-first traversal along escape indices; calls f(prim) once
@@ -354,6 +360,25 @@ __device__ __forceinline__ void traverse(const BvhView& t, const double* qlo, co
     }
 }
 
+// For queries over the tree's own primitive set (edges against edges): a
+// large query does not walk the tree; it meets only the large primitives.
+// Its pairs with the tree's primitives are reported from their side, through
+// their own loop over the large primitives, which therefore sees every large
+// primitive whatever the indices.  f(prim, fromLargeList).
+template <class F>
+__device__ __forceinline__ void traverse2(const BvhView& t, const double* qlo, const double* qhi, double gap, bool largeQuery, int* status, F f) {
+    if (t.nAll <= 0) return;
+    const int nb = *t.nbig, n = t.nAll - nb;
+    if (!largeQuery) {
+        auto g = [&](int p) { f(p, false); };
+        traverseTree(t, n, qlo, qhi, gap, status, g);
+    }
+    for (int b = 0; b < nb; ++b) {
+        const int p = (int)(t.keys[n + b] & 0xffffffffu);
+        if (overlaps(qlo, qhi, t.plo + 3 * p, t.phi + 3 * p, gap)) f(p, true);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Spatial-hash backend (the reference's SpatialHash, CollisionBroadPhase.cpp:
 // 11-763, as an A/B alternative to the LBVH): every primitive box is entered
@@ -373,6 +398,8 @@ constexpr long long HASH_MAX_QUERY = 4096;
 constexpr int HASH_BIAS = 1 << 20;  // cell coordinates are offset into [0, 2^21)
 
 struct HashView {
+    static constexpr bool kSplitsBig = false;
+    double bigExtent;
     int n, pairs;
     double inv;
     const uint64_t* key;
@@ -430,6 +457,11 @@ __device__ __forceinline__ void traverse(const HashView& t, const double* qlo, c
         const int p = t.big[b];
         if (overlaps(qlo, qhi, t.plo + 3 * p, t.phi + 3 * p, gap)) f(p);
     }
+}
+
+template <class F>
+__device__ __forceinline__ void traverse2(const HashView& t, const double* qlo, const double* qhi, double gap, bool, int* status, F f) {
+    traverse(t, qlo, qhi, gap, status, [&](int p) { f(p, false); });
 }
 
 __global__ void hashCountKernel(int n, const double* plo, const double* phi, double inv, int* count, int* bigFlag) {
@@ -512,19 +544,20 @@ __global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, 
 template <class View>
 __global__ void activeEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* rest, View tree, double sq,
                                double Hhat, Emit ccd, Emit eek, Emit moll, Emit ppe, int* status) {
-    CIPC_KERNEL_LOOP(eI, ne) {
-        int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
-        d3 p0 = ld3(x, e0), p1 = ld3(x, e1);
+    CIPC_KERNEL_LOOP(self, ne) {
         double lo[3], hi[3];
         boxInit(lo, hi);
-        boxAdd(lo, hi, p0); boxAdd(lo, hi, p1);
-        traverse(tree, lo, hi, sq, status, [&](int eJ) {
-            if (eJ <= eI) return;
+        boxAdd(lo, hi, ld3(x, edges[2 * self])); boxAdd(lo, hi, ld3(x, edges[2 * self + 1]));
+        const bool large = View::kSplitsBig && isLargeBox(lo, hi, tree.bigExtent);
+        // the pair (eI, eJ), eI < eJ, as the reference classifies it: eI's
+        // points first
+        auto pair = [&](int eI, int eJ) {
+            int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
             int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
             if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[g0]) && isCollider(btype[g1])) return;
             if (e0 == g0 || e0 == g1 || e1 == g0 || e1 == g1) return;
             ccd(((uint64_t)eI << 32) | (uint32_t)eJ, status);
-            d3 q0 = ld3(x, g0), q1 = ld3(x, g1);
+            d3 p0 = ld3(x, e0), p1 = ld3(x, e1), q0 = ld3(x, g0), q1 = ld3(x, g1);
             int t = dTypeEE(p0, p1, q0, q1);
             double cs = crossSqNormEE(p0, p1, q0, q1);
             double ex = 1e-3 * sqn(ld3(rest, e0) - ld3(rest, e1)) * sqn(ld3(rest, g0) - ld3(rest, g1));
@@ -546,6 +579,16 @@ __global__ void activeEEKernel(int ne, const int* edges, const int* btype, const
             if (mol) moll(((uint64_t)eI << 34) | ((uint64_t)eJ << 4) | (uint64_t)t, status);
             else if (t == 8) eek(((uint64_t)eI << 32) | (uint32_t)eJ, status);
             else ppe(ppeKey(c0, c1, c2), status);
+        };
+        traverse2(tree, lo, hi, sq, large, status, [&](int other, bool fromLarge) {
+            // a pair is handled once: by its lower index, except that a
+            // small edge handles its pairs with the large ones either way
+            if (!fromLarge || large) {
+                if (other > self) pair(self, other);
+            } else if (other != self) {
+                if (other > self) pair(self, other);
+                else pair(other, self);
+            }
         });
     }
 }
@@ -668,51 +711,89 @@ template <class View>
 __global__ void fullEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* dir, const double* treeBoxLo,
                              const double* treeBoxHi, double eeStepVal, const double* eeStepPtr, View tree, double eta, double* out, int* status) {
     const double eeStep = eeStepPtr ? *eeStepPtr : eeStepVal;
-    CIPC_KERNEL_LOOP(eJ, ne) {
-        int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
-        d3 q0 = ld3(x, g0), q1 = ld3(x, g1), dq0 = ld3(dir, g0), dq1 = ld3(dir, g1);
+    CIPC_KERNEL_LOOP(self, ne) {
         double qlo[3], qhi[3];
-        for (int k = 0; k < 3; ++k) { qlo[k] = treeBoxLo[3 * eJ + k]; qhi[k] = treeBoxHi[3 * eJ + k]; }
-        double blo[3], bhi[3];
-        boxInit(blo, bhi);
-        sweptAdd(blo, bhi, q0, dq0, eeStep);
-        sweptAdd(blo, bhi, q1, dq1, eeStep);
+        for (int k = 0; k < 3; ++k) { qlo[k] = treeBoxLo[3 * self + k]; qhi[k] = treeBoxHi[3 * self + k]; }
+        const bool large = View::kSplitsBig && isLargeBox(qlo, qhi, tree.bigExtent);
         double best = 1.0;
-        traverse(tree, qlo, qhi, 0.0, status, [&](int eI) {
-            if (eI <= eJ) return;
+        // the pair of query eJ and candidate eI > eJ as the reference forms it
+        // (Self_largestFeasibleStepSize_CCD): the swept boxes at the entry
+        // step must overlap, then the additive CCD with eI's points first
+        auto pair = [&](int eJ, int eI) {
+            int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
             int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
             if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[g0]) && isCollider(btype[g1])) return;
             if (e0 == g0 || e0 == g1 || e1 == g0 || e1 == g1) return;
+            d3 q0 = ld3(x, g0), q1 = ld3(x, g1), dq0 = ld3(dir, g0), dq1 = ld3(dir, g1);
             d3 p0 = ld3(x, e0), p1 = ld3(x, e1), dp0 = ld3(dir, e0), dp1 = ld3(dir, e1);
-            double clo[3], chi[3];
+            double blo[3], bhi[3], clo[3], chi[3];
+            boxInit(blo, bhi);
+            sweptAdd(blo, bhi, q0, dq0, eeStep);
+            sweptAdd(blo, bhi, q1, dq1, eeStep);
             boxInit(clo, chi);
             sweptAdd(clo, chi, p0, dp0, eeStep);
             sweptAdd(clo, chi, p1, dp1, eeStep);
             if (!overlaps(blo, bhi, clo, chi, 0.0)) return;
             double a = edgeEdgeCCD(p0, p1, q0, q1, -dp0, -dp1, -dq0, -dq1, eta, status);
             best = fmin(a, best);
+        };
+        traverse2(tree, qlo, qhi, 0.0, large, status, [&](int other, bool fromLarge) {
+            if (!fromLarge || large) {
+                if (other > self) pair(self, other);
+            } else if (other != self) {
+                if (other > self) pair(self, other);
+                else pair(other, self);
+            }
         });
-        out[eJ] = best;
+        out[self] = best;
     }
 }
 
+// The segment-triangle test of one (face, edge) pair (the filters of
+// checkEdgeTriIntersectionIfAny, IPCSolver.cpp:514-542).
+__device__ __forceinline__ bool faceEdgeHit(const int* faces, const int* edges, const int* btype, const double* x, int f, int e, double coplanarTol) {
+    int f0 = faces[3 * f], f1 = faces[3 * f + 1], f2 = faces[3 * f + 2];
+    int e0 = edges[2 * e], e1 = edges[2 * e + 1];
+    if (e0 == f0 || e0 == f1 || e0 == f2 || e1 == f0 || e1 == f1 || e1 == f2) return false;
+    if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return false;
+    return segTriIntersect(ld3(x, e0), ld3(x, e1), ld3(x, f0), ld3(x, f1), ld3(x, f2), coplanarTol);
+}
+
+// Faces against the edge tree.  A large face (one the face tree keeps out of
+// its tree) meets only the edge tree's large edges here; its pairs with the
+// other edges are tested by largeFaceKernel from the edges' side.
 template <class View>
 __global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, View tree, double coplanarTol,
                                 int* flag, int* status) {
     CIPC_KERNEL_LOOP(f, nsf) {
-        int f0 = faces[3 * f], f1 = faces[3 * f + 1], f2 = faces[3 * f + 2];
-        d3 a = ld3(x, f0), b = ld3(x, f1), c = ld3(x, f2);
         double lo[3], hi[3];
         boxInit(lo, hi);
-        boxAdd(lo, hi, a); boxAdd(lo, hi, b); boxAdd(lo, hi, c);
+        for (int k = 0; k < 3; ++k) boxAdd(lo, hi, ld3(x, faces[3 * f + k]));
+        const bool large = View::kSplitsBig && isLargeBox(lo, hi, tree.bigExtent);
         bool hit = false;
-        traverse(tree, lo, hi, 0.0, status, [&](int e) {
-            if (hit) return;
-            int e0 = edges[2 * e], e1 = edges[2 * e + 1];
-            if (e0 == f0 || e0 == f1 || e0 == f2 || e1 == f0 || e1 == f1 || e1 == f2) return;
-            if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
-            if (segTriIntersect(ld3(x, e0), ld3(x, e1), a, b, c, coplanarTol)) hit = true;
+        traverse2(tree, lo, hi, 0.0, large, status, [&](int e, bool) {
+            if (!hit && faceEdgeHit(faces, edges, btype, x, f, e, coplanarTol)) hit = true;
         });
+        if (hit) atomicOr(flag, 1);
+    }
+}
+
+// The edges that are not large (the edge tree's own) against the large faces
+// of the face tree (the last *nbig keys of its sorted order).
+__global__ void largeFaceKernel(int ne, const int* faces, const int* edges, const int* btype, const double* x, BvhView faceTree, BvhView edgeTree,
+                                double coplanarTol, int* flag) {
+    const int nbf = *faceTree.nbig;
+    if (nbf == 0) return;
+    const int nf = faceTree.nAll - nbf;
+    CIPC_KERNEL_LOOP(e, ne) {
+        const double* elo = edgeTree.plo + 3 * e;
+        const double* ehi = edgeTree.phi + 3 * e;
+        if (isLargeBox(elo, ehi, edgeTree.bigExtent)) continue;  // met by the large faces' own queries
+        bool hit = false;
+        for (int b = 0; b < nbf && !hit; ++b) {
+            const int f = (int)(faceTree.keys[nf + b] & 0xffffffffu);
+            if (overlaps(faceTree.plo + 3 * f, faceTree.phi + 3 * f, elo, ehi, 0.0) && faceEdgeHit(faces, edges, btype, x, f, e, coplanarTol)) hit = true;
+        }
         if (hit) atomicOr(flag, 1);
     }
 }
@@ -771,7 +852,7 @@ void buildBvh(Ctx& c, DevBvh& t, int n) {
     launch(sceneBoxFinalKernel, 1, 256, 0, c.s, nbBox, (const double*)t.boxPart, t.sceneBox);
     t.bigCount.reserve(1);
     CIPC_CUDA(cudaMemsetAsync(t.bigCount.p, 0, sizeof(int), c.s));
-    const double bigExtent = 0.1 * std::sqrt(c.P.bboxDiag2);
+    const double bigExtent = t.bigExtent = 0.1 * std::sqrt(c.P.bboxDiag2);
     launch(mortonKernel, blocksFor(n), TB, 0, c.s, n, t.primLo, t.primHi, t.sceneBox, bigExtent, t.keys, t.bigCount.p);
     // keys are (code << 32) | index (bit 62: kept out of the tree), written in
     // index order: a stable sort on bits 32-62 gives the order of a sort on
@@ -829,7 +910,7 @@ void buildHash(Ctx& c, DevBvh& t, int n) {
 }
 
 HashView hview(Ctx& c, const DevBvh& t) {
-    return HashView{t.n, t.hashPairs, 1.0 / c.P.avgEdge, t.hashKey, t.hashPrim, t.hashBig, c.counters.p + (&t == &c.edgeTree ? 14 : 11),
+    return HashView{t.bigExtent, t.n, t.hashPairs, 1.0 / c.P.avgEdge, t.hashKey, t.hashPrim, t.hashBig, c.counters.p + (&t == &c.edgeTree ? 14 : 11),
                     t.primLo, t.primHi};
 }
 
@@ -974,6 +1055,9 @@ bool isIntersected(Ctx& c) {
     if (c.nGround)
         launch(groundIntersectKernel, blocksFor(c.nGround), TB, 0, c.s, c.nGround, c.ground, c.x, c.P.groundN[0], c.P.groundN[1], c.P.groundN[2],
                                                                    c.P.groundD, c.counters.p + 7);
+    if (c.nse && c.nsf && c.broadPhase == CIPC_BROAD_PHASE_LBVH)
+        launch(largeFaceKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.faces, c.edges, c.btype, c.x, view(c.faceTree), view(c.edgeTree), c.coplanarTol,
+               c.counters.p + 7);
     if (c.nsf) withView(c, c.edgeTree, [&](auto v) { launch(intersectKernel<decltype(v)>, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, v, c.coplanarTol, c.counters.p + 7,
                             c.status); });
     int f = 0, st = 0;

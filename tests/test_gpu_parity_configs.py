@@ -79,14 +79,16 @@ def test_two_cubes_8_cells_100_steps(oracle_mod):
     o = oracle_mod.Oracle(sc, linear="multifrontal", threads=THREADS)
     g = cipc.Simulator(sc, surface=o.surface(), tol=1e-10)
     bb = np.sqrt(o.scalars()["bboxDiag2"])
-    worst = 0.0
+    log = []
     for s in range(100):
-        o.step(); g.step()
-        if (s + 1) % 10 == 0:
-            err = np.abs(o.get("x") - g.get("x")).max() / bb
-            worst = max(worst, err)
-            assert err <= TRAJ_TOL, (s + 1, err)
-    print(f"two cubes 8^3, 100 steps: worst trajectory error {worst:.2e} x bbox")
+        so, sg = o.step(), g.step()
+        err = np.abs(o.get("x") - g.get("x")).max() / bb
+        log.append((s + 1, so["newton"], sg["newtonIterations"], so["selfContacts"] + so["groundContacts"], err))
+    print("step, Newton (oracle, GPU), contacts, trajectory error / bbox:")
+    for row in log:
+        print("  %3d %3d %3d %5d %.3e" % row)
+    worst = max(r[4] for r in log[9::10])
+    assert worst <= TRAJ_TOL, [r for r in log if r[4] > TRAJ_TOL][:5]
 
 
 CONTACT_STATES = {

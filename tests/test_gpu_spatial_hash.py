@@ -14,8 +14,8 @@ def _canon(S):
 
 
 @pytest.mark.parametrize("make,steps", [
-    (lambda: cipc.scene_cloth_drape(10, 2), 25),
-    (lambda: cipc.scene_pile(4, 2, seed=3), 20),
+    (lambda: cipc.scene_cloth_drape(10, 2), 60),
+    (lambda: cipc.scene_pile(4, 2, seed=3), 45),
     (lambda: cipc.scene_two_cubes(3, gap=0.002), 10),
 ])
 def test_same_trajectory_as_lbvh(oracle_mod, make, steps):
