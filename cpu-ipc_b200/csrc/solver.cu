@@ -19,6 +19,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -238,11 +239,29 @@ bool lineSearch(Ctx& c, double& alpha, double kappa, cipc_step_stats& st, Energy
 }
 
 // Assembly stage: gradient into c.grad, Hessian into the static + contact BSR.
+// CIPC_DEBUG_TIMING=1: the assembly's parts timed on the host (with a
+// synchronisation after each) and printed to stderr.
+static bool debugTiming() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_DEBUG_TIMING"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+
 int assembleAll(Ctx& c) {
+    const bool dbg = debugTiming();
+    auto t0 = Clock::now();
     assembleElastic(c);
+    if (dbg) sync(c);
+    auto t1 = Clock::now();
     int coll = contactAssemble(c);
+    if (dbg) sync(c);
+    auto t2 = Clock::now();
     gatherGradient(c);
     checkStatus(c, "assembly");
+    auto t3 = Clock::now();
+    if (dbg)
+        std::fprintf(stderr, "[assembly] elastic %.3f ms, contact %.3f ms (%d self, %d mollified, %d friction), gradient+status %.3f ms\n", ms(t0, t1),
+                     ms(t1, t2), c.nSelf, c.nMoll, c.nFric, ms(t2, t3));
     c.assembled = true;
     return coll;
 }
