@@ -108,6 +108,7 @@ struct Ctx {
     // a tensor-core completion wait timed out: the network's forward pass is
     // refused for the rest of the context's life
     bool tcFault = false;
+    long long hostSyncs = 0;  // host waits on the context's stream (hostSync)
     DBuf<double> stepScal;  // device scalars of the chained step bounds
     // hook at the linear-solve seam (NewtonLinearSystem::solve): Adam
     // iterations of the network on every assembled Newton system, and/or a
@@ -251,6 +252,13 @@ inline void profEnd(Ctx& c, int kind) {
 }
 
 // ---- launchers (elastic.cu) ----
+// The host waits for the context's stream (counted: the host round trips of
+// the Newton driver).
+inline void hostSync(Ctx& c) {
+    ++c.hostSyncs;
+    CIPC_CUDA(cudaStreamSynchronize(c.s));
+}
+
 void buildStaticPattern(Ctx& c, const std::vector<int>& tets, const std::vector<int>& tris, const std::vector<int>& bendV);
 void assembleElastic(Ctx& c);          // vtxGrad, diagExtra, element blocks, static BSR values, element gradient
 void tetGradient(Ctx& c);              // elemG of the tetrahedra only (no Hessian)

@@ -886,7 +886,7 @@ void buildHash(Ctx& c, DevBvh& t, int n) {
     int last[2];
     CIPC_CUDA(cudaMemcpyAsync(&last[0], t.hashOffset.p + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaMemcpyAsync(&last[1], t.hashCount.p + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     const int pairs = last[0] + last[1];
     t.hashPairs = pairs;
     t.hashKey.reserve(std::max(1, pairs)); t.hashKeyAlt.reserve(std::max(1, pairs));
@@ -957,7 +957,7 @@ void groundActiveSet(Ctx& c) {
     groundActiveSetLaunch(c);
     int n = 0;
     CIPC_CUDA(cudaMemcpyAsync(&n, c.counters.p + 15, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     c.nGround = n;
 }
 
@@ -990,7 +990,7 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             CIPC_CUDA(cudaGetLastError());
             CIPC_CUDA(cudaMemcpyAsync(cnt, c.counters.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
             CIPC_CUDA(cudaMemcpyAsync(&stWord, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-            CIPC_CUDA(cudaStreamSynchronize(c.s));
+            hostSync(c);
             fits = true;
             for (int k = 0; k < 6; ++k)
                 if (cnt[k] > caps[k]) { caps[k] = cnt[k] + cnt[k] / 2 + 1024; fits = false; }
@@ -1030,7 +1030,7 @@ void buildCollisionSets(Ctx& c, bool rehash) {
         {
             int h[10];
             CIPC_CUDA(cudaMemcpyAsync(h, c.counters.p + 6, 10 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
-            CIPC_CUDA(cudaStreamSynchronize(c.s));
+            hostSync(c);
             nu = h[0];
             c.nGround = h[9];
         }
@@ -1063,7 +1063,7 @@ bool isIntersected(Ctx& c) {
     int f = 0, st = 0;
     CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     if (st) checkStatus(c, "intersection test");
     return f != 0;
 }
@@ -1211,7 +1211,7 @@ double stepBoundsDevice(Ctx& c) {
     CIPC_CUDA(cudaGetLastError());
     double h[9];
     CIPC_CUDA(cudaMemcpyAsync(h, s, sizeof(h), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     if (h[8] != 0.0) checkStatus(c, "step bounds");
     return h[7];
 }

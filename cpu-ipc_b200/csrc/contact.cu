@@ -669,7 +669,7 @@ void finalizeDynamic(Ctx& c) {
         CIPC_CUDA(cub::DeviceScan::ExclusiveSum(c.sortTmp.p, b2, c.counts.p, c.runs.p, nh + 1, c.s));
         int nu = 0;
         CIPC_CUDA(cudaMemcpyAsync(&nu, c.runs.p + nh, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        hostSync(c);
         c.nDynB = nu;
         if (nu > 0) {
             c.dynCol.reserve(nu); c.dynSrcStart.reserve(nu);
@@ -679,7 +679,7 @@ void finalizeDynamic(Ctx& c) {
             launch(validCountKernel, 1, 1, 0, c.s, nh, c.dynHKeyAlt, c.counters.p + 9);
             int nValid = 0;
             CIPC_CUDA(cudaMemcpyAsync(&nValid, c.counters.p + 9, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-            CIPC_CUDA(cudaStreamSynchronize(c.s));
+            hostSync(c);
             if (c.mixed) {
                 c.dynBF.reserve((size_t)9 * nu);
                 launch(dynReduceKernel<float>, blocksFor(nu), TB, 0, c.s, nu, nValid, c.dynSrcStart, c.dynHIdx, c.dynHValF, c.dynBF);
@@ -868,7 +868,7 @@ void closeConstraintCheck(Ctx& c, bool& update) {
                                                                        P.groundN[0], P.groundN[1], P.groundN[2], P.groundD, c.counters.p + 8);
     int f = 0;
     CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 8, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     update = f != 0;
 }
 

@@ -803,7 +803,7 @@ void mpnnSetWeights(Ctx& c, const float* w, int n) {
     zeroF(c, c.mpV.p, MP_NPARAM);
     zeroF(c, c.mpG.p, MP_NPARAM);
     launch(toBf16Kernel, blocksFor(MP_NPARAM), TB, 0, c.s, MP_NPARAM, (const float*)c.mpW.p, reinterpret_cast<bf16*>(c.mpWb.p));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     c.mpStep = 0;
     c.mpReady = true;
     c.mpFactorReady = false;
@@ -812,13 +812,13 @@ void mpnnSetWeights(Ctx& c, const float* w, int n) {
 void mpnnGetWeights(Ctx& c, float* w) {
     if (!c.mpReady) throw InvalidArgument("no network weights set");
     CIPC_CUDA(cudaMemcpyAsync(w, c.mpW.p, sizeof(float) * MP_NPARAM, cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
 }
 
 void mpnnGetGrad(Ctx& c, float* g) {
     if (!c.mpReady) throw InvalidArgument("no network weights set");
     CIPC_CUDA(cudaMemcpyAsync(g, c.mpG.p, sizeof(float) * MP_NPARAM, cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
 }
 
 // Flat list of the lower edges of a row-ranged pattern: three arrays of
@@ -836,7 +836,7 @@ static int buildLowerList(Ctx& c, const int* rowS, const int* rowE, const int* c
     CIPC_CUDA(cub::DeviceScan::ExclusiveSum(c.mpScanTmp.p, bytes, cnt, off, nv + 1, c.s));
     int n = 0;
     CIPC_CUDA(cudaMemcpyAsync(&n, off + nv, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     out.reserve(3 * (size_t)std::max(n, 1));
     if (n > 0) launch(lowerFillKernel, blocksFor(nv), TB, 0, c.s, nv, rowS, rowE, col, (const int*)off, out.p, out.p + n, out.p + 2 * (size_t)n);
     return n;
@@ -978,7 +978,7 @@ static double lossT(Ctx& c, const MT* val, const MT* dval, int nprobes, const fl
                (const double*)c.diagExtra.p, (const double*)c.mpS.p, (const float*)u, vv);
         launch(probeDotsKernel, nb, 256, 0, c.s, n3, (const float*)u, (const float*)vv, (const float*)w, c.red.p);
         CIPC_CUDA(cudaMemcpyAsync(part.data(), c.red.p, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, c.s));
-        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        hostSync(c);
         double uv = 0, ww = 0;
         for (int k = 0; k < nb; ++k) { uv += part[2 * k]; ww += part[2 * k + 1]; }
         if (!(ww > 0)) throw InvalidArgument("probe vector is zero");
@@ -995,7 +995,7 @@ static double lossT(Ctx& c, const MT* val, const MT* dval, int nprobes, const fl
     int nb2 = std::min(1024, std::max(1, (nv + 255) / 256));
     launch(logDiagKernel, nb2, 256, 0, c.s, nv, (const int*)c.diagSlot.p, (const float*)c.mpGS.p, c.red.p);
     CIPC_CUDA(cudaMemcpyAsync(part.data(), c.red.p, sizeof(double) * nb2, cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     double logDiag = 0;
     for (int k = 0; k < nb2; ++k) logDiag += part[k];
     if (!(T > 0) || !std::isfinite(T) || !std::isfinite(logDiag)) throw std::runtime_error("learned preconditioner loss is not finite");

@@ -1304,7 +1304,7 @@ static int runPcg(Ctx& c, const MT* val, const MT* dval, const VT* b, VT* x, VT*
         CIPC_CUDA(cudaGetLastError());
         CIPC_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, c.s));
         CIPC_CUDA(cudaMemcpyAsync(hs, c.scal.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
-        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        hostSync(c);
         it = (int)hs[4];
         if (hflag) break;
     }
@@ -1480,7 +1480,7 @@ static int runPcgPersistent(Ctx& c, const MT* val, const MT* dval, const VT* b, 
     double hs[8];
     CIPC_CUDA(cudaMemcpyAsync(&hflag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     CIPC_CUDA(cudaMemcpyAsync(hs, c.scal.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     if (hflag == 3) throw std::runtime_error("device status in PCG: grid barrier timed out");
     flagOut = hflag;
     relRes = hs[6] > 0 ? std::sqrt(hs[3] / hs[6]) : 0.0;

@@ -85,7 +85,7 @@ __global__ void motionKernel(int n, const int* idx, const double* x, const doubl
 using Clock = std::chrono::steady_clock;
 double ms(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); }
 
-void sync(Ctx& c) { CIPC_CUDA(cudaStreamSynchronize(c.s)); }
+void sync(Ctx& c) { hostSync(c); }
 
 void stepForward(Ctx& c, const double* x0, const double* d, double alpha, bool all = false) {
     launch(stepForwardKernel, blocksFor(c.nv), TB, 0, c.s, c.nv, x0, d, c.btype, alpha, all ? 1 : 0, c.x);
@@ -695,7 +695,7 @@ static DBuf<double>* stateBuf(Ctx& c, int which) {
 int cipc_gpu_get_state(cipc_gpu_context* h, int which, double* out) {
     return guarded(h, [&](Ctx& c) {
         if (!out) throw InvalidArgument("null output");
-        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        hostSync(c);
         CIPC_CUDA(cudaMemcpy(out, stateBuf(c, which)->p, sizeof(double) * 3 * c.nv, cudaMemcpyDeviceToHost));
     });
 }
@@ -704,7 +704,7 @@ int cipc_gpu_set_state(cipc_gpu_context* h, int which, const double* in) {
     return guarded(h, [&](Ctx& c) {
         if (!in) throw InvalidArgument("null input");
         if (which == 4) throw InvalidArgument("rest positions are fixed at creation");
-        CIPC_CUDA(cudaStreamSynchronize(c.s));
+        hostSync(c);
         CIPC_CUDA(cudaMemcpy(stateBuf(c, which)->p, in, sizeof(double) * 3 * c.nv, cudaMemcpyHostToDevice));
     });
 }

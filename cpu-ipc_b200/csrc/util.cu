@@ -68,7 +68,7 @@ double reduce(Ctx& c, const double* a, const double* b, int n) {
     launch(finalKernel<OPC>, 1, RB, 0, c.s, c.scratch.p + 8, nb, c.scratch.p);
     double h;
     CIPC_CUDA(cudaMemcpyAsync(&h, c.scratch.p, sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     return h;
 }
 }  // namespace
@@ -108,7 +108,7 @@ void deviceMaxTo(Ctx& c, const double* v, int n, double* dst) {
 
 void fetchSums(Ctx& c, double* h, int nslots) {
     CIPC_CUDA(cudaMemcpyAsync(h, c.sums.p, sizeof(double) * nslots, cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
 }
 double deviceMax(Ctx& c, const double* v, int n) { return reduce<1>(c, v, nullptr, n); }
 double deviceMin(Ctx& c, const double* v, int n, double init) { return std::min(init, reduce<2>(c, v, nullptr, n)); }
@@ -122,7 +122,7 @@ double deviceInfNorm(Ctx& c, const double* v, int n) {
 void checkStatus(Ctx& c, const char* stage) {
     int st = 0;
     CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaStreamSynchronize(c.s));
+    hostSync(c);
     if (st) {
         CIPC_CUDA(cudaMemsetAsync(c.status.p, 0, sizeof(int), c.s));
         std::string msg = std::string("device status in ") + stage + ":";
