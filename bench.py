@@ -329,6 +329,7 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
     if kind:
         sim.profile(kind, capacity=200000)
     launches0 = cipc.kernel_launches()
+    syncs0 = sim.host_syncs()
     total_ms = 0.0
     newton = pcg = 0
     stages = {k: 0.0 for k in STAGES}
@@ -344,10 +345,11 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
             stages[k] += st[k]
         ndyn.append(sim.counts()[8])
     launches = cipc.kernel_launches() - launches0
+    syncs = sim.host_syncs() - syncs0
     nprof, prof_ms = sim.profile_read() if kind else (0, 0.0)
     if kind:
         sim.profile(0)
-    return dict(ms=total_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches,
+    return dict(ms=total_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches, syncs=syncs,
                 stages={k: v / max(1, steps) for k, v in stages.items()})
 
 
@@ -471,6 +473,8 @@ def main():
                "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
                "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
                "ms_per_newton_iteration": max_ms / max(1, r["newton"]),
+               "host_syncs_per_newton_iteration": r["syncs"] / max(1, r["newton"]),
+               "kernel_launches_per_newton_iteration": r["launches"] / max(1, r["newton"]),
                "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
                "vertices": nv, "static_blocks": counts[7], "contact_blocks_mean": counts[8]}
         cfg["stage_ms_per_step"] = {k.replace("Milliseconds", ""): round(v, 3) for k, v in r["stages"].items()}

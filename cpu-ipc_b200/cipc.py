@@ -90,6 +90,7 @@ def lib():
         L.cipc_gpu_set_online_training.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_ulonglong]
         L.cipc_gpu_set_system_dump.argtypes = [vp, C.c_char_p]
         L.cipc_gpu_hook_systems.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.cipc_gpu_host_syncs.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.cipc_gpu_get_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.cipc_gpu_get_surface.argtypes = [vp, _ip, _ip, _ip]
         L.cipc_gpu_build_collision_sets.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -131,7 +132,7 @@ EXPORTED_SYMBOLS = [
     "cipc_gpu_kernel_launches", "cipc_gpu_pcg_bsr_noalloc", "cipc_gpu_export_bsr", "cipc_gpu_precond_num_params",
     "cipc_gpu_precond_set_weights", "cipc_gpu_precond_get_weights", "cipc_gpu_precond_loss", "cipc_gpu_precond_train",
     "cipc_gpu_precond_stats", "cipc_gpu_precond_factor", "cipc_gpu_set_online_training", "cipc_gpu_set_system_dump",
-    "cipc_gpu_hook_systems",
+    "cipc_gpu_hook_systems", "cipc_gpu_host_syncs",
 ]
 NOALLOC_MAX_ROWS = 32768
 
@@ -297,6 +298,12 @@ class Simulator:
     def set_system_dump(self, directory):
         """Write every Newton system to `directory` (None turns it off)."""
         self._chk(self.L.cipc_gpu_set_system_dump(self.h, None if directory is None else str(directory).encode()))
+
+    def host_syncs(self):
+        """Host waits on the context's stream since creation."""
+        n = C.c_longlong(0)
+        self._chk(self.L.cipc_gpu_host_syncs(self.h, C.byref(n)))
+        return n.value
 
     def hook_systems(self):
         n = C.c_longlong(0)

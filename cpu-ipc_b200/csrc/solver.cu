@@ -1028,6 +1028,10 @@ int cipc_gpu_set_system_dump(cipc_gpu_context* h, const char* directory) {
     return guarded(h, [&](Ctx& c) { c.dumpDir = directory ? directory : ""; });
 }
 
+int cipc_gpu_host_syncs(cipc_gpu_context* h, long long* count) {
+    return guarded(h, [&](Ctx& c) { *count = c.hostSyncs; });
+}
+
 int cipc_gpu_hook_systems(cipc_gpu_context* h, long long* count) {
     return guarded(h, [&](Ctx& c) { *count = c.hookSystems; });
 }

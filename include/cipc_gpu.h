@@ -230,6 +230,9 @@ int cipc_gpu_set_online_training(cipc_gpu_context* ctx, int iterations, int prob
  * diagonal extras, right-hand side, positions; int32 boundary types).  NULL
  * or "" turns it off. */
 int cipc_gpu_set_system_dump(cipc_gpu_context* ctx, const char* directory);
+/* Times the host has waited for the context's stream since creation (the
+ * Newton driver's host round trips; no counterpart in the reference). */
+int cipc_gpu_host_syncs(cipc_gpu_context* ctx, long long* count);
 /* Newton systems the hook has trained on or written since creation. */
 int cipc_gpu_hook_systems(cipc_gpu_context* ctx, long long* count);
 
