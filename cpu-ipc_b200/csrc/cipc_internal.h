@@ -48,10 +48,13 @@ template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t cap = 0;
+    // grows to twice the request: buffers sized by contact counts grow for a
+    // few steps and then stay (a reallocation costs a device-wide wait and
+    // page mapping, tens of milliseconds for the pile's contact buffers)
     void reserve(size_t n) {
         if (n <= cap) return;
         if (p) cudaFree(p);
-        size_t c = n < 64 ? 64 : n + n / 4;
+        size_t c = n < 64 ? 64 : 2 * n;
         CIPC_CUDA(cudaMalloc(&p, c * sizeof(T)));
         cap = c;
     }
