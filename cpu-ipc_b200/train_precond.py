@@ -8,10 +8,11 @@ the same pattern, at PCG relative residual 1e-6 (the FP64 true residual).
 
 Training streams the systems through the network as they arise: each train
 seed's pile runs --train-steps steps in mixed precision with the learned
-factor, and every Newton system, at the linear-solve seam, takes
---adam-iters Adam steps of the loss before it is solved (the systems stay on
-the GPU; nothing is written to disk).  The weights carry over from seed to
-seed.
+factor, and from step --train-from on every Newton system, at the
+linear-solve seam, takes --adam-iters Adam steps of the loss before it is
+solved (the systems stay on the GPU; nothing is written to disk).  The
+weights carry over from seed to seed; --init-weights starts from a previous
+run's.
 
 Evaluation: each test seed's pile settles --settle steps in FP64, then the
 same state is restored into every variant (FP64 block-Jacobi, mixed
@@ -46,6 +47,7 @@ def parse(argv=None):
     ap.add_argument("--train-seeds", default="0:50")
     ap.add_argument("--test-seeds", default="50:60")
     ap.add_argument("--train-steps", type=int, default=25)
+    ap.add_argument("--train-from", type=int, default=0, help="steps of each train seed run before its systems train the network")
     ap.add_argument("--adam-iters", type=int, default=4)
     ap.add_argument("--probes", type=int, default=4)
     ap.add_argument("--lr", type=float, default=2e-3)
@@ -66,8 +68,9 @@ def train(args, log):
         sim = cipc.Simulator(cipc.scene_pile(args.cubes, args.cells, seed=seed), precision="mixed", precond="learned")
         if w is not None:
             sim.set_precond_weights(w)
-        sim.set_online_training(args.adam_iters, args.probes, args.lr, 7919 * seed + 1)
-        for _ in range(args.train_steps):
+        for k in range(args.train_steps):
+            if k == args.train_from:
+                sim.set_online_training(args.adam_iters, args.probes, args.lr, 7919 * seed + 1)
             sim.step()
         n = sim.hook_systems()
         systems += n
