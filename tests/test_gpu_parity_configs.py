@@ -19,7 +19,8 @@ two solvers each stopped at 1e-6.
   the learned factor (weights trained on the restored system, then frozen),
   within 1e-6 of the bounding-box diagonal.
 * A twisted cylinder of 8 x 32 x 64 layers (92,160 tets, animated Dirichlet
-  caps): ten steps of trajectory.
+  caps): ten steps of trajectory; and at configuration 5's size (1,011,840
+  tets) the gradient, Newton matrix and energy of a perturbed state.
 * Additive CCD candidate by candidate: every partial-CCD candidate pair of
   the cloth contact state, and random near-contact pairs, against the
   oracle's time of impact (within 1e-6 relative, never larger).
@@ -240,3 +241,29 @@ def test_ccd_time_of_impact_per_candidate(oracle_mod):
     P = rng.standard_normal((n, 4, 3)) * scale
     D = rng.standard_normal((n, 4, 3)) * scale * 2
     _check_toi(oracle_mod, kinds, P, D)
+
+
+def test_twist_configuration_size_system(oracle_mod):
+    """The twisted cylinder at configuration 5's size (16 radial x 64
+    angular x 170 axial layers, wedge-split: 1,011,840 tets, 175,275
+    vertices): gradient, Newton matrix and energy of a perturbed state with
+    velocities, against the oracle."""
+    sc = cipc.scene_twist(16, 64, 170)
+    assert len(sc["tets"]) == 1011840
+    o = oracle_mod.Oracle(sc, linear="multifrontal", threads=THREADS)
+    g = cipc.Simulator(sc, surface=o.surface())
+    rng = np.random.default_rng(12)
+    free = (sc["btype"] == 0)[:, None]
+    x = o.get("x") + 2e-3 * rng.standard_normal((o.nv, 3)) * free
+    v = 0.2 * rng.standard_normal((o.nv, 3)) * free
+    dt = sc["params"]["dt"]
+    for f, a in (("x", x), ("vel", v), ("xtilde", o.get("vprev") + v * dt)):
+        o.set(f, a); g.set(f, a)
+    go, rp, col, val, rhs = o.system()
+    gg, _ = g.assemble()
+    assert np.abs(go - gg).max() <= GRAD_TOL * np.abs(go).max()
+    Ao = _oracle_full_matrix(rp, col, val, 3 * o.nv)
+    Ag = _gpu_full_matrix(g, sc["btype"])
+    assert abs(Ao - Ag).max() <= HESS_TOL * abs(Ao).max()
+    assert abs(o.energy(0.0) - g.energy(0.0)) <= ENERGY_TOL * abs(o.energy(0.0))
+    g.close()
