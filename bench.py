@@ -29,6 +29,8 @@ cloth has reached the cube), so the timed steps are in contact.  The same
 run also times the plain FP64 block-Jacobi GPU path on the same frames.
 Multi-GPU: replicas only (one independent simulation per rank, weak scaling).
 
+--scene twist measures the large twist (configuration 5: 1,011,840 tets,
+both caps rotated through animated Dirichlet conditions) from its first step.
 --scene cloth_drape measures the cloth-drape configuration instead: a
 128x128-vertex 1 m cloth (32,258 triangles, Baraff-Witkin membrane +
 quadratic bending, friction 0.3) 0.1 m above a fixed 0.5 m tetrahedral cube
@@ -65,7 +67,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="pile", choices=["cloth_drape", "pile"])
+    ap.add_argument("--scene", default="pile", choices=["cloth_drape", "pile", "twist"])
     ap.add_argument("--cloth", type=int, default=128)
     ap.add_argument("--pile-cubes", type=int, default=64)
     ap.add_argument("--pile-cells", type=int, default=12)
@@ -82,7 +84,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     a = ap.parse_args()
     if a.settle_steps is None:
-        a.settle_steps = 30 if a.scene == "pile" else 40
+        a.settle_steps = {"pile": 30, "cloth_drape": 40, "twist": 0}[a.scene]
     if a.train_steps is None:
         a.train_steps = a.settle_steps
     return a
@@ -91,6 +93,8 @@ def parse():
 def make_scene(args, cipc):
     if args.scene == "pile":
         return cipc.scene_pile(args.pile_cubes, args.pile_cells)
+    if args.scene == "twist":
+        return cipc.scene_twist(16, 64, 170)
     return cipc.scene_cloth_drape(args.cloth, 10)
 
 
@@ -98,10 +102,16 @@ def workload(args):
     """Name of the measured workload (the same string on both arms)."""
     if args.scene == "pile":
         return f"pile_{args.pile_cubes}x{args.pile_cells}"
+    if args.scene == "twist":
+        return "twist_16x64x170"
     return f"cloth_drape_{args.cloth}"
 
 
 def describe(args):
+    if args.scene == "twist":
+        return ("cylinder of radius 0.1 m and length 1 m, 16 radial x 64 angular x 170 axial layers, wedge-split (1,011,840 tets, "
+                "175,275 vertices), both end caps Dirichlet-rotated opposite ways at 2 pi rad/s, no gravity; Neo-Hookean E=1e5, nu=0.45, "
+                "friction 0.1, dt=0.01, relative dhat 1e-3")
     if args.scene == "pile":
         n, c = args.pile_cubes, args.pile_cells
         return (f"{n} cubes of 0.2 m ({c}^3 cells x 6 tets each, {n * 6 * c ** 3} tets, {n * (c + 1) ** 3} vertices) "
