@@ -14,6 +14,7 @@
 // CPU IPC/Friction.cpp:81-545; computeEnergy barrier part IPCSolver.cpp:398-451.
 #include "cipc_internal.h"
 #include "distance_derivs.cuh"
+#include "distance_rows.cuh"
 #include "geometry.cuh"
 
 #include <cub/cub.cuh>
@@ -84,6 +85,22 @@ __device__ void distDerivs(int kind, const d3* p, double* g, double* H) {
     }
 }
 
+// Row r of the Hessian of the squared distance (the warp's lanes form the
+// rows of one contact side by side); n = 3 * points entries.
+__device__ void distHessRow(int kind, const d3* p, int r, double* out) {
+    double v[12];
+    int np = npts(kind);
+    for (int k = 0; k < np; ++k) { v[3 * k] = p[k].x; v[3 * k + 1] = p[k].y; v[3 * k + 2] = p[k].z; }
+    switch (kind) {
+    case 0:
+        for (int j = 0; j < 6; ++j) out[j] = j == r ? 2.0 : ((j == r + 3 || j + 3 == r) ? -2.0 : 0.0);
+        return;
+    case 1: Hrow_PE<double>(v, r, out); return;
+    case 2: Hrow_PT<double>(v, r, out); return;
+    default: Hrow_EE<double>(v, r, out); return;
+    }
+}
+
 struct DynOut {
     int* gKey;
     double* gVal;
@@ -125,21 +142,23 @@ __global__ void selfBarrierKernel(int n, const int* active, const double* x, con
         int np = npts(kind), nd = 3 * np;
         int ne = nd == 9 ? 10 : nd;
         double cf, ca = 0.0, cb = 0.0;
+        d3 p[4];
+        for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
         if (lane == 0) {
-            d3 p[4];
-            for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
             double d = distVal(kind, p);
             double gb, hb;
             barrierG(d, Hhat, gb);
             barrierH(d, Hhat, hb);
             cf = (kind <= 1) ? kappa * -active[4 * i + 3] : kappa;
             double* g = S.W;
-            distDerivs(kind, p, g, withHessian ? S.B : nullptr);
+            distDerivs(kind, p, g, nullptr);
             for (int k = 0; k < nd; ++k) S.V[k] = cf * gb * g[k];
             if (!isfinite(d)) raiseStatus(status, CIPC_ST_NONFINITE);
             ca = cf * hb;
             cb = cf * gb;
         }
+        // the distance Hessian, one row per lane
+        if (withHessian && lane < nd) distHessRow(kind, p, lane, S.B + lane * nd);
         __syncwarp();
         if (withHessian) {
             // kappa (b'' g g^T + b' H), the warp's lanes over the entries
