@@ -449,10 +449,11 @@ def main():
     dt = scene["params"]["dt"]
     gdt2 = np.array([0.0, -9.8 * dt * dt, 0.0])
     t0 = time.perf_counter()
+    lib_ms = 0.0
     for _ in range(e2e_steps):
         for k in ("x", "vel", "vprev", "xtilde"):
             twin.set(k, pins[k])
-        twin.step()
+        lib_ms += twin.step()["stepMilliseconds"]
         pins["x"][:] = twin.get("x")
         pins["vel"][:] = twin.get("vel")
         # host-side state of the next step (updateInertialTarget)
@@ -506,7 +507,8 @@ def main():
             "data": "synthetic",
             "config": cfg,
             "roofline": roof,
-            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 4 * 24 * nv, "d2h_bytes_per_step": 2 * 24 * nv},
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 4 * 24 * nv, "d2h_bytes_per_step": 2 * 24 * nv,
+                    "steps": e2e_steps, "library_step_ms": lib_ms / e2e_steps, "wall_ms_per_step": 1000 * e2e_s / e2e_steps},
             "gpu_launches": int(r["launches"]),
             "clocks": clocks,
         }
