@@ -975,8 +975,10 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
     return true;
 }
 
-template <class MT, class VT, bool LEARNED, bool CACHED>
-__global__ void __launch_bounds__(PB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
+// MINB: blocks per SM the compiler must fit (registers); 3 for the
+// streaming variant that trades a few spills for 48 resident warps
+template <class MT, class VT, bool LEARNED, bool CACHED, int MINB = 1>
+__global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     extern __shared__ __align__(16) unsigned char pipeSmem[];
     // In a single-pass launch (CACHED) the block's matrix rows and its rows'
     // recurrence vectors live in shared memory: only the gathered vectors
@@ -1334,6 +1336,13 @@ static bool pcgClassic() {
     return v == 1;
 }
 
+// CIPC_PCG_OCC3=1 runs the streaming kernel's three-blocks-per-SM build.
+static bool pcgOcc3() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_PCG_OCC3"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+
 // CIPC_PCG_NOPACK=1 keeps the streaming kernel on the slot-aligned FP32 factor.
 static bool pcgNoPack() {
     static int v = -1;
@@ -1417,11 +1426,13 @@ static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool class
     }
     a.sliceMax = 0;
     a.rowsPerBlock = 0;
-    const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false>;
+    const bool occ3 = !classic && pcgOcc3();
+    const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED>
+                             : (occ3 ? (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false, 3> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false>);
     int perSM = 0;
     CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, 0));
     if (perSM < 1) throw std::runtime_error("persistent PCG kernel does not fit on an SM");
-    int grid = std::max(1, std::min(std::min(std::min(perSM, pcgBlocksPerSm()) * smCount, needed), cap));
+    int grid = std::max(1, std::min(std::min(std::min(perSM, occ3 ? 3 : pcgBlocksPerSm()) * smCount, needed), cap));
     ++g_kernelLaunches;
     CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PB), args, 0, c.s));
 }
