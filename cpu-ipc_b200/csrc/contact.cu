@@ -167,11 +167,11 @@ __global__ void selfBarrierKernel(int n, const int* active, const double* x, con
             const double* g = S.W;
             for (int e = lane; e < ne * ne; e += 32) {
                 const int r = e / ne, q = e - r * ne;
-                // the rows came from different lanes: (r, q) and (q, r) both
-                // take the upper-triangle entry, so the matrix the eigen-solver
-                // gets is exactly symmetric
-                const double h = r <= q ? S.B[r * nd + q] : S.B[q * nd + r];
-                S.A[e] = (r < nd && q < nd) ? (ca * g[r]) * g[q] + cb * h : 0.0;
+                // the rows came from different lanes: (r, q) and (q, r) are
+                // both formed from the upper-triangle entry, so the matrix the
+                // eigen-solver gets is exactly symmetric
+                const int lo = r <= q ? r : q, hi = r <= q ? q : r;
+                S.A[e] = (hi < nd) ? (ca * g[lo]) * g[hi] + cb * S.B[lo * nd + hi] : 0.0;
             }
             __syncwarp();
         }
