@@ -469,19 +469,8 @@ __device__ __forceinline__ void groupReduce3(VT acc[3]) {
 // acc += (A u)_row over the row's static and contact blocks (lane-strided)
 template <class MT, class VT>
 __device__ __forceinline__ void rowSpmv(const PcgArgs<MT, VT>& a, int row, int lane, const VT* u, VT acc[3]) {
-    // two slots per pass, their loads issued before either product (more
-    // loads in flight; the sums keep the slot order)
-    const int end = a.rowPtr[row + 1];
-    int k = a.rowPtr[row] + lane;
-    for (; k + GROUP < end; k += 2 * GROUP) {
-        const int c0 = a.col[k], c1 = a.col[k + GROUP];
-        VT x0[3] = {u[3 * c0], u[3 * c0 + 1], u[3 * c0 + 2]};
-        VT x1[3] = {u[3 * c1], u[3 * c1 + 1], u[3 * c1 + 2]};
-        blockMulAdd(a.val + (size_t)9 * k, x0, acc);
-        blockMulAdd(a.val + (size_t)9 * (k + GROUP), x1, acc);
-    }
-    if (k < end) {
-        const int c = a.col[k];
+    for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
+        int c = a.col[k];
         VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
         blockMulAdd(a.val + (size_t)9 * k, xv, acc);
     }
@@ -503,16 +492,7 @@ __device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int
         const int* ptr = TR ? a.gUptr : a.gLptr;
         const int* cl = TR ? a.gUcol : a.gLcol;
         const __half* G = TR ? a.gU : a.gL;
-        const int end = ptr[row + 1];
-        int k = ptr[row] + lane;
-        for (; k + GROUP < end; k += 2 * GROUP) {
-            const int c0 = cl[k], c1 = cl[k + GROUP];
-            VT x0[3] = {u[3 * c0], u[3 * c0 + 1], u[3 * c0 + 2]};
-            VT x1[3] = {u[3 * c1], u[3 * c1 + 1], u[3 * c1 + 2]};
-            blockMulAddH(G + (size_t)9 * k, x0, acc);
-            blockMulAddH(G + (size_t)9 * (k + GROUP), x1, acc);
-        }
-        if (k < end) {
+        for (int k = ptr[row] + lane; k < ptr[row + 1]; k += GROUP) {
             const int c = cl[k];
             VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
             blockMulAddH(G + (size_t)9 * k, xv, acc);
