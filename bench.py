@@ -13,10 +13,10 @@ states.
            library's stream, state resident in HBM; L2 is flushed (256 MiB
            write) before every timed step.
   e2e      same metric through the C ABI with host buffers, on the same
-           frames (a second simulator with the frozen weights replays the
-           untimed steps): every step uploads x, v, V_prev, x_tilde from
-           pinned host memory and reads x and v back; wall clock around the
-           calls.
+           frames (the simulator returns to its state at the first timed
+           frame, kept in pinned host memory): every step uploads x, v,
+           V_prev, x_tilde from pinned host memory and reads x and v back;
+           wall clock around the calls.
   roofline achieved bandwidth of the dominant kernel, the persistent PCG
            solve: algorithmic bytes per launch (iterations x bytes per
            iteration) / launch time, both from the timed region (CUDA events
@@ -26,7 +26,8 @@ first --train-steps steps (Adam on the GPU, not timed), then frozen.  Timing
 starts after --settle-steps untimed steps and the warm-up (pile: 30, the
 lower layers of cubes rest on the box and on each other; cloth: 40, the
 cloth has reached the cube), so the timed steps are in contact.  The same
-run also times the plain FP64 block-Jacobi GPU path on the same frames.
+run also times the plain FP64 block-Jacobi GPU path on the same frames, from
+the same state (restored from pinned host memory).
 Multi-GPU: replicas only (one independent simulation per rank, weak scaling).
 
 --scene twist measures the large twist (configuration 5: 1,011,840 tets,
@@ -415,6 +416,14 @@ def main():
         pg.barrier()
     torch.cuda.synchronize()
 
+    # the state the timed frames start from, kept in pinned host memory for
+    # the end-to-end leg below
+    pins = {k: torch.empty((nv, 3), dtype=torch.float64, pin_memory=True).numpy() for k in ("x", "vel", "vprev", "xtilde")}
+    for k in pins:
+        pins[k][:] = sim.get(k)
+    kappa0 = sim.scalars()["kappa"]
+    torch.cuda.synchronize()
+
     # ---- device-timed steps ----
     sampler = ClockSampler(dev)
     sampler.start()
@@ -426,42 +435,45 @@ def main():
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStop()
     clocks = sampler.stop()
-    rp = device_timed(plain, args.steps, flush, None, cipc, torch) if plain is not None else None
+    rp = None
+    if plain is not None:
+        # the plain path times the same frames from the same state
+        for k in ("x", "vel", "vprev", "xtilde"):
+            plain.set(k, pins[k])
+        plain.set_kappa(kappa0)
+        plain.collision_sets()
+        rp = device_timed(plain, args.steps, flush, None, cipc, torch)
     max_ms = max_over_ranks(r["ms"], pg, "cuda")
     value = whole_job_rate(args.steps, world, max_ms)
 
     # ---- end to end through the C ABI with pinned host buffers, on the same
-    # frames as the device-timed steps: a second simulator with the frozen
-    # weights replays the settle and warm-up steps, then the timed frames run
-    # through the host-buffer calls ----
-    twin = cipc.Simulator(scene, precision=args.precision, precond=args.precond)
-    if learned:
-        twin.set_precond_weights(sim.precond_weights())
-    for _ in range(args.settle_steps + max(3, args.warmup)):
-        twin.step()
-    pins = {k: torch.empty((nv, 3), dtype=torch.float64, pin_memory=True).numpy() for k in ("x", "vel", "vprev", "xtilde")}
-    for k in pins:
-        pins[k][:] = twin.get(k)
+    # frames as the device-timed steps: the simulator goes back to the state
+    # it had at the first timed frame (kept in pinned host memory), and the
+    # timed frames run again through the host-buffer calls: every step
+    # uploads x, v, V_prev and x_tilde and reads x and v back ----
+    for k in ("x", "vel", "vprev", "xtilde"):
+        sim.set(k, pins[k])
+    sim.set_kappa(kappa0)
+    sim.collision_sets()
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
-    e2e_steps = max(3, args.steps)
+    e2e_steps = args.steps
     dt = scene["params"]["dt"]
-    gdt2 = np.array([0.0, -9.8 * dt * dt, 0.0])
+    gdt2 = np.array([0.0, -9.8 * dt * dt, 0.0]) if scene["params"].get("apply_gravity", 1) else np.zeros(3)
     t0 = time.perf_counter()
     lib_ms = 0.0
     for _ in range(e2e_steps):
         for k in ("x", "vel", "vprev", "xtilde"):
-            twin.set(k, pins[k])
-        lib_ms += twin.step()["stepMilliseconds"]
-        pins["x"][:] = twin.get("x")
-        pins["vel"][:] = twin.get("vel")
+            sim.set(k, pins[k])
+        lib_ms += sim.step()["stepMilliseconds"]
+        pins["x"][:] = sim.get("x")
+        pins["vel"][:] = sim.get("vel")
         # host-side state of the next step (updateInertialTarget)
         pins["vprev"][:] = pins["x"]
         pins["xtilde"][:] = pins["x"] + pins["vel"] * dt + gdt2
     e2e_s = time.perf_counter() - t0
     e2e_value = whole_job_rate(e2e_steps, world, 1000.0 * max_over_ranks(e2e_s, pg, "cuda"))
-    twin.close()
 
     if rank == 0:
         counts = sim.counts()
