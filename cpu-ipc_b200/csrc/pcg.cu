@@ -1316,13 +1316,17 @@ static bool pcgClassic() {
     return v == 1;
 }
 
-// The streaming kernel runs its three-blocks-per-SM build (48 resident
+// Blocks per SM of the streaming kernel's build: 3 by default (48 resident
 // warps for a few register spills: measured 10-24 % faster per solve on the
-// pile than two blocks per SM); CIPC_PCG_OCC3=0 selects the two-block build.
-static bool pcgOcc3() {
+// pile than two blocks per SM); CIPC_PCG_OCC=2 or 4 selects the other builds.
+static int pcgOcc() {
     static int v = -1;
-    if (v < 0) { const char* e = std::getenv("CIPC_PCG_OCC3"); v = (e && *e == '0') ? 0 : 1; }
-    return v == 1;
+    if (v < 0) {
+        const char* e = std::getenv("CIPC_PCG_OCC");
+        v = e ? std::atoi(e) : 3;
+        if (v != 2 && v != 4) v = 3;
+    }
+    return v;
 }
 
 // CIPC_PCG_NOPACK=1 keeps the streaming kernel on the slot-aligned FP32 factor.
@@ -1408,13 +1412,15 @@ static void launchPersistent(Ctx& c, PcgArgs<MT, VT>& a, int smCount, bool class
     }
     a.sliceMax = 0;
     a.rowsPerBlock = 0;
-    const bool occ3 = !classic && pcgOcc3();
+    const int occ = classic ? 0 : pcgOcc();
     const void* fn = classic ? (const void*)pcgPersistentKernel<MT, VT, LEARNED>
-                             : (occ3 ? (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false, 3> : (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false>);
+                   : occ == 4 ? (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false, 4>
+                   : occ == 3 ? (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false, 3>
+                              : (const void*)pcgPipelinedKernel<MT, VT, LEARNED, false>;
     int perSM = 0;
     CIPC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, PB, 0));
     if (perSM < 1) throw std::runtime_error("persistent PCG kernel does not fit on an SM");
-    int grid = std::max(1, std::min(std::min(std::min(perSM, occ3 ? 3 : pcgBlocksPerSm()) * smCount, needed), cap));
+    int grid = std::max(1, std::min(std::min(std::min(perSM, occ >= 3 ? occ : pcgBlocksPerSm()) * smCount, needed), cap));
     ++g_kernelLaunches;
     CIPC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PB), args, 0, c.s));
 }
