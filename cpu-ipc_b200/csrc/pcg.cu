@@ -955,9 +955,11 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
     return true;
 }
 
-// MINB: blocks per SM the compiler must fit (registers); 3 for the
-// streaming variant that trades a few spills for 48 resident warps
-template <class MT, class VT, bool LEARNED, bool CACHED, int MINB = 1>
+// MINB: blocks per SM the compiler must fit (registers: 64 per thread for
+// 2, the build of the single-pass kernel and of the two-block streaming
+// kernel); 3 and 4 for the streaming builds that trade register spills for
+// 48 or 64 resident warps
+template <class MT, class VT, bool LEARNED, bool CACHED, int MINB = 2>
 __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a) {
     extern __shared__ __align__(16) unsigned char pipeSmem[];
     // In a single-pass launch (CACHED) the block's matrix rows and its rows'
