@@ -1,10 +1,13 @@
 // Contact terms on the GPU: log-barrier (PP/PE/PT/EE), the mollified
 // nearly-parallel edge-edge term, the ground barrier and lagged friction.
 //
-// Each self contact is handled by one warp: lane 0 evaluates the closed-form
-// distance derivatives into shared memory, the warp projects the 6/9/12-DOF
-// Hessian onto the PSD cone with a parallel Jacobi sweep, then writes its
-// gradient rows and all vertex-pair 3x3 blocks as keyed entries.  The entries
+// Each self contact is handled by one half warp: lane 0 of the half
+// evaluates the distance and gradient, each of the first 3 x points lanes one
+// row of the distance Hessian, the half projects the (zero-padded) 12 x 12
+// barrier Hessian onto the PSD cone with a register-resident parallel Jacobi
+// sweep, then writes its gradient rows and all vertex-pair 3x3 blocks as
+// keyed entries.  The nearly-parallel edge-edge term keeps one warp per
+// contact and the shared-memory sweep.  The entries
 // are radix-sorted by (vertex) and (row, col) and summed per segment, so the
 // result is deterministic and needs no floating-point atomics.
 //
@@ -29,6 +32,7 @@ constexpr int TB = 128;
 constexpr int WPB = 4;  // warps per block in the warp-per-contact kernels
 inline int blocksFor(int n, int tb = TB) { return std::max(1, std::min((n + tb - 1) / tb, 148 * 32)); }
 inline int warpBlocksFor(int n) { return std::max(1, std::min((n + WPB - 1) / WPB, 148 * 64)); }
+inline int halfWarpBlocksFor(int n) { return std::max(1, std::min((n + 2 * WPB - 1) / (2 * WPB), 148 * 64)); }
 
 constexpr int GSENT = 0x7fffffff;
 constexpr uint64_t HSENT = 0xffffffffffffffffull;
@@ -114,11 +118,12 @@ __device__ __forceinline__ void putH(const DynOut& o, size_t e, int k, double v)
     else ((double*)o.hVal)[9 * e + k] = v;
 }
 
-// Writes the warp's projected n x n matrix (leading dimension n) as 16 block
+// Writes the projected n x n matrix (leading dimension ld) as 16 block
 // entries on vertices idx[0..np-1]; unused or non-free entries get the
-// sentinel key.
-__device__ void writeBlocks(const DynOut& o, size_t hBase, const double* A, int ld, const int* idx, int np, const int* btype, int lane) {
-    for (int e = lane; e < 16 * 9; e += 32) {
+// sentinel key.  `step` lanes (a warp or a half warp) share the entries.
+__device__ void writeBlocks(const DynOut& o, size_t hBase, const double* A, int ld, const int* idx, int np, const int* btype, int lane,
+                            int step = 32) {
+    for (int e = lane; e < 16 * 9; e += step) {
         int blk = e / 9, k = e % 9;
         int a = blk / 4, b = blk % 4;
         size_t slot = hBase + blk;
@@ -129,62 +134,74 @@ __device__ void writeBlocks(const DynOut& o, size_t hBase, const double* A, int 
     }
 }
 
+// shared scratch of one contact in the half-warp kernel
+struct HalfSmem {
+    double A[144], B[144], V[144];
+    double g[12], gv[12], lam[12];
+};
+
 // Self-contact barrier: gradient kappa*b'(d)*grad d (x multiplicity for
-// PP/PE) and Hessian PSD(kappa*(b'' g g^T + b' H)).
+// PP/PE) and Hessian PSD(kappa*(b'' g g^T + b' H)); contact 2w + h of the
+// grid's warps w on half h.
 __global__ void selfBarrierKernel(int n, const int* active, const double* x, const int* btype, double Hhat, double kappa, DynOut o,
                                   size_t gBase, size_t hBase, int withHessian, int* status) {
-    __shared__ JacobiSmem sm[WPB];
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    JacobiSmem& S = sm[w];
-    for (int i = blockIdx.x * WPB + w; i < n; i += gridDim.x * WPB) {
+    __shared__ HalfSmem sm[2 * WPB];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+    HalfSmem& S = sm[2 * w + half];
+    for (int i0 = 2 * (blockIdx.x * WPB + w); i0 < n; i0 += 2 * gridDim.x * WPB) {
+        const int i = i0 + half;
+        const bool act = i < n;
         int idx[4] = {0, 0, 0, 0};
-        int kind = decode(active + 4 * i, idx);
-        int np = npts(kind), nd = 3 * np;
-        int ne = nd == 9 ? 10 : nd;
-        double cf, ca = 0.0, cb = 0.0;
-        d3 p[4];
-        for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
-        if (lane == 0) {
-            double d = distVal(kind, p);
-            double gb, hb;
-            barrierG(d, Hhat, gb);
-            barrierH(d, Hhat, hb);
-            cf = (kind <= 1) ? kappa * -active[4 * i + 3] : kappa;
-            double* g = S.W;
-            distDerivs(kind, p, g, nullptr);
-            for (int k = 0; k < nd; ++k) S.V[k] = cf * gb * g[k];
-            if (!isfinite(d)) raiseStatus(status, CIPC_ST_NONFINITE);
-            ca = cf * hb;
-            cb = cf * gb;
+        int np = 0, nd = 0;
+        double ca = 0.0, cb = 0.0;
+        if (act) {
+            const int kind = decode(active + 4 * i, idx);
+            np = npts(kind);
+            nd = 3 * np;
+            d3 p[4];
+            for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
+            if (hl == 0) {
+                double d = distVal(kind, p);
+                double gb, hb;
+                barrierG(d, Hhat, gb);
+                barrierH(d, Hhat, hb);
+                const double cf = (kind <= 1) ? kappa * -active[4 * i + 3] : kappa;
+                distDerivs(kind, p, S.g, nullptr);
+                for (int k = 0; k < nd; ++k) S.gv[k] = cf * gb * S.g[k];
+                if (!isfinite(d)) raiseStatus(status, CIPC_ST_NONFINITE);
+                ca = cf * hb;
+                cb = cf * gb;
+            }
+            // the distance Hessian, one row per lane
+            if (withHessian && hl < nd) distHessRow(kind, p, hl, S.B + hl * nd);
         }
-        // the distance Hessian, one row per lane
-        if (withHessian && lane < nd) distHessRow(kind, p, lane, S.B + lane * nd);
         __syncwarp();
         if (withHessian) {
-            // kappa (b'' g g^T + b' H), the warp's lanes over the entries
-            ca = __shfl_sync(0xffffffffu, ca, 0);
-            cb = __shfl_sync(0xffffffffu, cb, 0);
-            const double* g = S.W;
-            for (int e = lane; e < ne * ne; e += 32) {
-                const int r = e / ne, q = e - r * ne;
-                // the rows came from different lanes: (r, q) and (q, r) are
-                // both formed from the upper-triangle entry, so the matrix the
-                // eigen-solver gets is exactly symmetric
-                const int lo = r <= q ? r : q, hi = r <= q ? q : r;
-                S.A[e] = (hi < nd) ? (ca * g[lo]) * g[hi] + cb * S.B[lo * nd + hi] : 0.0;
+            // kappa (b'' g g^T + b' H), zero-padded to 12 x 12; the rows came
+            // from different lanes: (r, q) and (q, r) are both formed from the
+            // upper-triangle entry, so the matrix the eigen-solver gets is
+            // exactly symmetric
+            ca = __shfl_sync(0xffffffffu, ca, 0, 16);
+            cb = __shfl_sync(0xffffffffu, cb, 0, 16);
+            if (act) {
+                for (int e = hl; e < 144; e += 16) {
+                    const int r = e / 12, q = e - r * 12;
+                    const int lo = r <= q ? r : q, hi = r <= q ? q : r;
+                    S.A[e] = (hi < nd) ? (ca * S.g[lo]) * S.g[hi] + cb * S.B[lo * nd + hi] : 0.0;
+                }
             }
             __syncwarp();
         }
         // gradient entries (4 per contact)
-        if (lane < 4) {
-            size_t slot = gBase + 4 * (size_t)i + lane;
-            bool valid = lane < np;
-            o.gKey[slot] = valid ? idx[lane] : GSENT;
-            for (int k = 0; k < 3; ++k) o.gVal[3 * slot + k] = valid ? S.V[3 * lane + k] : 0.0;
+        if (act && hl < 4) {
+            const size_t slot = gBase + 4 * (size_t)i + hl;
+            const bool valid = hl < np;
+            o.gKey[slot] = valid ? idx[hl] : GSENT;
+            for (int k = 0; k < 3; ++k) o.gVal[3 * slot + k] = valid ? S.gv[3 * hl + k] : 0.0;
         }
         if (withHessian) {
-            if (!warpPsdProject(S, ne, lane) && lane == 0) raiseStatus(status, CIPC_ST_JACOBI_CAP);
-            writeBlocks(o, hBase + 16 * (size_t)i, S.A, ne, idx, np, btype, lane);
+            if (!halfWarpPsdProject12(S.A, S.V, S.lam, hl, act) && act && hl == 0) raiseStatus(status, CIPC_ST_JACOBI_CAP);
+            if (act) writeBlocks(o, hBase + 16 * (size_t)i, S.A, 12, idx, np, btype, hl, 16);
         }
         __syncwarp();
     }
@@ -635,7 +652,7 @@ int contactAssemble(Ctx& c) {
     size_t g = 0, h = 0;
     if (c.nSelf) {
         profBegin(c, PROF_BARRIER);
-        launch(selfBarrierKernel, warpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.x, c.btype, P.Hhat, P.kappa, o, g, h, 1, c.status);
+        launch(selfBarrierKernel, halfWarpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.x, c.btype, P.Hhat, P.kappa, o, g, h, 1, c.status);
         profEnd(c, PROF_BARRIER);
     }
     g += 4 * (size_t)c.nSelf; h += 16 * (size_t)c.nSelf;
@@ -820,7 +837,7 @@ void contactGradientKappa(Ctx& c, double* gc) {
     if (c.nSelf) {
         reserveDyn(c, c.nSelf);
         DynOut o = dynOut(c);
-        launch(selfBarrierKernel, warpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.x, c.btype, P.Hhat, 1.0, o, 0, 0, 0, c.status);
+        launch(selfBarrierKernel, halfWarpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.x, c.btype, P.Hhat, 1.0, o, 0, 0, 0, c.status);
         c.nDynG = 4 * c.nSelf;
         c.nDynH = 0;
         finalizeDynamic(c);

@@ -912,30 +912,22 @@ __device__ __forceinline__ void rowAx(const PcgArgs<MT, VT>& a, const RowIter& i
     groupReduce3(acc);
 }
 
-// out = M^-1 in for the factor: S in -> tmp (own rows), barrier, t = G tmp,
-// barrier, out = S^T G^T t.  Ends without a barrier; false on timeout.
+// out = M^-1 w for the factor, with tmp = S w already written by the rows'
+// owners in the pass before: barrier, t = G tmp, barrier, out = S^T G^T t.
+// Ends without a barrier; false on timeout.
 template <class MT, class VT>
-__device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const VT* in, VT* tmp, VT* out, unsigned& ep) {
+__device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const VT* tmp, VT* out, unsigned& ep) {
     const unsigned nb = gridDim.x;
-    for (int base = it.first; base < a.nv; base += it.stride) {
-        int row = base + it.grp;
-        if (row < a.nv && it.lane == 0) {
-            const double* S = a.S + 9 * row;
-            double r0 = in[3 * row], r1 = in[3 * row + 1], r2 = in[3 * row + 2];
-            tmp[3 * row] = (VT)(S[0] * r0);
-            tmp[3 * row + 1] = (VT)(S[3] * r0 + S[4] * r1);
-            tmp[3 * row + 2] = (VT)(S[6] * r0 + S[7] * r1 + S[8] * r2);
-        }
-    }
+    const int q = it.lane;
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
         int row = base + it.grp;
         bool active = row < a.nv;
         VT acc[3] = {VT(0), VT(0), VT(0)};
-        if (active) rowFactor<false>(a, row, it.lane, (const VT*)tmp, acc);
+        if (active) rowFactor<false>(a, row, it.lane, tmp, acc);
         groupReduce3(acc);
-        if (active && it.lane == 0)
-            for (int q = 0; q < 3; ++q) a.t[3 * row + q] = acc[q];
+        // lanes 0, 1, 2 of the group store components 0, 1, 2
+        if (active && q < 3) a.t[3 * row + q] = q == 0 ? acc[0] : (q == 1 ? acc[1] : acc[2]);
     }
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
@@ -944,12 +936,11 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
         VT acc[3] = {VT(0), VT(0), VT(0)};
         if (active) rowFactor<true>(a, row, it.lane, (const VT*)a.t, acc);
         groupReduce3(acc);
-        if (active && it.lane == 0) {
-            const double* S = a.S + 9 * row;
-            double y0 = acc[0], y1 = acc[1], y2 = acc[2];
-            out[3 * row] = (VT)(S[0] * y0 + S[3] * y1 + S[6] * y2);
-            out[3 * row + 1] = (VT)(S[4] * y1 + S[7] * y2);
-            out[3 * row + 2] = (VT)(S[8] * y2);
+        if (active && q < 3) {
+            // component q of S^T y (S lower triangular)
+            const double* S = a.S + 9 * (size_t)row;
+            const double y0 = acc[0], y1 = acc[1], y2 = acc[2];
+            out[3 * row + q] = (VT)(q == 0 ? S[0] * y0 + S[3] * y1 + S[6] * y2 : (q == 1 ? S[4] * y1 + S[7] * y2 : S[8] * y2));
         }
     }
     return true;
@@ -1008,15 +999,17 @@ __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a
     VT* sw = a.Ap;  // S w, gathered by the factor's first pass
     // the row's M-related output from the group's three components of v:
     // block-Jacobi m = Dinv v into mOut (and the shared copy), or with a
-    // factor (cached path) S v into sw; lanes q < 3 of active rows store
+    // factor S v into sw, the input of the factor's first pass; lanes q < 3
+    // of active rows store
     auto precondRow = [&](int row, bool active, const VT v[3], VT* mOut) {
         if (!active || q >= 3) return;
         if (!LEARNED) {
             const VT mq = rowDot(blkRow(row), v);
             mOut[3 * row + q] = mq;
             if (CACHED) ownM[3 * (row - rc.row0) + q] = mq;
-        } else if (CACHED) {
-            const double* S = rc.blk + 9 * (row - rc.row0);  // lower triangular
+        } else {
+            // lower triangular
+            const double* S = CACHED ? rc.blk + 9 * (row - rc.row0) : a.S + 9 * (size_t)row;
             const double v0 = v[0], v1 = v[1], v2 = v[2];
             sw[3 * row + q] = (VT)(q == 0 ? S[0] * v0 : (q == 1 ? S[3] * v0 + S[4] * v1 : S[6] * v0 + S[7] * v1 + S[8] * v2));
         }
@@ -1049,7 +1042,7 @@ __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a
     if (LEARNED) {
         if (CACHED) {
             if (!factorCachedPasses(a, rc, it, (const VT*)sw, a.u, ownU, ep)) return;
-        } else if (!factorPasses(a, it, (const VT*)a.r, sw, a.u, ep)) {
+        } else if (!factorPasses(a, it, (const VT*)sw, a.u, ep)) {
             return;
         }
     }
@@ -1080,7 +1073,7 @@ __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a
     if (LEARNED) {
         if (CACHED) {
             if (!factorCachedPasses(a, rc, it, (const VT*)sw, a.mA, ownM, ep)) return;
-        } else if (!factorPasses(a, it, (const VT*)a.w, sw, a.mA, ep)) {
+        } else if (!factorPasses(a, it, (const VT*)sw, a.mA, ep)) {
             return;
         }
     }
@@ -1133,12 +1126,12 @@ __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a
         const int set = (iter + 1) & 1;
         blockReduce3(lrr, lg, ld);
         if (threadIdx.x == 0) { part(set, 0)[blockIdx.x] = lrr; part(set, 1)[blockIdx.x] = lg; part(set, 2)[blockIdx.x] = ld; }
-        // the factor's m is replaced only in its third pass, two barriers
+        // the factor's m is replaced only in its last pass, two barriers
         // after every row read it
         if (LEARNED) {
             if (CACHED) {
                 if (!factorCachedPasses(a, rc, it, (const VT*)sw, mNext, ownM, ep)) return;
-            } else if (!factorPasses(a, it, (const VT*)a.w, sw, mNext, ep)) {
+            } else if (!factorPasses(a, it, (const VT*)sw, mNext, ep)) {
                 return;
             }
         }
