@@ -181,6 +181,7 @@ struct Ctx {
     DBuf<int> dynRowStart, dynRowEnd, dynCol, dynSrcStart;
     DBuf<double> dynBD;
     DBuf<float> dynBF;
+    DBuf<double> barrierUpper;      // packed upper triangles of the self-contact barrier Hessians (78 per contact)
     DBuf<unsigned char> groundTmp;  // temporary storage of the ground-set selection (runs beside the PP/PE encoding)
     DBuf<unsigned char> sortTmp;
 

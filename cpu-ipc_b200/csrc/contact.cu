@@ -134,74 +134,77 @@ __device__ void writeBlocks(const DynOut& o, size_t hBase, const double* A, int 
     }
 }
 
-// shared scratch of one contact in the half-warp kernel
+// shared scratch of one contact in the half-warp projection kernel
 struct HalfSmem {
-    double A[144], B[144], V[144];
-    double g[12], gv[12], lam[12];
+    double A[144], V[144], lam[12];
 };
 
-// Self-contact barrier: gradient kappa*b'(d)*grad d (x multiplicity for
-// PP/PE) and Hessian PSD(kappa*(b'' g g^T + b' H)); contact 2w + h of the
-// grid's warps w on half h.
-__global__ void selfBarrierKernel(int n, const int* active, const double* x, const int* btype, double Hhat, double kappa, DynOut o,
-                                  size_t gBase, size_t hBase, int withHessian, int* status) {
+// index of entry (lo, hi), lo <= hi < 12, in a packed upper triangle (78)
+__host__ __device__ constexpr int upperIndex(int lo, int hi) { return lo * 12 - lo * (lo - 1) / 2 + (hi - lo); }
+
+// Self-contact barrier, one thread per contact: the gradient entries
+// kappa*b'(d)*grad d (x multiplicity for PP/PE) and, withHessian, the upper
+// triangle of kappa*(b'' g g^T + b' H) zero-padded to 12 x 12, 78 values per
+// contact at upper + 78 i, for the projection kernel.  Every entry (r, q) is
+// formed once, so the matrix the eigen-solver gets is exactly symmetric.
+__global__ void selfBarrierKernel(int n, const int* active, const double* x, double Hhat, double kappa, DynOut o, size_t gBase,
+                                  int withHessian, double* upper, int* status) {
+    CIPC_KERNEL_LOOP(i, n) {
+        int idx[4] = {0, 0, 0, 0};
+        const int kind = decode(active + 4 * i, idx);
+        const int np = npts(kind), nd = 3 * np;
+        d3 p[4];
+        for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
+        const double d = distVal(kind, p);
+        double gb, hb;
+        barrierG(d, Hhat, gb);
+        barrierH(d, Hhat, hb);
+        const double cf = (kind <= 1) ? kappa * -active[4 * i + 3] : kappa;
+        if (!isfinite(d)) raiseStatus(status, CIPC_ST_NONFINITE);
+        double g[12], H[144];
+        distDerivs(kind, p, g, withHessian ? H : nullptr);
+        for (int a = 0; a < 4; ++a) {
+            const size_t slot = gBase + 4 * (size_t)i + a;
+            const bool valid = a < np;
+            o.gKey[slot] = valid ? idx[a] : GSENT;
+            for (int k = 0; k < 3; ++k) o.gVal[3 * slot + k] = valid ? cf * gb * g[3 * a + k] : 0.0;
+        }
+        if (withHessian) {
+            const double ca = cf * hb, cb = cf * gb;
+            double* U = upper + 78 * (size_t)i;
+            for (int lo = 0; lo < 12; ++lo)
+                for (int hi = lo; hi < 12; ++hi)
+                    U[upperIndex(lo, hi)] = (hi < nd) ? (ca * g[lo]) * g[hi] + cb * H[lo * nd + hi] : 0.0;
+        }
+    }
+}
+
+// PSD projection of the self-contact barrier Hessians, one half warp per
+// contact (two per warp): the packed upper triangle is unfolded into a
+// symmetric 12 x 12 in shared memory, projected by the register-resident
+// Jacobi sweep and written as the contact's 16 vertex-pair blocks.  Three
+// blocks per SM: 168 registers (the columns of the matrix and of its
+// eigenvectors stay in registers) for 12 resident warps.
+__global__ void __launch_bounds__(32 * WPB, 3) selfBarrierPsdKernel(int n, const int* active, const int* btype, const double* upper, DynOut o, size_t hBase, int* status) {
     __shared__ HalfSmem sm[2 * WPB];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
     HalfSmem& S = sm[2 * w + half];
     for (int i0 = 2 * (blockIdx.x * WPB + w); i0 < n; i0 += 2 * gridDim.x * WPB) {
         const int i = i0 + half;
         const bool act = i < n;
-        int idx[4] = {0, 0, 0, 0};
-        int np = 0, nd = 0;
-        double ca = 0.0, cb = 0.0;
         if (act) {
-            const int kind = decode(active + 4 * i, idx);
-            np = npts(kind);
-            nd = 3 * np;
-            d3 p[4];
-            for (int k = 0; k < np; ++k) p[k] = ld3(x, idx[k]);
-            if (hl == 0) {
-                double d = distVal(kind, p);
-                double gb, hb;
-                barrierG(d, Hhat, gb);
-                barrierH(d, Hhat, hb);
-                const double cf = (kind <= 1) ? kappa * -active[4 * i + 3] : kappa;
-                distDerivs(kind, p, S.g, nullptr);
-                for (int k = 0; k < nd; ++k) S.gv[k] = cf * gb * S.g[k];
-                if (!isfinite(d)) raiseStatus(status, CIPC_ST_NONFINITE);
-                ca = cf * hb;
-                cb = cf * gb;
+            const double* U = upper + 78 * (size_t)i;
+            for (int e = hl; e < 144; e += 16) {
+                const int r = e / 12, q = e - r * 12;
+                S.A[e] = U[r <= q ? upperIndex(r, q) : upperIndex(q, r)];
             }
-            // the distance Hessian, one row per lane
-            if (withHessian && hl < nd) distHessRow(kind, p, hl, S.B + hl * nd);
         }
         __syncwarp();
-        if (withHessian) {
-            // kappa (b'' g g^T + b' H), zero-padded to 12 x 12; the rows came
-            // from different lanes: (r, q) and (q, r) are both formed from the
-            // upper-triangle entry, so the matrix the eigen-solver gets is
-            // exactly symmetric
-            ca = __shfl_sync(0xffffffffu, ca, 0, 16);
-            cb = __shfl_sync(0xffffffffu, cb, 0, 16);
-            if (act) {
-                for (int e = hl; e < 144; e += 16) {
-                    const int r = e / 12, q = e - r * 12;
-                    const int lo = r <= q ? r : q, hi = r <= q ? q : r;
-                    S.A[e] = (hi < nd) ? (ca * S.g[lo]) * S.g[hi] + cb * S.B[lo * nd + hi] : 0.0;
-                }
-            }
-            __syncwarp();
-        }
-        // gradient entries (4 per contact)
-        if (act && hl < 4) {
-            const size_t slot = gBase + 4 * (size_t)i + hl;
-            const bool valid = hl < np;
-            o.gKey[slot] = valid ? idx[hl] : GSENT;
-            for (int k = 0; k < 3; ++k) o.gVal[3 * slot + k] = valid ? S.gv[3 * hl + k] : 0.0;
-        }
-        if (withHessian) {
-            if (!halfWarpPsdProject12(S.A, S.V, S.lam, hl, act) && act && hl == 0) raiseStatus(status, CIPC_ST_JACOBI_CAP);
-            if (act) writeBlocks(o, hBase + 16 * (size_t)i, S.A, 12, idx, np, btype, hl, 16);
+        if (!halfWarpPsdProject12(S.A, S.V, S.lam, hl, act) && act && hl == 0) raiseStatus(status, CIPC_ST_JACOBI_CAP);
+        if (act) {
+            int idx[4] = {0, 0, 0, 0};
+            const int np = npts(decode(active + 4 * i, idx));
+            writeBlocks(o, hBase + 16 * (size_t)i, S.A, 12, idx, np, btype, hl, 16);
         }
         __syncwarp();
     }
@@ -652,7 +655,9 @@ int contactAssemble(Ctx& c) {
     size_t g = 0, h = 0;
     if (c.nSelf) {
         profBegin(c, PROF_BARRIER);
-        launch(selfBarrierKernel, halfWarpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.x, c.btype, P.Hhat, P.kappa, o, g, h, 1, c.status);
+        c.barrierUpper.reserve(78 * (size_t)c.nSelf);
+        launch(selfBarrierKernel, blocksFor(c.nSelf), TB, 0, c.s, c.nSelf, c.selfActive, c.x, P.Hhat, P.kappa, o, g, 1, c.barrierUpper.p, c.status);
+        launch(selfBarrierPsdKernel, halfWarpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.btype, c.barrierUpper.p, o, h, c.status);
         profEnd(c, PROF_BARRIER);
     }
     g += 4 * (size_t)c.nSelf; h += 16 * (size_t)c.nSelf;
@@ -837,7 +842,7 @@ void contactGradientKappa(Ctx& c, double* gc) {
     if (c.nSelf) {
         reserveDyn(c, c.nSelf);
         DynOut o = dynOut(c);
-        launch(selfBarrierKernel, halfWarpBlocksFor(c.nSelf), 32 * WPB, 0, c.s, c.nSelf, c.selfActive, c.x, c.btype, P.Hhat, 1.0, o, 0, 0, 0, c.status);
+        launch(selfBarrierKernel, blocksFor(c.nSelf), TB, 0, c.s, c.nSelf, c.selfActive, c.x, P.Hhat, 1.0, o, (size_t)0, 0, (double*)nullptr, c.status);
         c.nDynG = 4 * c.nSelf;
         c.nDynH = 0;
         finalizeDynamic(c);
