@@ -170,14 +170,17 @@ __device__ inline bool warpPsdProject(JacobiSmem& S, int n, int lane) {
 
 // ---------------------------------------------------------------------------
 // The same projection for a 12 x 12 matrix held in registers by the 16 lanes
-// of a half warp: column j of the matrix and of the eigenvector matrix in
-// lane j (lanes 12-15 hold nothing).  Each round of the round-robin schedule
-// takes the partner column by shuffle (right rotation), mixes the row pairs
-// in registers (left rotation) and mixes the eigenvector columns the same
-// way, so a sweep touches no shared memory; two matrices share a warp.
-// Smaller contacts are zero-padded to 12: their padded rows and columns stay
-// zero and add eigenvalues 0, so the projection of the leading block is
-// unchanged.
+// of a half warp, by one-sided (Hestenes) Jacobi on B = A + mu I with
+// mu = ||A||_F, which is positive semidefinite, so that its singular vectors
+// are the eigenvectors of A.  Lane j holds column j of W (B V as the sweeps
+// proceed) and of V (lanes 12-15 hold nothing).  A rotation of columns p, q
+// needs only those two columns: each round takes the partner's columns by
+// shuffle and updates its own, with no row operations, so the round's code
+// is the same for every round and no register is indexed by the lane.  At
+// the end lambda_j = w_j . v_j - mu.  Two matrices share a warp.  Smaller
+// contacts are zero-padded to 12: a padded column never rotates (its inner
+// product with every other column is zero) and adds the eigenvalue 0, so the
+// projection of the leading block is unchanged.
 // ---------------------------------------------------------------------------
 
 // partner of index i in round r of the round-robin schedule over m + 1 indices
@@ -185,106 +188,91 @@ __device__ inline bool warpPsdProject(JacobiSmem& S, int n, int lane) {
 __host__ __device__ constexpr int rrPartner(int m, int r, int i) {
     return i == m ? r : (i == r ? m : (2 * r - i + m) % m);
 }
-// the pair of round r that holds index i: 0 for (r, m), else 1 .. (m - 1) / 2
-__host__ __device__ constexpr int rrPairIndex(int m, int r, int i) {
-    return (i == m || i == r) ? 0 : (((i - r + m) % m) <= m / 2 ? (i - r + m) % m : m - (i - r + m) % m);
-}
-// lower index of pair k of round r
-__host__ __device__ constexpr int rrPairLow(int m, int r, int k) {
-    return k == 0 ? r : ((r + k) % m < (r - k + m) % m ? (r + k) % m : (r - k + m) % m);
-}
-
-template <int N>
-__device__ __forceinline__ double pickReg(const double (&a)[N], int k) {
-    double v = a[0];
-#pragma unroll
-    for (int i = 1; i < N; ++i) v = (k == i) ? a[i] : v;
-    return v;
-}
 
 // Projects the symmetric 12 x 12 matrix A (shared memory, row-major) onto
 // the PSD cone as warpPsdProject does: A is left unchanged when no
 // eigenvalue is negative, else replaced by V max(L, 0) V^T (formed from the
 // upper triangle of each product, so exactly symmetric).  V (144 doubles)
 // and lam (12) are shared scratch of the same half warp.  Every lane of the
-// warp calls it; `active` is false on a half without a matrix.  Returns false
-// if the sweep cap was hit.
+// warp calls it; `active` is false on a half without a matrix.  A sweep
+// rotates every pair whose columns are not orthogonal to 1e-15 (relative);
+// the sweeps stop after one whose largest relative inner product was at most
+// 1e-8 (quadratic convergence leaves about 1e-16).  Returns false if the
+// sweep cap was hit.
 __device__ inline bool halfWarpPsdProject12(double* A, double* V, double* lam, int hl, bool active) {
     constexpr int N = 12, M = N - 1;
     constexpr unsigned FULL = 0xffffffffu;
     const int j = hl;
     const bool own = active && j < N;
-    double a[N], v[N];
+    double w[N], v[N];
+    double fro = 0.0;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-        a[k] = own ? A[k * N + j] : 0.0;
+        w[k] = own ? A[k * N + j] : 0.0;
+        fro += w[k] * w[k];
+    }
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) fro += __shfl_xor_sync(FULL, fro, o, 16);
+    const double mu = sqrt(fro);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (k == j) w[k] += mu;
         v[k] = (k == j) ? 1.0 : 0.0;
     }
-    bool done = !active, converged = !active;
+    // a zero or non-finite matrix is left as it is
+    bool done = !active || !(mu > 0.0 && mu < 1e300);
+    bool converged = done;
     for (int sweep = 0; sweep < 40; ++sweep) {
-        double off = 0.0, dg = 0.0;
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            const double t = a[k] * a[k];
-            if (k == j) dg += t; else off += t;
-        }
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-            off += __shfl_xor_sync(FULL, off, o, 16);
-            dg += __shfl_xor_sync(FULL, dg, o, 16);
-        }
-        // the stopping rule of warpPsdProject
-        if (!done && (off <= 1e-30 * dg || off == 0.0 || !(dg < 1e300))) { done = true; converged = true; }
         if (__all_sync(FULL, done)) break;
-#pragma unroll
+        double mx = 0.0;
         for (int r = 0; r < M; ++r) {
             const int P = j < N ? rrPartner(M, r, j) : j;
             const bool lower = j < P;
-            const double dj = pickReg<N>(a, j), apq = pickReg<N>(a, P);
-            const double dp = __shfl_sync(FULL, dj, P, 16);
-            // the rotation of pair (p, q), p < q, on lane p
-            double c = 1.0, s = 0.0;
-            if (!done && lower && apq != 0.0) {
-                const double theta = (dp - dj) / (2.0 * apq);
-                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                c = 1.0 / sqrt(t * t + 1.0);
-                s = t * c;
-            }
-            double cp[N / 2], sp[N / 2];
-#pragma unroll
-            for (int k = 0; k < N / 2; ++k) {
-                cp[k] = __shfl_sync(FULL, c, rrPairLow(M, r, k), 16);
-                sp[k] = __shfl_sync(FULL, s, rrPairLow(M, r, k), 16);
-            }
-            const int lo = lower ? j : P;
-            const double cj = __shfl_sync(FULL, c, lo, 16);
-            const double sj = lower ? -__shfl_sync(FULL, s, lo, 16) : __shfl_sync(FULL, s, lo, 16);
-            // column j' = c_j col_j + sn_j col_P (column p' = c col_p - s col_q, q' = s col_p + c col_q)
-            double na[N];
+            double wp[N];
+            double gam = 0.0, nn = 0.0;
 #pragma unroll
             for (int k = 0; k < N; ++k) {
-                const double o = __shfl_sync(FULL, a[k], P, 16);
-                na[k] = cj * a[k] + sj * o;
+                wp[k] = __shfl_sync(FULL, w[k], P, 16);
+                gam += w[k] * wp[k];
+                nn += w[k] * w[k];
             }
-            // rows: row i' = c_i row_i + sn_i row_pi, with the signs of the columns
+            const double np = __shfl_sync(FULL, nn, P, 16);
+            // alpha = |w_p|^2, beta = |w_q|^2 for the pair p < q (both lanes
+            // form the same gamma: the same products in the same order)
+            const double al = lower ? nn : np, be = lower ? np : nn;
+            double c = 1.0, s = 0.0;
+            if (!done && P != j && gam != 0.0) {
+                const double rel = fabs(gam) / (sqrt(al) * sqrt(be));
+                mx = fmax(mx, rel);
+                if (rel > 1e-15) {
+                    const double z = (be - al) / (2.0 * gam);
+                    const double t = (z >= 0 ? 1.0 : -1.0) / (fabs(z) + sqrt(1.0 + z * z));
+                    c = 1.0 / sqrt(1.0 + t * t);
+                    s = c * t;
+                }
+            }
+            // w_p' = c w_p - s w_q, w_q' = s w_p + c w_q, and the same for V
+            const double sj = lower ? -s : s;
 #pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const int pi = rrPartner(M, r, i), k = rrPairIndex(M, r, i);
-                const double si = i < pi ? -sp[k] : sp[k];
-                a[i] = cp[k] * na[i] + si * na[pi];
-            }
+            for (int k = 0; k < N; ++k) w[k] = c * w[k] + sj * wp[k];
 #pragma unroll
             for (int k = 0; k < N; ++k) {
                 const double o = __shfl_sync(FULL, v[k], P, 16);
-                v[k] = cj * v[k] + sj * o;
+                v[k] = c * v[k] + sj * o;
             }
         }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o, 16));
+        if (!done && mx <= 1e-8) { done = true; converged = true; }
     }
-    const double lj = pickReg<N>(a, j);
+    double lj = 0.0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) lj += w[k] * v[k];
+    lj -= mu;
     double mn = own ? lj : 1e300;
 #pragma unroll
     for (int o = 8; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(FULL, mn, o, 16));
-    const bool project = active && mn < 0.0;
+    const bool project = active && converged && mn < 0.0 && mu < 1e300;
     if (project && j < N) {
         lam[j] = fmax(lj, 0.0);
 #pragma unroll

@@ -437,65 +437,6 @@ __device__ __forceinline__ bool gridBarrierSum(unsigned* bar, int* flag, unsigne
     return ok != 0;
 }
 
-// Bulk prefetch of the 16-byte granules inside [p, p + bytes) into L2 (a
-// hint: nothing is written, and the range is clipped inward to whole
-// granules, so no byte outside it is touched).
-__device__ __forceinline__ void prefetchL2(const void* p, size_t bytes) {
-    if (!p) return;
-    uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
-    const uintptr_t e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
-    while (a < e) {
-        const uint32_t n = (uint32_t)(e - a < 65536 ? e - a : 65536);
-        asm volatile(
-            "{\n\t.reg .u64 g;\n\t"
-            "cvta.to.global.u64 g, %0;\n\t"
-            "cp.async.bulk.prefetch.L2.global [g], %1;\n\t}" ::"l"(a), "r"(n)
-            : "memory");
-        a += n;
-    }
-}
-
-// Streaming passes: block b works through the row chunks [b + k * grid) *
-// CHUNK of CHUNK = 128 rows (16 warps of 8 row groups), the same rows in
-// every pass.  While it works on one chunk, its first thread prefetches the
-// arrays of the next chunk into L2 (the static matrix rows, the factor rows
-// and the rows' own vectors), so that the warps' dependent loads (column,
-// then the gathered vector) wait on L2 rather than on HBM.
-constexpr int CHUNK = PB / GROUP;
-
-template <class MT, class VT>
-__device__ __forceinline__ void prefetchChunk(const PcgArgs<MT, VT>& a, int pass, int r0, bool learned) {
-    const int r1 = min(a.nv, r0 + CHUNK);
-    if (r0 >= r1) return;
-    const size_t rows = (size_t)(r1 - r0);
-    if (pass == 0) {
-        const int s0 = a.rowPtr[r0], s1 = a.rowPtr[r1];
-        prefetchL2(a.col + s0, sizeof(int) * (size_t)(s1 - s0));
-        prefetchL2(a.val + (size_t)9 * s0, sizeof(MT) * 9 * (size_t)(s1 - s0));
-        VT* const own[8] = {a.x, a.r, a.u, a.w, a.z, a.q, a.s, a.p};
-        for (int k = 0; k < 8; ++k) prefetchL2(own[k] + 3 * (size_t)r0, sizeof(VT) * 3 * rows);
-        prefetchL2(a.diagExtra + 9 * (size_t)r0, sizeof(double) * 9 * rows);
-        prefetchL2((learned ? a.S : a.Dinv) + 9 * (size_t)r0, sizeof(double) * 9 * rows);
-    } else if (a.gL) {
-        const int* ptr = pass == 1 ? a.gLptr : a.gUptr;
-        const int s0 = ptr[r0], s1 = ptr[r1];
-        prefetchL2((pass == 1 ? a.gLcol : a.gUcol) + s0, sizeof(int) * (size_t)(s1 - s0));
-        prefetchL2((pass == 1 ? a.gL : a.gU) + (size_t)9 * s0, sizeof(__half) * 9 * (size_t)(s1 - s0));
-        if (pass == 2) prefetchL2(a.S + 9 * (size_t)r0, sizeof(double) * 9 * rows);
-    }
-}
-
-// Called by every thread at the top of each chunk of a streaming pass, with
-// the first row of its warp's groups: thread 0 of the block prefetches the
-// block's next chunk of this pass, or after its last chunk the first chunk
-// of the pass that follows.
-template <class MT, class VT>
-__device__ __forceinline__ void prefetchNext(const PcgArgs<MT, VT>& a, int pass, int nextPass, int base, int stride, bool learned) {
-    if (threadIdx.x != 0) return;
-    if (base + stride < a.nv) prefetchChunk(a, pass, base + stride, learned);
-    else prefetchChunk(a, nextPass, blockIdx.x * CHUNK, learned);
-}
-
 // Row-group iteration shared by every phase: the same (block, lane group)
 // owns the same rows in all phases.
 struct RowIter {
@@ -980,7 +921,6 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
     const int q = it.lane;
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
-        prefetchNext(a, 1, 2, base, it.stride, true);
         int row = base + it.grp;
         bool active = row < a.nv;
         VT acc[3] = {VT(0), VT(0), VT(0)};
@@ -991,7 +931,6 @@ __device__ bool factorPasses(const PcgArgs<MT, VT>& a, const RowIter& it, const 
     }
     if (!gridBarrier(a.bar, a.flag, nb, ep)) return false;
     for (int base = it.first; base < a.nv; base += it.stride) {
-        prefetchNext(a, 2, 0, base, it.stride, true);
         int row = base + it.grp;
         bool active = row < a.nv;
         VT acc[3] = {VT(0), VT(0), VT(0)};
@@ -1111,7 +1050,6 @@ __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a
     // w = A u, m = M w, gamma = (r,u), delta = (w,u)
     double g = 0, dl = 0;
     for (int base = it.first; base < rEnd; base += it.stride) {
-        if (!CACHED) prefetchNext(a, 0, LEARNED ? 1 : 0, base, it.stride, LEARNED);
         const int row = base + it.grp;
         const bool active = row < rEnd;
         VT acc[3] = {VT(0), VT(0), VT(0)};
@@ -1159,7 +1097,6 @@ __global__ void __launch_bounds__(PB, MINB) pcgPipelinedKernel(PcgArgs<MT, VT> a
         const VT bt = (VT)beta, al = (VT)alpha;
         double lrr = 0, lg = 0, ld = 0;
         for (int base = it.first; base < rEnd; base += it.stride) {
-            if (!CACHED) prefetchNext(a, 0, LEARNED ? 1 : 0, base, it.stride, LEARNED);
             const int row = base + it.grp;
             const bool active = row < rEnd;
             VT acc[3] = {VT(0), VT(0), VT(0)};

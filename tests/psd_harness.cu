@@ -1,7 +1,7 @@
 // GPU harness for the PSD projections of the contact kernels
-// (cpu-ipc_b200/csrc/cipc_device.cuh): the half-warp register sweep
-// (halfWarpPsdProject12, two matrices per warp) and the warp shared-memory
-// sweep (warpPsdProject), each applied to n row-major 12 x 12 matrices.
+// (cpu-ipc_b200/csrc/cipc_device.cuh): the half-warp one-sided Jacobi sweep
+// in registers (halfWarpPsdProject12, two matrices per warp) and the warp
+// shared-memory two-sided sweep (warpPsdProject), each applied to n row-major 12 x 12 matrices.
 #include "cipc_device.cuh"
 
 namespace {

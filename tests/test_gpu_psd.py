@@ -1,6 +1,7 @@
-"""PSD projection of the contact Hessians on a B200: the half-warp register
-sweep (halfWarpPsdProject12, used by the self-contact barrier kernel) and the
-warp shared-memory sweep (warpPsdProject, the mollified edge-edge kernel),
+"""PSD projection of the contact Hessians on a B200: the half-warp one-sided
+Jacobi sweep in registers (halfWarpPsdProject12, used by the self-contact
+barrier kernel) and the warp shared-memory two-sided sweep (warpPsdProject,
+the mollified edge-edge and hinge kernels),
 both against numpy's eigen-decomposition V max(L, 0) V^T, which is the rule
 of the reference's makePD (CPU IPC/IPCSolver.cpp:238-267).
 
