@@ -212,5 +212,128 @@ __global__ void __launch_bounds__(THREADS) denseTcKernel(int n, G gather, E emit
     if (warp == 0) tmemFree(dTmem, OUT);
 }
 
+// Weight gradient of a 64 -> 32 layer on the tensor cores:
+//   dW^T (64 x 32) = sum over items of x_item^T d_item, db = sum of d_item,
+// x the item's 64 BF16-exact inputs ([X1 | X2], 32 + 32 FP32 values already
+// rounded to BF16 by the forward's rule), d its 32 FP32 output gradients.
+// One tile of 128 items is one K = 128 slab of the contraction: the operand
+// A (M = 128 x K, K-major) holds x^T in rows 0-63, ones in row 64 (the bias
+// gradient comes out as row 64 of the product) and zeros below; B (N = 32 x
+// K) holds d^T split into two BF16 terms, hi = bf16(d) and lo = bf16(d - hi),
+// so that the two MMAs per K step carry d to about 16 bits and every product
+// is exact in the FP32 accumulator.  Each CTA accumulates its tiles in
+// tensor memory and writes one partial (OUT * 64 weights then OUT biases, the
+// layout of the CUDA-core kernel's partials); items with mask 0 contribute
+// nothing.  Dynamic shared memory: WG_SMEM bytes.  Waits are bounded as in
+// denseTcKernel.
+constexpr int WG_K = 128;  // items per tile
+constexpr int WG_SMEM = M * WG_K * 2 + 2 * 32 * WG_K * 2;
+
+__global__ void __launch_bounds__(THREADS) weightGradTcKernel(int items, const float* D, const float* X1, const float* X2, const unsigned char* mask,
+                                                              float* partial, int* status, int timeoutBit) {
+    constexpr int IN = 64, OUT = 32, NW = OUT * IN + OUT;
+    extern __shared__ __align__(1024) unsigned char wgSmem[];
+    unsigned char* sA = wgSmem;                  // M x WG_K
+    unsigned char* sBh = wgSmem + M * WG_K * 2;  // OUT x WG_K
+    unsigned char* sBl = sBh + OUT * WG_K * 2;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmemBase;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // rows 65-127 of A stay zero
+    for (int r = 65 + warp; r < M; r += THREADS / 32)
+        for (int k = lane; k < WG_K; k += 32) *reinterpret_cast<__nv_bfloat16*>(sA + coreOffset(r, k, M)) = __float2bfloat16_rn(0.f);
+    if (tid == 0) {
+        mbarInit(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tmemAlloc(&tmemBase, OUT);
+    fenceProxyAsync();
+    fenceBeforeSync();
+    __syncthreads();
+    fenceAfterSync();
+    const uint32_t dTmem = tmemBase;
+    constexpr uint32_t idesc = instrDesc(M, OUT);
+    constexpr uint32_t lboA = (M / 8) * 128, lboB = (OUT / 8) * 128, sbo = 128;
+    unsigned phase = 0;
+    bool any = false, ok = true;
+    for (int base = blockIdx.x * WG_K; base < items; base += gridDim.x * WG_K) {
+        // thread t stores item base + t as column t of A and of the two B terms
+        const int it = base + tid;
+        const bool on = it < items && (!mask || mask[it]);
+        const float4* x1 = reinterpret_cast<const float4*>(X1 + (size_t)(on ? it : 0) * 32);
+        const float4* x2 = reinterpret_cast<const float4*>(X2 + (size_t)(on ? it : 0) * 32);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const float4 v = on ? (q < 8 ? x1[q] : x2[q - 8]) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) *reinterpret_cast<__nv_bfloat16*>(sA + coreOffset(4 * q + u, tid, M)) = __float2bfloat16_rn(e[u]);
+        }
+        *reinterpret_cast<__nv_bfloat16*>(sA + coreOffset(64, tid, M)) = __float2bfloat16_rn(on ? 1.f : 0.f);
+        const float4* dv = reinterpret_cast<const float4*>(D + (size_t)(on ? it : 0) * OUT);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 v = on ? dv[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const __nv_bfloat16 hi = __float2bfloat16_rn(e[u]);
+                const __nv_bfloat16 lo = __float2bfloat16_rn(e[u] - __bfloat162float(hi));
+                *reinterpret_cast<__nv_bfloat16*>(sBh + coreOffset(4 * q + u, tid, OUT)) = hi;
+                *reinterpret_cast<__nv_bfloat16*>(sBl + coreOffset(4 * q + u, tid, OUT)) = lo;
+            }
+        }
+        fenceProxyAsync();
+        fenceBeforeSync();
+        __syncthreads();
+        fenceAfterSync();
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < WG_K / 16; ++s) {
+                const uint64_t a = smemDesc(smemAddr(sA) + s * 2 * lboA, lboA, sbo);
+                mmaBf16(dTmem, a, smemDesc(smemAddr(sBh) + s * 2 * lboB, lboB, sbo), idesc, any || s > 0);
+                mmaBf16(dTmem, a, smemDesc(smemAddr(sBl) + s * 2 * lboB, lboB, sbo), idesc, true);
+            }
+            mmaCommit(&mbar);
+        }
+        any = true;
+        const bool done = mbarWait(&mbar, phase);
+        if (!__syncthreads_and(done)) {
+            // as in denseTcKernel: a second bounded wait before the tensor
+            // memory is freed; the host treats the bit as fatal
+            if (tid == 0) {
+                atomicOr(status, timeoutBit);
+                mbarWait(&mbar, phase);
+            }
+            ok = false;
+            break;
+        }
+        phase ^= 1u;
+        fenceAfterSync();
+    }
+    if (ok) {
+        // accumulator lane m = row m of the product: weights for m < 64, biases at m = 64
+        float acc[32];
+        if (any) {
+            tmemLoad32(dTmem + ((uint32_t)(warp * 32) << 16), acc);
+        } else {
+#pragma unroll
+            for (int o = 0; o < 32; ++o) acc[o] = 0.f;
+        }
+        float* P = partial + (size_t)blockIdx.x * NW;
+        if (tid < IN) {
+#pragma unroll
+            for (int o = 0; o < OUT; ++o) P[o * IN + tid] = acc[o];
+        } else if (tid == IN) {
+#pragma unroll
+            for (int o = 0; o < OUT; ++o) P[OUT * IN + o] = acc[o];
+        }
+    }
+    fenceBeforeSync();
+    __syncthreads();
+    fenceAfterSync();
+    if (warp == 0) tmemFree(dTmem, OUT);
+}
+
 }  // namespace tc
 }  // namespace cipc

@@ -539,10 +539,9 @@ constexpr int WG_THREADS = 256;
 constexpr int WG_GRID = 296;     // CTAs of the split-K reduction (2 per SM)
 
 // X = [X1 (ld1, IN1 columns) ; X2 (ld2, IN2 columns)] per item; mask may be
-// null (all items active).  partial[cta][OUT*(IN1+IN2) + OUT].  RX: the
-// layer's forward multiplies BF16-rounded inputs (tensor-core layers), so
-// the weight gradient uses the same rounded X.
-template <int OUT, int IN1, int IN2, bool RX = false>
+// null (all items active).  partial[cta][OUT*(IN1+IN2) + OUT].  The heads
+// and the embeddings (the tensor-core layers use weightGradTcKernel).
+template <int OUT, int IN1, int IN2>
 __global__ void __launch_bounds__(WG_THREADS) weightGradKernel(int items, const float* D, const float* X1, const float* X2, const unsigned char* mask,
                                                                float* partial) {
     constexpr int IN = IN1 + IN2;
@@ -564,7 +563,7 @@ __global__ void __launch_bounds__(WG_THREADS) weightGradKernel(int items, const 
             bool on = it < items && (!mask || mask[it]);
             float v = 0.f;
             if (on) v = i < IN1 ? X1[(size_t)it * IN1 + i] : X2[(size_t)it * IN2 + (i - IN1)];
-            sX[r][i] = RX ? __bfloat162float(__float2bfloat16_rn(v)) : v;
+            sX[r][i] = v;
         }
         __syncthreads();
         for (int q = 0; q < PER; ++q) {
@@ -1040,6 +1039,20 @@ static double lossT(Ctx& c, const MT* val, const MT* dval, int nprobes, const fl
         launch(kernel, grid, WG_THREADS, 0, c.s, n, (const float*)BD, X1, X2, mask, c.mpPart.p);
         launch(weightGradReduceKernel, blocksFor(nw), TB, 0, c.s, nw, out, grid, (const float*)c.mpPart.p, gW + wOff, gW + bOff);
     };
+    // the 64 -> 32 message-passing layers: the same contraction on the tensor cores
+    auto wgradTc = [&](int n, const float* X1, const float* X2, const unsigned char* mask, int wOff, int bOff) {
+        if (n <= 0) return;
+        static bool attr = false;
+        if (!attr) {
+            CIPC_CUDA(cudaFuncSetAttribute(tc::weightGradTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::WG_SMEM));
+            attr = true;
+        }
+        const int nw = MPNN_H * 2 * MPNN_H + MPNN_H;
+        const int grid = std::max(1, std::min(WG_GRID, (n + tc::WG_K - 1) / tc::WG_K));
+        launch(tc::weightGradTcKernel, grid, tc::THREADS, tc::WG_SMEM, c.s, n, (const float*)BD, X1, X2, mask, c.mpPart.p, c.status.p,
+               (int)CIPC_ST_TC_TIMEOUT);
+        launch(weightGradReduceKernel, blocksFor(nw), TB, 0, c.s, nw, MPNN_H, grid, (const float*)c.mpPart.p, gW + wOff, gW + bOff);
+    };
     int nd = d.on ? c.nDynB : 0;
     // heads
     launch(headDiagBackKernel, blocksFor(nv), TB, 0, c.s, nv, (const float*)c.mpHeadD.p, (const int*)c.diagSlot.p, (const float*)c.mpDGS.p, wb, BD,
@@ -1056,18 +1069,16 @@ static double lossT(Ctx& c, const MT* val, const MT* dval, int nprobes, const fl
     for (int l = MPNN_L - 1; l >= 0; --l) {
         const float* agg = c.mpAgg.p + (size_t)l * MPNN_H * nv;
         launch(nodeLayerBackKernel, blocksFor(nv), TB, 0, c.s, nv, (const float*)H(l + 1), (const float*)DH(l + 1), wb + mpWh(l), BD, DH(l), c.mpDAgg.p);
-        wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H, true>, MPNN_H, 2 * MPNN_H, nv, (const float*)H(l), agg, (const unsigned char*)nullptr, mpWh(l), mpBh(l));
+        wgradTc(nv, (const float*)H(l), agg, (const unsigned char*)nullptr, mpWh(l), mpBh(l));
         launch(aggBackKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const float*)c.mpDAgg.p, (const int*)c.mpDeg.p, DES(l + 1));
         if (d.on) launch(aggBackKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const float*)c.mpDAgg.p, (const int*)c.mpDeg.p, DED(l + 1));
         launch(edgeLayerBackKernel, blocksFor(nv), TB, 0, c.s, nv, rs, re, col, (const float*)H(l), (const float*)ES(l + 1), (const float*)DES(l + 1),
                wb + mpWe(l), BD, BX, DES(l), c.mpDS.p);
-        wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H, true>, MPNN_H, 2 * MPNN_H, c.nnzb, (const float*)ES(l), (const float*)BX,
-              (const unsigned char*)c.mpLowS.p, mpWe(l), mpBe(l));
+        wgradTc(c.nnzb, (const float*)ES(l), (const float*)BX, (const unsigned char*)c.mpLowS.p, mpWe(l), mpBe(l));
         if (d.on) {
             launch(edgeLayerBackKernel, blocksFor(nv), TB, 0, c.s, nv, d.rs, d.re, d.col, (const float*)H(l), (const float*)ED(l + 1),
                    (const float*)DED(l + 1), wb + mpWe(l), BD, BX, DED(l), c.mpDSD.p);
-            wgrad(weightGradKernel<MPNN_H, MPNN_H, MPNN_H, true>, MPNN_H, 2 * MPNN_H, nd, (const float*)ED(l), (const float*)BX,
-                  (const unsigned char*)c.mpLowD.p, mpWe(l), mpBe(l));
+            wgradTc(nd, (const float*)ED(l), (const float*)BX, (const unsigned char*)c.mpLowD.p, mpWe(l), mpBe(l));
         }
         launch(dsGatherKernel, blocksFor(nv), TB, 0, c.s, nv, (const int*)c.rowPtr.p, col, (const int*)c.mpMirS.p, (const float*)c.mpDS.p, d.rs, d.re,
                d.col, (const int*)c.mpMirD.p, (const float*)c.mpDSD.p, DH(l));
