@@ -17,7 +17,6 @@
 // CPU IPC/Friction.cpp:81-545; computeEnergy barrier part IPCSolver.cpp:398-451.
 #include "cipc_internal.h"
 #include "distance_derivs.cuh"
-#include "distance_rows.cuh"
 #include "geometry.cuh"
 
 #include <cub/cub.cuh>
@@ -86,22 +85,6 @@ __device__ void distDerivs(int kind, const d3* p, double* g, double* H) {
     case 1: g_PE<double>(v, g); if (H) H_PE<double>(v, H); return;
     case 2: g_PT<double>(v, g); if (H) H_PT<double>(v, H); return;
     default: g_EE<double>(v, g); if (H) H_EE<double>(v, H); return;
-    }
-}
-
-// Row r of the Hessian of the squared distance (the warp's lanes form the
-// rows of one contact side by side); n = 3 * points entries.
-__device__ void distHessRow(int kind, const d3* p, int r, double* out) {
-    double v[12];
-    int np = npts(kind);
-    for (int k = 0; k < np; ++k) { v[3 * k] = p[k].x; v[3 * k + 1] = p[k].y; v[3 * k + 2] = p[k].z; }
-    switch (kind) {
-    case 0:
-        for (int j = 0; j < 6; ++j) out[j] = j == r ? 2.0 : ((j == r + 3 || j + 3 == r) ? -2.0 : 0.0);
-        return;
-    case 1: Hrow_PE<double>(v, r, out); return;
-    case 2: Hrow_PT<double>(v, r, out); return;
-    default: Hrow_EE<double>(v, r, out); return;
     }
 }
 

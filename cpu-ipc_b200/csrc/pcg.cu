@@ -814,10 +814,16 @@ __device__ __forceinline__ void rowAxCached(const PcgArgs<MT, VT>& a, const RowC
     const int lr = row - rc.row0;
     if (row < it.limit) {
         const int kb = rc.rp[lr] - rc.s0, ke = rc.rp[lr + 1] - rc.s0;
-        for (int kk = kb + it.lane; kk < ke; kk += GROUP) {
-            int c = rc.col[kk];
-            VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
-            blockMulAdd(rc.val + (size_t)9 * kk, xv, acc);
+        // two of the lane's slots per round: both gathers are issued before
+        // the products, which stay in slot order
+        for (int kk = kb + it.lane; kk < ke; kk += 2 * GROUP) {
+            const int k1 = kk + GROUP;
+            const bool two = k1 < ke;
+            const int c0 = rc.col[kk], c1 = two ? rc.col[k1] : c0;
+            const VT x0[3] = {u[3 * c0], u[3 * c0 + 1], u[3 * c0 + 2]};
+            const VT x1[3] = {u[3 * c1], u[3 * c1 + 1], u[3 * c1 + 2]};
+            blockMulAdd(rc.val + (size_t)9 * kk, x0, acc);
+            if (two) blockMulAdd(rc.val + (size_t)9 * k1, x1, acc);
         }
         const int ds = rc.drs[2 * lr], de = rc.drs[2 * lr + 1];
         if (rc.d0 >= 0) {
@@ -844,16 +850,26 @@ __device__ __forceinline__ void rowFactorCached(const PcgArgs<MT, VT>& a, const 
                                                 VT acc[3]) {
     const int lr = row - rc.row0;
     const int kb = rc.rp[lr] - rc.s0, ke = rc.rp[lr + 1] - rc.s0;
-    for (int kk = kb + it.lane; kk < ke; kk += GROUP) {
-        int c = rc.col[kk];
-        if (TR ? c < row : c > row) continue;
-        VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
+    // the factor block of slot kk (transposed on the diagonal of G^T)
+    auto slotMulAdd = [&](int kk, int c, const VT* xv) {
         const float* B = rc.gval ? rc.gval + (size_t)9 * kk : a.gS + (size_t)9 * (kk + rc.s0);
         if (TR && c == row) {
             for (int q = 0; q < 3; ++q) acc[q] += (VT)B[q] * xv[0] + (VT)B[3 + q] * xv[1] + (VT)B[6 + q] * xv[2];
         } else {
             blockMulAdd(B, xv, acc);
         }
+    };
+    // two of the lane's slots per round, as rowAxCached; slots outside this
+    // pass's triangle are skipped
+    for (int kk = kb + it.lane; kk < ke; kk += 2 * GROUP) {
+        const int k1 = kk + GROUP;
+        const int c0 = rc.col[kk], c1 = k1 < ke ? rc.col[k1] : row;
+        const bool on0 = !(TR ? c0 < row : c0 > row), on1 = k1 < ke && !(TR ? c1 < row : c1 > row);
+        const int g0 = on0 ? c0 : row, g1 = on1 ? c1 : row;
+        const VT x0[3] = {u[3 * g0], u[3 * g0 + 1], u[3 * g0 + 2]};
+        const VT x1[3] = {u[3 * g1], u[3 * g1 + 1], u[3 * g1 + 2]};
+        if (on0) slotMulAdd(kk, c0, x0);
+        if (on1) slotMulAdd(k1, c1, x1);
     }
     const int ds = rc.drs[2 * lr], de = rc.drs[2 * lr + 1];
     for (int k = ds + it.lane; k < de; k += GROUP) {

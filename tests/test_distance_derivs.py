@@ -37,8 +37,6 @@ def dd():
     L = C.CDLL(so)
     L.dd_grad_hess.restype = C.c_int
     L.dd_grad_hess.argtypes = [C.c_int, dp, dp, dp]
-    L.dd_hess_rows.restype = C.c_int
-    L.dd_hess_rows.argtypes = [C.c_int, dp, dp]
     return L
 
 
@@ -68,20 +66,3 @@ def test_generated_derivatives_match_the_oracle(dd, name):
         worst_h = max(worst_h, np.abs(H.reshape(n, n) - Ho).max() / np.abs(Ho).max())
     assert worst_g <= 1e-10, worst_g
     assert worst_h <= 1e-9, worst_h
-
-
-@pytest.mark.parametrize("name", ["PE", "PT", "EE"])
-def test_row_by_row_hessians_match_the_whole(dd, name):
-    """The barrier kernel forms the distance Hessian one row per lane
-    (distance_rows.cuh); every row agrees with the whole-matrix code."""
-    kind, npts = KINDS[name]
-    rng = np.random.default_rng(10 + kind)
-    n = 3 * npts
-    for trial in range(100):
-        v = np.ascontiguousarray(rng.standard_normal(3 * 4) * 10.0 ** rng.uniform(-3, 1))
-        g, H, R = np.zeros(12), np.zeros(144), np.zeros(144)
-        dd.dd_grad_hess(kind, v.ctypes.data_as(dp), g.ctypes.data_as(dp), H.ctypes.data_as(dp))
-        assert dd.dd_hess_rows(kind, v.ctypes.data_as(dp), R.ctypes.data_as(dp)) == n
-        Hf, Rf = H[:n * n].reshape(n, n), R[:n * n].reshape(n, n)
-        scale = np.abs(Hf).max()
-        assert np.abs(Hf - Rf).max() <= 1e-12 * scale
