@@ -492,10 +492,17 @@ __device__ __forceinline__ void rowFactor(const PcgArgs<MT, VT>& a, int row, int
         const int* ptr = TR ? a.gUptr : a.gLptr;
         const int* cl = TR ? a.gUcol : a.gLcol;
         const __half* G = TR ? a.gU : a.gL;
-        for (int k = ptr[row] + lane; k < ptr[row + 1]; k += GROUP) {
-            const int c = cl[k];
-            VT xv[3] = {u[3 * c], u[3 * c + 1], u[3 * c + 2]};
-            blockMulAddH(G + (size_t)9 * k, xv, acc);
+        // two of the lane's slots per round: both gathers are issued before
+        // the products, which stay in slot order
+        const int ke = ptr[row + 1];
+        for (int k = ptr[row] + lane; k < ke; k += 2 * GROUP) {
+            const int k1 = k + GROUP;
+            const bool two = k1 < ke;
+            const int c0 = cl[k], c1 = two ? cl[k1] : c0;
+            const VT x0[3] = {u[3 * c0], u[3 * c0 + 1], u[3 * c0 + 2]};
+            const VT x1[3] = {u[3 * c1], u[3 * c1 + 1], u[3 * c1 + 2]};
+            blockMulAddH(G + (size_t)9 * k, x0, acc);
+            if (two) blockMulAddH(G + (size_t)9 * k1, x1, acc);
         }
     } else for (int k = a.rowPtr[row] + lane; k < a.rowPtr[row + 1]; k += GROUP) {
         int c = a.col[k];
