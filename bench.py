@@ -345,11 +345,13 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
     newton = pcg = 0
     stages = {k: 0.0 for k in STAGES}
     ndyn = []
+    step_ms = []
     for _ in range(steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         ms, st = sim.timed_steps(1)
         total_ms += ms
+        step_ms.append(round(ms, 3))
         newton += st["newtonIterations"]
         pcg += st["pcgIterations"]
         for k in STAGES:
@@ -360,7 +362,7 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
     nprof, prof_ms = sim.profile_read() if kind else (0, 0.0)
     if kind:
         sim.profile(0)
-    return dict(ms=total_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches, syncs=syncs,
+    return dict(ms=total_ms, step_ms=step_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches, syncs=syncs,
                 stages={k: v / max(1, steps) for k, v in stages.items()})
 
 
@@ -495,7 +497,7 @@ def main():
         cfg = {"workload": workload(args), "description": describe(args), "newton_threshold": scene["params"]["newtonThr"],
                "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
                "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
-               "ms_per_newton_iteration": max_ms / max(1, r["newton"]),
+               "ms_per_newton_iteration": max_ms / max(1, r["newton"]), "step_ms": r["step_ms"],
                "host_syncs_per_newton_iteration": r["syncs"] / max(1, r["newton"]),
                "kernel_launches_per_newton_iteration": r["launches"] / max(1, r["newton"]),
                "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
@@ -510,7 +512,7 @@ def main():
         if rp is not None:
             plain_v = args.steps / (rp["ms"] / 1000.0)
             cfg["plain_fp64_gpu"] = {"steps_per_s": plain_v, "ms_per_newton_iteration": rp["ms"] / max(1, rp["newton"]),
-                                     "newton_iterations": rp["newton"], "pcg_iterations": rp["pcg"],
+                                     "newton_iterations": rp["newton"], "pcg_iterations": rp["pcg"], "step_ms": rp["step_ms"],
                                      "speedup_of_this_config": (value / world) / plain_v}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

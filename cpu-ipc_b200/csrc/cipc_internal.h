@@ -113,6 +113,8 @@ struct Ctx {
     bool tcFault = false;
     long long hostSyncs = 0;  // host waits on the context's stream (hostSync)
     DBuf<double> stepScal;  // device scalars of the chained step bounds
+    DBuf<int2> ccdPairs;    // candidate pairs of the full edge-edge CCD (query, candidate)
+    DBuf<int> ccdPairCount; // their number (may exceed the buffer: the caller grows it and runs again)
     // hook at the linear-solve seam (NewtonLinearSystem::solve): Adam
     // iterations of the network on every assembled Newton system, and/or a
     // dump of every system to files in dumpDir

@@ -685,57 +685,81 @@ __global__ void partialCCDKernel(int nPT, int nEE, const uint64_t* ccdPT, const 
     }
 }
 
+// Full point-triangle CCD in two kernels (as the edge-edge one below): the
+// walk of each surface vertex's swept box emits (vertex, face) pairs that do
+// not share a vertex and are not all colliders, then one thread per pair
+// runs the additive CCD.
 template <class View>
-__global__ void fullPTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, const double* dir, double stepVal,
-                             const double* stepPtr, View tree, double eta, double* out, int* status) {
+__global__ void fullPTPairsKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, const double* dir,
+                                  double stepVal, const double* stepPtr, View tree, int2* pairs, int cap, int* count, int* status) {
     const double step = stepPtr ? *stepPtr : stepVal;
     CIPC_KERNEL_LOOP(svI, nsv) {
-        int vI = surfVerts[svI];
-        d3 p = ld3(x, vI), dp = ld3(dir, vI);
+        const int vI = surfVerts[svI];
+        const d3 p = ld3(x, vI), dp = ld3(dir, vI);
         double lo[3], hi[3];
         boxInit(lo, hi);
         sweptAdd(lo, hi, p, dp, step);
-        double best = 1.0;
         traverse(tree, lo, hi, 0.0, status, [&](int sfI) {
-            int f0 = faces[3 * sfI], f1 = faces[3 * sfI + 1], f2 = faces[3 * sfI + 2];
+            const int f0 = faces[3 * sfI], f1 = faces[3 * sfI + 1], f2 = faces[3 * sfI + 2];
             if (isCollider(btype[vI]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
             if (vI == f0 || vI == f1 || vI == f2) return;
-            double a = pointTriangleCCD(p, ld3(x, f0), ld3(x, f1), ld3(x, f2), -dp, -ld3(dir, f0), -ld3(dir, f1), -ld3(dir, f2), eta, status);
-            best = fmin(a, best);
+            cg::coalesced_group g = cg::coalesced_threads();
+            int base = 0;
+            if (g.thread_rank() == 0) base = atomicAdd(count, (int)g.size());
+            const int i = g.shfl(base, 0) + (int)g.thread_rank();
+            if (i < cap) pairs[i] = make_int2(vI, sfI);
         });
-        out[svI] = best;
     }
 }
 
+__global__ void fullPTAccdKernel(const int2* pairs, const int* count, int cap, const int* faces, const double* x, const double* dir, double eta,
+                                 double* outMin, int* status) {
+    const int n = min(*count, cap);
+    double best = 1.0;
+    CIPC_KERNEL_LOOP(k, n) {
+        const int2 pr = pairs[k];
+        const int vI = pr.x, f0 = faces[3 * pr.y], f1 = faces[3 * pr.y + 1], f2 = faces[3 * pr.y + 2];
+        best = fmin(pointTriangleCCD(ld3(x, vI), ld3(x, f0), ld3(x, f1), ld3(x, f2), -ld3(dir, vI), -ld3(dir, f0), -ld3(dir, f1), -ld3(dir, f2), eta,
+                                     status),
+                    best);
+    }
+    best = blockReduce(best, MinOp(), 1.0);
+    if (threadIdx.x == 0) atomicMin(reinterpret_cast<unsigned long long*>(outMin), (unsigned long long)__double_as_longlong(best));
+}
+
+// Full edge-edge CCD in two kernels, so that the additive CCD runs one
+// thread per candidate pair instead of inside the divergent tree walk.  The
+// walk emits (query eJ, candidate eI > eJ) as the reference forms its pairs
+// (Self_largestFeasibleStepSize_CCD): no two colliders, no shared vertex, and
+// swept boxes at the entry step that overlap.  Pairs past `cap` are counted
+// but not stored; the caller grows the buffer and runs again.
 template <class View>
-__global__ void fullEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* dir, const double* treeBoxLo,
-                             const double* treeBoxHi, double eeStepVal, const double* eeStepPtr, View tree, double eta, double* out, int* status) {
+__global__ void fullEEPairsKernel(int ne, const int* edges, const int* btype, const double* x, const double* dir, const double* treeBoxLo,
+                                  const double* treeBoxHi, double eeStepVal, const double* eeStepPtr, View tree, int2* pairs, int cap, int* count,
+                                  int* status) {
     const double eeStep = eeStepPtr ? *eeStepPtr : eeStepVal;
     CIPC_KERNEL_LOOP(self, ne) {
         double qlo[3], qhi[3];
         for (int k = 0; k < 3; ++k) { qlo[k] = treeBoxLo[3 * self + k]; qhi[k] = treeBoxHi[3 * self + k]; }
         const bool large = View::kSplitsBig && isLargeBox(qlo, qhi, tree.bigExtent);
-        double best = 1.0;
-        // the pair of query eJ and candidate eI > eJ as the reference forms it
-        // (Self_largestFeasibleStepSize_CCD): the swept boxes at the entry
-        // step must overlap, then the additive CCD with eI's points first
         auto pair = [&](int eJ, int eI) {
             int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
             int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
             if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[g0]) && isCollider(btype[g1])) return;
             if (e0 == g0 || e0 == g1 || e1 == g0 || e1 == g1) return;
-            d3 q0 = ld3(x, g0), q1 = ld3(x, g1), dq0 = ld3(dir, g0), dq1 = ld3(dir, g1);
-            d3 p0 = ld3(x, e0), p1 = ld3(x, e1), dp0 = ld3(dir, e0), dp1 = ld3(dir, e1);
             double blo[3], bhi[3], clo[3], chi[3];
             boxInit(blo, bhi);
-            sweptAdd(blo, bhi, q0, dq0, eeStep);
-            sweptAdd(blo, bhi, q1, dq1, eeStep);
+            sweptAdd(blo, bhi, ld3(x, g0), ld3(dir, g0), eeStep);
+            sweptAdd(blo, bhi, ld3(x, g1), ld3(dir, g1), eeStep);
             boxInit(clo, chi);
-            sweptAdd(clo, chi, p0, dp0, eeStep);
-            sweptAdd(clo, chi, p1, dp1, eeStep);
+            sweptAdd(clo, chi, ld3(x, e0), ld3(dir, e0), eeStep);
+            sweptAdd(clo, chi, ld3(x, e1), ld3(dir, e1), eeStep);
             if (!overlaps(blo, bhi, clo, chi, 0.0)) return;
-            double a = edgeEdgeCCD(p0, p1, q0, q1, -dp0, -dp1, -dq0, -dq1, eta, status);
-            best = fmin(a, best);
+            cg::coalesced_group g = cg::coalesced_threads();
+            int base = 0;
+            if (g.thread_rank() == 0) base = atomicAdd(count, (int)g.size());
+            const int i = g.shfl(base, 0) + (int)g.thread_rank();
+            if (i < cap) pairs[i] = make_int2(eJ, eI);
         };
         traverse2(tree, qlo, qhi, 0.0, large, status, [&](int other, bool fromLarge) {
             if (!fromLarge || large) {
@@ -745,9 +769,31 @@ __global__ void fullEEKernel(int ne, const int* edges, const int* btype, const d
                 else pair(other, self);
             }
         });
-        out[self] = best;
     }
 }
+
+// The additive CCD of every stored pair (eI's points first, as the
+// reference calls it); the minimum of 1 and every time of impact goes into
+// *outMin by an atomic minimum on the bit pattern (non-negative doubles order
+// as their bits), so the result does not depend on the order of the pairs.
+__global__ void fullEEAccdKernel(const int2* pairs, const int* count, int cap, const int* edges, const double* x, const double* dir, double eta,
+                                 double* outMin, int* status) {
+    const int n = min(*count, cap);
+    double best = 1.0;
+    CIPC_KERNEL_LOOP(k, n) {
+        const int2 pr = pairs[k];
+        const int g0 = edges[2 * pr.x], g1 = edges[2 * pr.x + 1];
+        const int e0 = edges[2 * pr.y], e1 = edges[2 * pr.y + 1];
+        const d3 q0 = ld3(x, g0), q1 = ld3(x, g1), dq0 = ld3(dir, g0), dq1 = ld3(dir, g1);
+        const d3 p0 = ld3(x, e0), p1 = ld3(x, e1), dp0 = ld3(dir, e0), dp1 = ld3(dir, e1);
+        best = fmin(edgeEdgeCCD(p0, p1, q0, q1, -dp0, -dp1, -dq0, -dq1, eta, status), best);
+    }
+    best = blockReduce(best, MinOp(), 1.0);
+    if (threadIdx.x == 0) atomicMin(reinterpret_cast<unsigned long long*>(outMin), (unsigned long long)__double_as_longlong(best));
+}
+
+__global__ void setDoubleKernel(double* p, double v) { *p = v; }
+__global__ void copyCountKernel(const int* count, double* out) { *out = (double)*count; }
 
 // The segment-triangle test of one (face, edge) pair (the filters of
 // checkEdgeTriIntersectionIfAny, IPCSolver.cpp:514-542).
@@ -1098,6 +1144,41 @@ double cflBound(Ctx& c) {
     return mx > 0.0 ? sqrt(c.P.Hhat) / (mx * 2.0) : 1.0;
 }
 
+// The full edge-edge CCD over the swept edge tree (built with the entry
+// step stepVal, or *stepPtr when given): candidate pairs, then one thread per
+// pair; min(1, every time of impact) into the device scalar *outMin.  The
+// pair count stays on the device (ccdPairCount): a caller that finds it above
+// the buffer's capacity grows the buffer and runs again.
+static int ccdPairsReserve(Ctx& c) {
+    c.ccdPairCount.reserve(2);
+    c.ccdPairs.reserve(std::max<size_t>(1024, 8 * (size_t)std::max(c.nse, c.nsv)));
+    return (int)std::min<size_t>(c.ccdPairs.cap, 0x7fffffff);
+}
+static void fullEEDevice(Ctx& c, const double* d, double stepVal, const double* stepPtr, double* outMin) {
+    const int cap = ccdPairsReserve(c);
+    CIPC_CUDA(cudaMemsetAsync(c.ccdPairCount.p + 1, 0, sizeof(int), c.s));
+    launch(setDoubleKernel, 1, 1, 0, c.s, outMin, 1.0);
+    withView(c, c.edgeTree, [&](auto v) {
+        launch(fullEEPairsKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi,
+               stepVal, stepPtr, v, c.ccdPairs.p, cap, c.ccdPairCount.p + 1, c.status);
+    });
+    launch(fullEEAccdKernel, 148 * 8, TB, 0, c.s, (const int2*)c.ccdPairs.p, (const int*)c.ccdPairCount.p + 1, cap, c.edges, c.x, d, 1.0 - 0.8,
+           outMin, c.status);
+}
+// The same for the point-triangle pairs (surface vertices against the swept
+// face tree), count in ccdPairCount[0].
+static void fullPTDevice(Ctx& c, const double* d, double stepVal, const double* stepPtr, double* outMin) {
+    const int cap = ccdPairsReserve(c);
+    CIPC_CUDA(cudaMemsetAsync(c.ccdPairCount.p, 0, sizeof(int), c.s));
+    launch(setDoubleKernel, 1, 1, 0, c.s, outMin, 1.0);
+    withView(c, c.faceTree, [&](auto v) {
+        launch(fullPTPairsKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, stepVal, stepPtr, v,
+               c.ccdPairs.p, cap, c.ccdPairCount.p, c.status);
+    });
+    launch(fullPTAccdKernel, 148 * 8, TB, 0, c.s, (const int2*)c.ccdPairs.p, (const int*)c.ccdPairCount.p, cap, c.faces, c.x, d, 1.0 - 0.8, outMin,
+           c.status);
+}
+
 // Swept build with the entry step, then Self_largestFeasibleStepSize_CCD.
 double fullCCDDir(Ctx& c, const double* d, double alpha) {
     double step = alpha;
@@ -1105,21 +1186,26 @@ double fullCCDDir(Ctx& c, const double* d, double alpha) {
     buildBroad(c, c.faceTree, c.nsf);
     computeEdgeBoxes(c, c.x, d, step, true);
     buildBroad(c, c.edgeTree, c.nse);
-    c.energyBuf.reserve(std::max(std::max(c.nsv, c.nse), 1));
-    if (c.nsv) {
-        profBegin(c, PROF_FULLCCD);
-        withView(c, c.faceTree, [&](auto v) { launch(fullPTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, d, step, (const double*)nullptr, v,
-               1.0 - 0.8, c.energyBuf, c.status); });
-        profEnd(c, PROF_FULLCCD);
-        step = std::min(step, deviceMin(c, c.energyBuf, c.nsv, 1e308));
-    }
-    if (c.nse) {
-        profBegin(c, PROF_FULLCCD);
-        withView(c, c.edgeTree, [&](auto v) { launch(fullEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, d, c.edgeTree.primLo, c.edgeTree.primHi, step,
-               (const double*)nullptr, v, 1.0 - 0.8, c.energyBuf, c.status); });
-        profEnd(c, PROF_FULLCCD);
-        step = std::min(step, deviceMin(c, c.energyBuf, c.nse, 1e308));
-    }
+    c.stepScal.reserve(16);
+    double* sm = c.stepScal.p + 12;  // [12] minimum, [13] pair count
+    // one pass (point-triangle or edge-edge) with the host's entry step; a
+    // pair buffer that was too small is grown and the pass runs again
+    auto pass = [&](bool pt) {
+        for (;;) {
+            profBegin(c, PROF_FULLCCD);
+            if (pt) fullPTDevice(c, d, step, nullptr, sm);
+            else fullEEDevice(c, d, step, nullptr, sm);
+            profEnd(c, PROF_FULLCCD);
+            launch(copyCountKernel, 1, 1, 0, c.s, (const int*)c.ccdPairCount.p + (pt ? 0 : 1), sm + 1);
+            double h[2];
+            CIPC_CUDA(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, c.s));
+            hostSync(c);
+            if (h[1] <= (double)c.ccdPairs.cap) { step = std::min(step, h[0]); return; }
+            c.ccdPairs.reserve((size_t)h[1]);
+        }
+    };
+    if (c.nsv) pass(true);
+    if (c.nse) pass(false);
     checkStatus(c, "full CCD");
     return step;
 }
@@ -1130,7 +1216,8 @@ namespace {
 // Scalars of the chained step bounds (stepBoundsDevice), one thread each.
 // s: 0 ground min, 1 partial-CCD min, 2 max surface move, 3 entry step,
 // 4 full point-triangle min, 5 edge-edge entry step, 6 full edge-edge min,
-// 7 merged step, 8 status word.
+// 7 merged step, 8 status word, 9 and 10 point-triangle and edge-edge
+// CCD pair counts.
 __global__ void stepEntryKernel(double* s, int nsv) {
     double a = nsv ? s[0] : 1.0;
     a = fmin(1.0, a);
@@ -1191,28 +1278,35 @@ double stepBoundsDevice(Ctx& c) {
         buildBroad(c, c.faceTree, c.nsf);
         computeEdgeBoxes(c, c.x, c.dir, 0.0, true, s + 3);
         buildBroad(c, c.edgeTree, c.nse);
+        ccdPairsReserve(c);
+        CIPC_CUDA(cudaMemsetAsync(c.ccdPairCount.p, 0, 2 * sizeof(int), c.s));
         if (c.nsv) {
             profBegin(c, PROF_FULLCCD);
-            withView(c, c.faceTree, [&](auto v) { launch(fullPTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, c.dir, 0.0, (const double*)(s + 3),
-                   v, 1.0 - 0.8, c.energyBuf, c.status); });
+            fullPTDevice(c, c.dir, 0.0, s + 3, s + 4);
             profEnd(c, PROF_FULLCCD);
-            deviceMinTo(c, c.energyBuf, c.nsv, s + 4);
             launch(stepEeEntryKernel, 1, 1, 0, c.s, s);
         }
         if (c.nse) {
             profBegin(c, PROF_FULLCCD);
-            withView(c, c.edgeTree, [&](auto v) { launch(fullEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.dir, c.edgeTree.primLo, c.edgeTree.primHi, 0.0,
-                   (const double*)(s + 5), v, 1.0 - 0.8, c.energyBuf, c.status); });
+            fullEEDevice(c, c.dir, 0.0, s + 5, s + 6);
             profEnd(c, PROF_FULLCCD);
-            deviceMinTo(c, c.energyBuf, c.nse, s + 6);
         }
+        launch(copyCountKernel, 1, 1, 0, c.s, (const int*)c.ccdPairCount.p, s + 9);
+        launch(copyCountKernel, 1, 1, 0, c.s, (const int*)c.ccdPairCount.p + 1, s + 10);
     }
     launch(stepMergeKernel, 1, 1, 0, c.s, s, c.nsv, c.nse, nPartial, c.P.useBarrier ? 1 : 0, std::sqrt(c.P.Hhat), (const int*)c.status.p);
     CIPC_CUDA(cudaGetLastError());
-    double h[9];
+    double h[11];
     CIPC_CUDA(cudaMemcpyAsync(h, s, sizeof(h), cudaMemcpyDeviceToHost, c.s));
     hostSync(c);
     if (h[8] != 0.0) checkStatus(c, "step bounds");
+    const double pairs = std::max(h[9], h[10]);
+    if (c.P.useBarrier && pairs > (double)c.ccdPairs.cap) {
+        // more CCD candidates than the pair buffer holds: grow it and
+        // recompute the bounds (every input is unchanged)
+        c.ccdPairs.reserve((size_t)pairs);
+        return stepBoundsDevice(c);
+    }
     return h[7];
 }
 

@@ -662,7 +662,7 @@ void cipc_gpu_destroy(cipc_gpu_context* h) {
         DBuf<uint64_t>* us[] = {&c.ccdPT, &c.ccdEE, &c.kPT, &c.kEE, &c.kMoll, &c.kPPE, &c.kTmp, &c.uniq, &c.dynHKey, &c.dynHKeyAlt,
                                 &c.faceTree.keys, &c.faceTree.keysAlt, &c.edgeTree.keys, &c.edgeTree.keysAlt};
         for (auto* d : us) d->free();
-        c.sortTmp.free(); c.groundTmp.free(); c.barrierUpper.free(); c.stepScal.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
+        c.sortTmp.free(); c.groundTmp.free(); c.barrierUpper.free(); c.ccdPairs.free(); c.ccdPairCount.free(); c.stepScal.free(); c.faceTree.sortTmp.free(); c.edgeTree.sortTmp.free();
         c.gLptr.free(); c.gLcol.free(); c.gLslot.free(); c.gUptr.free(); c.gUcol.free(); c.gUslot.free(); c.gLval.free(); c.gUval.free();
         for (DevBvh* t : {&c.faceTree, &c.edgeTree}) {
             t->hashKey.free(); t->hashKeyAlt.free(); t->hashPrim.free(); t->hashPrimAlt.free(); t->hashCount.free(); t->hashOffset.free();
