@@ -513,9 +513,14 @@ struct Emit {
     }
 };
 
+// Active sets in two kernels per kind, so that the distance classification
+// runs one thread per candidate instead of inside the divergent tree walk:
+// the walk emits every candidate pair (the partial-CCD set), then one thread
+// per stored candidate classifies it and emits the contact keys.  The sets
+// are sorted afterwards, so the order of emission does not matter.
 template <class View>
-__global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, View tree, double sq,
-                               double Hhat, Emit ccd, Emit ptk, Emit ppe, int* status) {
+__global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, const int* btype, const double* x, View tree, double sq, Emit ccd,
+                               int* status) {
     CIPC_KERNEL_LOOP(svI, nsv) {
         int vI = surfVerts[svI];
         d3 p = ld3(x, vI);
@@ -525,60 +530,47 @@ __global__ void activePTKernel(int nsv, const int* surfVerts, const int* faces, 
             if (isCollider(btype[vI]) && isCollider(btype[f0]) && isCollider(btype[f1]) && isCollider(btype[f2])) return;
             if (vI == f0 || vI == f1 || vI == f2) return;
             ccd(((uint64_t)svI << 32) | (uint32_t)sfI, status);
-            d3 a = ld3(x, f0), b = ld3(x, f1), c = ld3(x, f2);
-            int t = dTypePT(p, a, b, c);
-            double d;
-            switch (t) {
-            case 0: d = dPP(p, a); if (d < Hhat) ppe(ppeKey(-vI - 1, f0, -1), status); break;
-            case 1: d = dPP(p, b); if (d < Hhat) ppe(ppeKey(-vI - 1, f1, -1), status); break;
-            case 2: d = dPP(p, c); if (d < Hhat) ppe(ppeKey(-vI - 1, f2, -1), status); break;
-            case 3: d = dPE(p, a, b); if (d < Hhat) ppe(ppeKey(-vI - 1, f0, f1), status); break;
-            case 4: d = dPE(p, b, c); if (d < Hhat) ppe(ppeKey(-vI - 1, f1, f2), status); break;
-            case 5: d = dPE(p, c, a); if (d < Hhat) ppe(ppeKey(-vI - 1, f2, f0), status); break;
-            default: d = dPT(p, a, b, c); if (d < Hhat) ptk(((uint64_t)svI << 32) | (uint32_t)sfI, status); break;
-            }
         });
     }
 }
 
+// the point-triangle candidates (svI << 32 | sfI) stored by activePTKernel
+__global__ void activePTClassKernel(const uint64_t* cand, const int* count, int cap, const int* surfVerts, const int* faces, const double* x,
+                                    double Hhat, Emit ptk, Emit ppe, int* status) {
+    const int n = min(*count, cap);
+    CIPC_KERNEL_LOOP(k, n) {
+        const uint64_t key = cand[k];
+        const int svI = (int)(key >> 32), sfI = (int)(key & 0xffffffffu);
+        const int vI = surfVerts[svI];
+        const int f0 = faces[3 * sfI], f1 = faces[3 * sfI + 1], f2 = faces[3 * sfI + 2];
+        const d3 p = ld3(x, vI), a = ld3(x, f0), b = ld3(x, f1), c = ld3(x, f2);
+        double d;
+        switch (dTypePT(p, a, b, c)) {
+        case 0: d = dPP(p, a); if (d < Hhat) ppe(ppeKey(-vI - 1, f0, -1), status); break;
+        case 1: d = dPP(p, b); if (d < Hhat) ppe(ppeKey(-vI - 1, f1, -1), status); break;
+        case 2: d = dPP(p, c); if (d < Hhat) ppe(ppeKey(-vI - 1, f2, -1), status); break;
+        case 3: d = dPE(p, a, b); if (d < Hhat) ppe(ppeKey(-vI - 1, f0, f1), status); break;
+        case 4: d = dPE(p, b, c); if (d < Hhat) ppe(ppeKey(-vI - 1, f1, f2), status); break;
+        case 5: d = dPE(p, c, a); if (d < Hhat) ppe(ppeKey(-vI - 1, f2, f0), status); break;
+        default: d = dPT(p, a, b, c); if (d < Hhat) ptk(key, status); break;
+        }
+    }
+}
+
 template <class View>
-__global__ void activeEEKernel(int ne, const int* edges, const int* btype, const double* x, const double* rest, View tree, double sq,
-                               double Hhat, Emit ccd, Emit eek, Emit moll, Emit ppe, int* status) {
+__global__ void activeEEKernel(int ne, const int* edges, const int* btype, const double* x, View tree, double sq, Emit ccd, int* status) {
     CIPC_KERNEL_LOOP(self, ne) {
         double lo[3], hi[3];
         boxInit(lo, hi);
         boxAdd(lo, hi, ld3(x, edges[2 * self])); boxAdd(lo, hi, ld3(x, edges[2 * self + 1]));
         const bool large = View::kSplitsBig && isLargeBox(lo, hi, tree.bigExtent);
-        // the pair (eI, eJ), eI < eJ, as the reference classifies it: eI's
-        // points first
+        // the pair (eI, eJ), eI < eJ, as the reference forms it
         auto pair = [&](int eI, int eJ) {
             int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
             int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
             if (isCollider(btype[e0]) && isCollider(btype[e1]) && isCollider(btype[g0]) && isCollider(btype[g1])) return;
             if (e0 == g0 || e0 == g1 || e1 == g0 || e1 == g1) return;
             ccd(((uint64_t)eI << 32) | (uint32_t)eJ, status);
-            d3 p0 = ld3(x, e0), p1 = ld3(x, e1), q0 = ld3(x, g0), q1 = ld3(x, g1);
-            int t = dTypeEE(p0, p1, q0, q1);
-            double cs = crossSqNormEE(p0, p1, q0, q1);
-            double ex = 1e-3 * sqn(ld3(rest, e0) - ld3(rest, e1)) * sqn(ld3(rest, g0) - ld3(rest, g1));
-            bool mol = cs < ex;
-            double d;
-            int c0 = 0, c1 = 0, c2 = -1;
-            switch (t) {
-            case 0: d = dPP(p0, q0); c0 = -e0 - 1; c1 = g0; break;
-            case 1: d = dPP(p0, q1); c0 = -e0 - 1; c1 = g1; break;
-            case 2: d = dPE(p0, q0, q1); c0 = -e0 - 1; c1 = g0; c2 = g1; break;
-            case 3: d = dPP(p1, q0); c0 = -e1 - 1; c1 = g0; break;
-            case 4: d = dPP(p1, q1); c0 = -e1 - 1; c1 = g1; break;
-            case 5: d = dPE(p1, q0, q1); c0 = -e1 - 1; c1 = g0; c2 = g1; break;
-            case 6: d = dPE(q0, p0, p1); c0 = -g0 - 1; c1 = e0; c2 = e1; break;
-            case 7: d = dPE(q1, p0, p1); c0 = -g1 - 1; c1 = e0; c2 = e1; break;
-            default: d = dEE(p0, p1, q0, q1); break;
-            }
-            if (!(d < Hhat)) return;
-            if (mol) moll(((uint64_t)eI << 34) | ((uint64_t)eJ << 4) | (uint64_t)t, status);
-            else if (t == 8) eek(((uint64_t)eI << 32) | (uint32_t)eJ, status);
-            else ppe(ppeKey(c0, c1, c2), status);
         };
         traverse2(tree, lo, hi, sq, large, status, [&](int other, bool fromLarge) {
             // a pair is handled once: by its lower index, except that a
@@ -590,6 +582,41 @@ __global__ void activeEEKernel(int ne, const int* edges, const int* btype, const
                 else pair(other, self);
             }
         });
+    }
+}
+
+// the edge-edge candidates (eI << 32 | eJ) stored by activeEEKernel,
+// classified as the reference does with eI's points first
+__global__ void activeEEClassKernel(const uint64_t* cand, const int* count, int cap, const int* edges, const double* x, const double* rest,
+                                    double Hhat, Emit eek, Emit moll, Emit ppe, int* status) {
+    const int n = min(*count, cap);
+    CIPC_KERNEL_LOOP(k, n) {
+        const uint64_t key = cand[k];
+        const int eI = (int)(key >> 32), eJ = (int)(key & 0xffffffffu);
+        const int e0 = edges[2 * eI], e1 = edges[2 * eI + 1];
+        const int g0 = edges[2 * eJ], g1 = edges[2 * eJ + 1];
+        const d3 p0 = ld3(x, e0), p1 = ld3(x, e1), q0 = ld3(x, g0), q1 = ld3(x, g1);
+        const int t = dTypeEE(p0, p1, q0, q1);
+        const double cs = crossSqNormEE(p0, p1, q0, q1);
+        const double ex = 1e-3 * sqn(ld3(rest, e0) - ld3(rest, e1)) * sqn(ld3(rest, g0) - ld3(rest, g1));
+        const bool mol = cs < ex;
+        double d;
+        int c0 = 0, c1 = 0, c2 = -1;
+        switch (t) {
+        case 0: d = dPP(p0, q0); c0 = -e0 - 1; c1 = g0; break;
+        case 1: d = dPP(p0, q1); c0 = -e0 - 1; c1 = g1; break;
+        case 2: d = dPE(p0, q0, q1); c0 = -e0 - 1; c1 = g0; c2 = g1; break;
+        case 3: d = dPP(p1, q0); c0 = -e1 - 1; c1 = g0; break;
+        case 4: d = dPP(p1, q1); c0 = -e1 - 1; c1 = g1; break;
+        case 5: d = dPE(p1, q0, q1); c0 = -e1 - 1; c1 = g0; c2 = g1; break;
+        case 6: d = dPE(q0, p0, p1); c0 = -g0 - 1; c1 = e0; c2 = e1; break;
+        case 7: d = dPE(q1, p0, p1); c0 = -g1 - 1; c1 = e0; c2 = e1; break;
+        default: d = dEE(p0, p1, q0, q1); break;
+        }
+        if (!(d < Hhat)) continue;
+        if (mol) moll(((uint64_t)eI << 34) | ((uint64_t)eJ << 4) | (uint64_t)t, status);
+        else if (t == 8) eek(key, status);
+        else ppe(ppeKey(c0, c1, c2), status);
     }
 }
 
@@ -808,20 +835,35 @@ __device__ __forceinline__ bool faceEdgeHit(const int* faces, const int* edges, 
 // Faces against the edge tree.  A large face (one the face tree keeps out of
 // its tree) meets only the edge tree's large edges here; its pairs with the
 // other edges are tested by largeFaceKernel from the edges' side.
+// Intersection test in two kernels, as the full CCD: each face's walk over
+// the edge tree emits its candidate (face, edge) pairs, then one thread per
+// pair runs the segment-triangle test (faceEdgeHit) and raises the flag.
 template <class View>
-__global__ void intersectKernel(int nsf, const int* faces, const int* edges, const int* btype, const double* x, View tree, double coplanarTol,
-                                int* flag, int* status) {
+__global__ void intersectPairsKernel(int nsf, const int* faces, const double* x, View tree, int2* pairs, int cap, int* count, int* status) {
     CIPC_KERNEL_LOOP(f, nsf) {
         double lo[3], hi[3];
         boxInit(lo, hi);
         for (int k = 0; k < 3; ++k) boxAdd(lo, hi, ld3(x, faces[3 * f + k]));
         const bool large = View::kSplitsBig && isLargeBox(lo, hi, tree.bigExtent);
-        bool hit = false;
         traverse2(tree, lo, hi, 0.0, large, status, [&](int e, bool) {
-            if (!hit && faceEdgeHit(faces, edges, btype, x, f, e, coplanarTol)) hit = true;
+            cg::coalesced_group g = cg::coalesced_threads();
+            int base = 0;
+            if (g.thread_rank() == 0) base = atomicAdd(count, (int)g.size());
+            const int i = g.shfl(base, 0) + (int)g.thread_rank();
+            if (i < cap) pairs[i] = make_int2(f, e);
         });
-        if (hit) atomicOr(flag, 1);
     }
+}
+
+__global__ void intersectTestKernel(const int2* pairs, const int* count, int cap, const int* faces, const int* edges, const int* btype,
+                                    const double* x, double coplanarTol, int* flag) {
+    const int n = min(*count, cap);
+    bool hit = false;
+    CIPC_KERNEL_LOOP(k, n) {
+        const int2 pr = pairs[k];
+        if (!hit && faceEdgeHit(faces, edges, btype, x, pr.x, pr.y, coplanarTol)) hit = true;
+    }
+    if (hit) atomicOr(flag, 1);
 }
 
 // The edges that are not large (the edge tree's own) against the large faces
@@ -1026,12 +1068,20 @@ void buildCollisionSets(Ctx& c, bool rehash) {
             Emit eCcdPT{c.ccdPT, caps[0], c.counters.p + 0}, ePT{c.kPT, caps[1], c.counters.p + 1}, ePPE{c.kPPE, caps[2], c.counters.p + 2};
             Emit eCcdEE{c.ccdEE, caps[3], c.counters.p + 3}, eEE{c.kEE, caps[4], c.counters.p + 4}, eMoll{c.kMoll, caps[5], c.counters.p + 5};
             profBegin(c, PROF_ACTIVE);
-            if (c.nsv)
-                withView(c, c.faceTree, [&](auto v) { launch(activePTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, v, sq, c.P.Hhat,
-                                                                  eCcdPT, ePT, ePPE, c.status); });
-            if (c.nse)
-                withView(c, c.edgeTree, [&](auto v) { launch(activeEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, c.rest, v, sq, c.P.Hhat, eCcdEE,
-                                                                  eEE, eMoll, ePPE, c.status); });
+            if (c.nsv) {
+                withView(c, c.faceTree, [&](auto v) {
+                    launch(activePTKernel<decltype(v)>, blocksFor(c.nsv), TB, 0, c.s, c.nsv, c.surfVerts, c.faces, c.btype, c.x, v, sq, eCcdPT, c.status);
+                });
+                launch(activePTClassKernel, 148 * 8, TB, 0, c.s, (const uint64_t*)c.ccdPT.p, (const int*)c.counters.p + 0, caps[0], c.surfVerts, c.faces,
+                       c.x, c.P.Hhat, ePT, ePPE, c.status);
+            }
+            if (c.nse) {
+                withView(c, c.edgeTree, [&](auto v) {
+                    launch(activeEEKernel<decltype(v)>, blocksFor(c.nse), TB, 0, c.s, c.nse, c.edges, c.btype, c.x, v, sq, eCcdEE, c.status);
+                });
+                launch(activeEEClassKernel, 148 * 8, TB, 0, c.s, (const uint64_t*)c.ccdEE.p, (const int*)c.counters.p + 3, caps[3], c.edges, c.x, c.rest,
+                       c.P.Hhat, eEE, eMoll, ePPE, c.status);
+            }
             profEnd(c, PROF_ACTIVE);
             CIPC_CUDA(cudaGetLastError());
             CIPC_CUDA(cudaMemcpyAsync(cnt, c.counters.p, 6 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
@@ -1095,6 +1145,9 @@ void buildCollisionSets(Ctx& c, bool rehash) {
     }
 }
 
+// the candidate-pair buffer shared by the intersection test and the full CCD
+static int ccdPairsReserve(Ctx& c);
+
 bool isIntersected(Ctx& c) {
     c.counters.reserve(16);
     CIPC_CUDA(cudaMemsetAsync(c.counters.p + 7, 0, sizeof(int), c.s));
@@ -1104,14 +1157,28 @@ bool isIntersected(Ctx& c) {
     if (c.nse && c.nsf && c.broadPhase == CIPC_BROAD_PHASE_LBVH)
         launch(largeFaceKernel, blocksFor(c.nse), TB, 0, c.s, c.nse, c.faces, c.edges, c.btype, c.x, view(c.faceTree), view(c.edgeTree), c.coplanarTol,
                c.counters.p + 7);
-    if (c.nsf) withView(c, c.edgeTree, [&](auto v) { launch(intersectKernel<decltype(v)>, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.edges, c.btype, c.x, v, c.coplanarTol, c.counters.p + 7,
-                            c.status); });
-    int f = 0, st = 0;
-    CIPC_CUDA(cudaMemcpyAsync(&f, c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    hostSync(c);
-    if (st) checkStatus(c, "intersection test");
-    return f != 0;
+    for (;;) {
+        int cap = 0;
+        if (c.nsf) {
+            cap = ccdPairsReserve(c);
+            CIPC_CUDA(cudaMemsetAsync(c.ccdPairCount.p, 0, sizeof(int), c.s));
+            withView(c, c.edgeTree, [&](auto v) {
+                launch(intersectPairsKernel<decltype(v)>, blocksFor(c.nsf), TB, 0, c.s, c.nsf, c.faces, c.x, v, c.ccdPairs.p, cap, c.ccdPairCount.p,
+                       c.status);
+            });
+            launch(intersectTestKernel, 148 * 8, TB, 0, c.s, (const int2*)c.ccdPairs.p, (const int*)c.ccdPairCount.p, cap, c.faces, c.edges, c.btype,
+                   c.x, c.coplanarTol, c.counters.p + 7);
+        }
+        int h[3] = {0, 0, 0};
+        CIPC_CUDA(cudaMemcpyAsync(&h[0], c.counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        CIPC_CUDA(cudaMemcpyAsync(&h[1], c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        if (c.nsf) CIPC_CUDA(cudaMemcpyAsync(&h[2], c.ccdPairCount.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        hostSync(c);
+        if (h[1]) checkStatus(c, "intersection test");
+        // a hit among the stored pairs stands; otherwise every pair must have been tested
+        if (h[0] != 0 || h[2] <= cap) return h[0] != 0;
+        c.ccdPairs.reserve((size_t)h[2]);
+    }
 }
 
 // Rebuild the static trees at the current positions (sh.build in the line search).
