@@ -334,6 +334,13 @@ def whole_job_rate(steps_per_rank, world, max_ms):
     return world * steps_per_rank / (max_ms / 1000.0)
 
 
+def mark(what):
+    """With CIPC_DEBUG_ALLOC=1 (the library then reports every buffer
+    reallocation on stderr), mark the bench's phases on stderr too."""
+    if os.environ.get("CIPC_DEBUG_ALLOC") == "1":
+        print(f"[bench] {what}", file=sys.stderr, flush=True)
+
+
 def device_timed(sim, steps, flush, kind, cipc, torch):
     """Device time of `steps` single steps (CUDA events on the library's
     stream), L2 flushed before each; profile of one kernel family."""
@@ -346,12 +353,15 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
     stages = {k: 0.0 for k in STAGES}
     ndyn = []
     step_ms = []
+    step_newton = []
     for _ in range(steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         ms, st = sim.timed_steps(1)
         total_ms += ms
         step_ms.append(round(ms, 3))
+        step_newton.append(st["newtonIterations"])
+        mark(f"step {ms:.1f} ms")
         newton += st["newtonIterations"]
         pcg += st["pcgIterations"]
         for k in STAGES:
@@ -362,7 +372,7 @@ def device_timed(sim, steps, flush, kind, cipc, torch):
     nprof, prof_ms = sim.profile_read() if kind else (0, 0.0)
     if kind:
         sim.profile(0)
-    return dict(ms=total_ms, step_ms=step_ms, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches, syncs=syncs,
+    return dict(ms=total_ms, step_ms=step_ms, step_newton=step_newton, newton=newton, pcg=pcg, ndyn=ndyn, nprof=nprof, prof_ms=prof_ms, launches=launches, syncs=syncs,
                 stages={k: v / max(1, steps) for k, v in stages.items()})
 
 
@@ -432,7 +442,9 @@ def main():
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStart()
     fb0 = sim.precond_stats()["fallbacks"]
+    mark("timed steps")
     r = device_timed(sim, args.steps, flush, args.roofline_kernel, cipc, torch)
+    mark("timed steps done")
     fb_timed = sim.precond_stats()["fallbacks"] - fb0
     if args.profile_timed:
         torch.cuda.cudart().cudaProfilerStop()
@@ -444,7 +456,9 @@ def main():
             plain.set(k, pins[k])
         plain.set_kappa(kappa0)
         plain.collision_sets()
+        mark("plain steps")
         rp = device_timed(plain, args.steps, flush, None, cipc, torch)
+        mark("plain steps done")
     max_ms = max_over_ranks(r["ms"], pg, "cuda")
     value = whole_job_rate(args.steps, world, max_ms)
 
@@ -498,6 +512,7 @@ def main():
                "precision": args.precision, "preconditioner": args.precond, "pcg_rel_tol": 1e-6,
                "newton_iterations": r["newton"], "pcg_iterations": r["pcg"],
                "ms_per_newton_iteration": max_ms / max(1, r["newton"]), "step_ms": r["step_ms"],
+               "step_newton_iterations": r["step_newton"],
                "host_syncs_per_newton_iteration": r["syncs"] / max(1, r["newton"]),
                "kernel_launches_per_newton_iteration": r["launches"] / max(1, r["newton"]),
                "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed step",
@@ -513,6 +528,7 @@ def main():
             plain_v = args.steps / (rp["ms"] / 1000.0)
             cfg["plain_fp64_gpu"] = {"steps_per_s": plain_v, "ms_per_newton_iteration": rp["ms"] / max(1, rp["newton"]),
                                      "newton_iterations": rp["newton"], "pcg_iterations": rp["pcg"], "step_ms": rp["step_ms"],
+                                     "step_newton_iterations": rp["step_newton"],
                                      "speedup_of_this_config": (value / world) / plain_v}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
 #include <stdexcept>
 #include <cstdint>
 #include <string>
@@ -43,6 +44,11 @@ struct InvalidArgument : std::invalid_argument {
     using std::invalid_argument::invalid_argument;
 };
 
+// CIPC_DEBUG_ALLOC=1: every reallocation of a grow-only buffer is timed on
+// the host and printed to stderr.
+bool debugAlloc();
+void reportAlloc(size_t oldBytes, size_t newBytes, double ms);
+
 // Grow-only device buffer.
 template <class T>
 struct DBuf {
@@ -53,9 +59,12 @@ struct DBuf {
     // page mapping, tens of milliseconds for the pile's contact buffers)
     void reserve(size_t n) {
         if (n <= cap) return;
+        const bool dbg = debugAlloc();
+        const auto t0 = dbg ? std::chrono::steady_clock::now() : std::chrono::steady_clock::time_point();
         if (p) cudaFree(p);
         size_t c = n < 64 ? 64 : 2 * n;
         CIPC_CUDA(cudaMalloc(&p, c * sizeof(T)));
+        if (dbg) reportAlloc(cap * sizeof(T), c * sizeof(T), std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
         cap = c;
     }
     void free() { if (p) cudaFree(p); p = nullptr; cap = 0; }

@@ -119,6 +119,15 @@ double deviceInfNorm(Ctx& c, const double* v, int n) {
     return std::max(0.0, m);
 }
 
+bool debugAlloc() {
+    static int v = -1;
+    if (v < 0) { const char* e = std::getenv("CIPC_DEBUG_ALLOC"); v = (e && *e == '1') ? 1 : 0; }
+    return v == 1;
+}
+void reportAlloc(size_t oldBytes, size_t newBytes, double ms) {
+    std::fprintf(stderr, "[alloc] %zu -> %zu bytes in %.3f ms\n", oldBytes, newBytes, ms);
+}
+
 void checkStatus(Ctx& c, const char* stage) {
     int st = 0;
     CIPC_CUDA(cudaMemcpyAsync(&st, c.status.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
