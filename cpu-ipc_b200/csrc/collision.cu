@@ -24,6 +24,7 @@
 #include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace cipc {
 
@@ -1216,9 +1217,16 @@ double cflBound(Ctx& c) {
 // pair; min(1, every time of impact) into the device scalar *outMin.  The
 // pair count stays on the device (ccdPairCount): a caller that finds it above
 // the buffer's capacity grows the buffer and runs again.
+// First size of the pair buffer: 8 pairs per query, or CIPC_CCD_PAIRS_INITIAL
+// pairs (a small value exercises the grow-and-rerun path).
+static size_t ccdPairsInitial(const Ctx& c) {
+    static long long v = -2;
+    if (v == -2) { const char* e = std::getenv("CIPC_CCD_PAIRS_INITIAL"); v = e ? std::atoll(e) : -1; }
+    return v > 0 ? (size_t)v : std::max<size_t>(1024, 8 * (size_t)std::max(c.nse, c.nsv));
+}
 static int ccdPairsReserve(Ctx& c) {
     c.ccdPairCount.reserve(2);
-    c.ccdPairs.reserve(std::max<size_t>(1024, 8 * (size_t)std::max(c.nse, c.nsv)));
+    c.ccdPairs.reserve(ccdPairsInitial(c));
     return (int)std::min<size_t>(c.ccdPairs.cap, 0x7fffffff);
 }
 static void fullEEDevice(Ctx& c, const double* d, double stepVal, const double* stepPtr, double* outMin) {
