@@ -340,8 +340,8 @@ int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
     const int kmin = 6;
     for (; k < 10000; ++k) {
         auto t0 = Clock::now();
+        // assembleAll ends with a read of the status word: the stream is idle here
         st.collisions += assembleAll(c);
-        sync(c);
         auto t1 = Clock::now();
         linearSolve(c, k);
         st.pcgIterations += c.lastPcgIters;
@@ -368,8 +368,8 @@ int solveBarrierSubproblem(Ctx& c, double kappa, cipc_step_stats& st) {
             st.lineSearchMilliseconds += ms(t3, t4);
             break;
         }
+        // postLineSearch ends with a read-back (its minimum distance): the stream is idle here
         postLineSearch(c, kappa);
-        sync(c);
         auto t5 = Clock::now();
         st.assemblyMilliseconds += ms(t0, t1);
         st.linearSolveMilliseconds += ms(t1, t2);
